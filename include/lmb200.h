@@ -1,0 +1,218 @@
+/*
+ * lmb200 -- B200 (sm_100a) Lorenz-Mie holography kernels behind a C ABI.
+ *
+ * Plain C entry points: device pointers, sizes and a cudaStream_t passed
+ * as void*.  Every function returns an int status (LMB_OK = 0) and never
+ * throws, traps or spin-waits.  All arrays are device memory unless a
+ * parameter says "host".  Calls on one stream are ordered; the library
+ * keeps no hidden state between calls except what is named here.
+ *
+ * Units follow the reference: pixel coordinates and particle positions in
+ * pixels, radii and wavelength in micrometres, magnification in
+ * micrometres per pixel, the wave number k in radians per pixel.
+ */
+#ifndef LMB200_H
+#define LMB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LMB_OK 0
+#define LMB_ERR_ARG 1          /* invalid argument (null pointer, bad size) */
+#define LMB_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define LMB_ERR_NMAX 3         /* a sphere needs more orders than nmax_cap */
+#define LMB_ERR_WORKSPACE 4    /* workspace too small */
+#define LMB_ERR_UNSUPPORTED 5  /* flag combination not supported */
+
+/* flags */
+#define LMB_CARTESIAN 1   /* project the field on x, y, z (else r, theta, phi) */
+#define LMB_BOHREN 2      /* Bohren & Huffman sign convention */
+#define LMB_FP64 4        /* compute the field sum in FP64 (else FP32) */
+
+/* Largest number of partial-wave orders any entry point accepts. */
+#define LMB_NMAX_LIMIT 1024
+
+/*
+ * A homogeneous sphere: position (pixels), radius a_p (um), refractive
+ * index n_p and absorption k_p.  Same six properties, same order, as
+ * Sphere.properties (theory/Sphere.py:63-68, theory/Particle.py:91-95).
+ */
+typedef struct lmb_sphere {
+  double x_p, y_p, z_p, a_p, n_p, k_p;
+} lmb_sphere;
+
+/* Library version as major*10000 + minor*100 + patch. */
+int lmb_version(void);
+
+/* Human-readable text of a status code (static storage). */
+const char *lmb_status_string(int status);
+
+/*
+ * Mie coefficients of nspheres homogeneous spheres, FP64.
+ * Replaces Sphere.ab / Sphere.mie_coefficients (theory/Sphere.py:70-89,
+ * 147-226) and Sphere.wiscombe_yang (:91-123).
+ *   ab    [nspheres][nmax_cap+1][2] complex128 (interleaved re, im):
+ *         ab[s][n][0] = a_n, ab[s][n][1] = b_n, row 0 and rows above
+ *         nmax[s] are zero.
+ *   dab   optional (may be NULL): [nspheres][nmax_cap+1][4] complex128,
+ *         d a_n/d a_p, d b_n/d a_p, d a_n/d n_p, d b_n/d n_p.
+ *   nmax  [nspheres] int: number of orders (the reference's nmax;
+ *         norders = nmax + 1).
+ *   status [nspheres] int: LMB_OK or LMB_ERR_NMAX.
+ */
+int lmb_sphere_ab(const lmb_sphere *spheres, int nspheres, double n_m,
+                  double wavelength, int nmax_cap, double *ab, double *dab,
+                  int *nmax, int *status, void *stream);
+
+/*
+ * Multilayer (core-shell) spheres, FP64, Yang (2003) recurrences.
+ * Replaces lib/obsolete/sphere_coefficients.py:65-220 (with its list-input
+ * handling repaired).  Each sphere has nlayers radii and complex indices,
+ * ordered from the core outwards:
+ *   radii    [nspheres][nlayers] um
+ *   indices  [nspheres][nlayers][2] (re, im)
+ * Outputs as lmb_sphere_ab; dab (optional) holds the derivatives with
+ * respect to the outer radius (all radii scaled together, i.e. at fixed
+ * radius fractions) and to the real part of the outer layer's index.
+ */
+int lmb_layered_ab(const double *radii, const double *indices, int nlayers,
+                   int nspheres, double n_m, double wavelength, int nmax_cap,
+                   double *ab, double *dab, int *nmax, int *status,
+                   void *stream);
+
+/*
+ * Scattered field of nitems independent particle lists at npts shared
+ * coordinates.  Replaces LorenzMie.field / scattered_field / lorenzmie
+ * (theory/LorenzMie.py:135-342) and TorchLorenzMieBatch.batch_field
+ * (theory/torchLorenzMieBatch.py:285-373).
+ *   coords      [3][npts] FP64 (x row, y row, z row)
+ *   spheres     [nparticles] positions; ab/nmax as from lmb_sphere_ab
+ *               (or lmb_layered_ab) for the same particles
+ *   item_start  [nitems+1] host int array: particles of item i are
+ *               item_start[i] .. item_start[i+1]-1 (CSR)
+ *   k           wave number in the medium, rad/pixel (Instrument.wavenumber)
+ *   out         [nitems][3][npts] complex64 (FP32) or complex128 (LMB_FP64)
+ */
+int lmb_field(const double *coords, long long npts, const lmb_sphere *spheres,
+              const int *item_start, int nitems, const double *ab,
+              const int *nmax, int nmax_cap, double k, int flags, void *out,
+              void *stream);
+
+/*
+ * Holograms |E + x|^2 of nitems particle lists; same inputs as lmb_field.
+ * Replaces LorenzMie.hologram (theory/LorenzMie.py:113-133) and
+ * TorchLorenzMieBatch.batch_hologram (theory/torchLorenzMieBatch.py:258-283).
+ *   out [nitems][npts] float32 (FP32) or float64 (LMB_FP64)
+ */
+int lmb_hologram(const double *coords, long long npts,
+                 const lmb_sphere *spheres, const int *item_start, int nitems,
+                 const double *ab, const int *nmax, int nmax_cap, double k,
+                 int flags, void *out, void *stream);
+
+/*
+ * Hologram and its Jacobian for nitems single-sphere items, FP32 sums,
+ * Cartesian field (LMB_BOHREN honoured).  Fills the analytic-Jacobian
+ * slot of the reference: jaxLorenzMie.jac / jac_params
+ * (theory/jaxLorenzMie.py:321, 354-395) used by Optimizer._analytical_jac
+ * (analysis/Optimizer.py:218-220, 251-255); covers k_p as well.
+ *   spheres [nitems]; ab/dab/nmax from lmb_sphere_ab with dab != NULL
+ *   holo    [nitems][npts] float64 (may be NULL)
+ *   jac     [nitems][6][npts] float64: dH/d(x_p, y_p, z_p, a_p, n_p, k_p)
+ */
+int lmb_jacobian(const double *coords, long long npts,
+                 const lmb_sphere *spheres, int nitems, const double *ab,
+                 const double *dab, const int *nmax, int nmax_cap, double k,
+                 int flags, double *holo, double *jac, void *stream);
+
+/*
+ * Vector-Jacobian product of the hologram: grad[i][j] =
+ * sum_p gout[i][p] dH_i[p]/d param_j for single-sphere items, without
+ * forming the Jacobian (the backward pass of an autograd function).
+ * Uses caller-provided scratch of lmb_vjp_workspace_bytes(...) bytes.
+ *   gout [nitems][npts] float32; grad [nitems][6] float64
+ */
+size_t lmb_vjp_workspace_bytes(long long npts, int nitems);
+int lmb_hologram_vjp(const double *coords, long long npts,
+                     const lmb_sphere *spheres, int nitems, const double *ab,
+                     const double *dab, const int *nmax, int nmax_cap,
+                     double k, int flags, const float *gout, double *grad,
+                     void *workspace, size_t workspace_bytes, void *stream);
+
+/*
+ * A feature to fit: a crop of a normalized hologram.  Pixels are either a
+ * regular grid (nx > 0: pixel i sits at x = x0 + i % nx, y = y0 + i / nx,
+ * npix = nx*ny, as Hologram.flat_coordinates, analysis/Hologram.py:69-77)
+ * or an explicit list (nx == 0: npix pixels with coordinates in coords).
+ * data_offset indexes the packed data (and coords) arrays.
+ */
+typedef struct lmb_feature {
+  double x0, y0;
+  int nx, ny;
+  long long npix;
+  long long data_offset;
+} lmb_feature;
+
+/* Fit settings; defaults of Optimizer.settings (analysis/Optimizer.py:102-113). */
+typedef struct lmb_fit_settings {
+  double ftol, xtol, gtol, factor;
+  int max_nfev;
+  int variables;   /* bit j set = parameter j of (x_p,y_p,z_p,a_p,n_p,k_p) free */
+  int flags;       /* LMB_BOHREN */
+  int max_iterations; /* hard cap on evaluations per call, >= 1 */
+} lmb_fit_settings;
+
+/* Per-feature fit result (Optimizer.result, analysis/Optimizer.py:166-186). */
+typedef struct lmb_fit_result {
+  double dparams[6];  /* uncertainty of each free parameter (0 when fixed) */
+  double redchi;
+  double cost;        /* 0.5 * sum of squared residuals */
+  int status;         /* scipy least_squares status: 1..4 success, 0 max_nfev,
+                         <0 failure (-1 improper input, -2 non-finite
+                         residuals, -3 nmax above cap) */
+  int success;
+  int nfev, njev;
+} lmb_fit_result;
+
+/* Scratch bytes lmb_fit_batch needs for these sizes. */
+size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
+                               int nmax_cap);
+
+/*
+ * Batched Levenberg-Marquardt fit of one sphere per feature, entirely on
+ * the device.  Replaces Optimizer.optimize (analysis/Optimizer.py:196-222)
+ * with its scipy least_squares(method='lm') loop, residuals
+ * (H - data)/noise (:257-260) and _statistics (:262-278); one call fits
+ * every feature (the reference loops over features in Frame.optimize,
+ * analysis/Frame.py:163-174).
+ *   features [nfeatures]
+ *   data     packed float32 normalized intensities
+ *   coords   packed float32 (x, y) pairs for explicit-pixel features, or NULL
+ *   params   [nfeatures] in: start values, out: fitted values
+ *   results  [nfeatures]
+ *   workspace / workspace_bytes: scratch of lmb_fit_workspace_bytes(...)
+ * The call returns once every feature has terminated (or
+ * max_iterations evaluations have run); it synchronizes the stream.
+ */
+int lmb_fit_batch(const lmb_feature *features, int nfeatures,
+                  long long total_pixels, const float *data,
+                  const float *coords, lmb_sphere *params, double n_m,
+                  double wavelength, double magnification, double noise,
+                  int nmax_cap, const lmb_fit_settings *settings,
+                  lmb_fit_result *results, void *workspace,
+                  size_t workspace_bytes, void *stream);
+
+/*
+ * Measured FP32 fused-multiply-add throughput of the current device in
+ * FLOP/s (2 per FMA), for roofline reporting.  Runs a short kernel.
+ */
+int lmb_measure_fp32_peak(double *flops, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LMB200_H */

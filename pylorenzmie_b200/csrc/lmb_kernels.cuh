@@ -1,0 +1,625 @@
+// Device kernels of lmb200 (sm_100a).  Included by lmb200.cu only.
+//
+// Data layout in HBM (all row-major, struct-of-arrays where it is read by
+// pixel):
+//   coordinates        [3][npts] FP64
+//   ab                 [nparticles][nmax_cap+1][2] complex128 (a_n, b_n)
+//   dab                [nparticles][nmax_cap+1][4] complex128
+//   field / hologram   [items][3][npts] complex, [items][npts] real
+//   fit data           packed float32 crops, one contiguous run per feature
+//   fit tiles          int2 (feature, first pixel); partial sums [tile][28]
+// The per-order coefficients of the particle being summed are staged once
+// per CTA into shared memory as FP32 (or FP64) records with the order
+// prefactor folded in; every pixel of the CTA reads them as broadcasts.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lmb200.h"
+#include "lmb_lm.cuh"
+#include "lmb_mie.cuh"
+#include "lmb_pixel.cuh"
+
+namespace lmb {
+
+// ---------------------------------------------------------------------------
+// Mie coefficients: one warp per sphere.
+
+struct AbScratch {
+  zd *d1in, *d1inz, *zeta, *zetax;
+  double *d1m, *d1mx, *psi, *psix;
+};
+
+__host__ __device__ inline size_t ab_scratch_bytes(int nmaxp) {
+  return size_t(nmaxp) * (4 * sizeof(zd) + 4 * sizeof(double));
+}
+
+__device__ inline AbScratch carve_ab_scratch(char* base, int nmaxp) {
+  AbScratch s;
+  s.d1in = reinterpret_cast<zd*>(base);
+  s.d1inz = s.d1in + nmaxp;
+  s.zeta = s.d1inz + nmaxp;
+  s.zetax = s.zeta + nmaxp;
+  s.d1m = reinterpret_cast<double*>(s.zetax + nmaxp);
+  s.d1mx = s.d1m + nmaxp;
+  s.psi = s.d1mx + nmaxp;
+  s.psix = s.psi + nmaxp;
+  return s;
+}
+
+// Called by all 32 lanes of a warp.  ab: [nmaxp][2] zd, dab: [nmaxp][4] zd
+// (may be null).  Returns the status (uniform over the warp).
+__device__ int warp_sphere_ab(double a_p, double n_p, double k_p, double n_m,
+                              double wavelength, int nmax_cap, AbScratch w,
+                              zd* ab, zd* dab, int* nmax_out) {
+  const int lane = threadIdx.x & 31;
+  const int nmaxp = nmax_cap + 1;
+  const MieScalars s = mie_setup(a_p, n_p, k_p, n_m, wavelength);
+  const bool ok = (s.x > 0.) && (s.x < 1e7) && s.nmax >= 1 &&
+                  s.nmax <= nmax_cap && isfinite(s.m.re) && isfinite(s.m.im);
+  if (!ok) {
+    for (int n = lane; n < nmaxp; n += 32) {
+      ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
+      if (dab)
+        for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
+    }
+    if (lane == 0) *nmax_out = (s.nmax >= 0 && s.nmax < (1 << 30)) ? s.nmax : 0;
+    return LMB_ERR_NMAX;
+  }
+  if (lane == 0) mie_d1_inside(s, w.d1in, w.d1inz);
+  if (lane == 1) mie_d1_medium(s, w.d1m, w.d1mx);
+  __syncwarp();
+  if (lane == 0) mie_upward(s, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+  __syncwarp();
+  for (int n = lane; n < nmaxp; n += 32) {
+    if (n == 0 || n > s.nmax) {
+      ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
+      if (dab)
+        for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
+      continue;
+    }
+    zd out[2], dout[4];
+    mie_coefficient(s, n, w.d1in, w.d1inz, w.psi, w.psix, w.zeta, w.zetax, out,
+                    dab ? dout : (zd*)0);
+    ab[2 * n] = out[0];
+    ab[2 * n + 1] = out[1];
+    if (dab)
+      for (int j = 0; j < 4; ++j) dab[4 * n + j] = dout[j];
+  }
+  if (lane == 0) *nmax_out = s.nmax;
+  __syncwarp();
+  return LMB_OK;
+}
+
+__global__ void k_sphere_ab(const lmb_sphere* spheres, int n, double n_m,
+                            double wavelength, int nmax_cap, zd* ab, zd* dab,
+                            int* nmax, int* status) {
+  extern __shared__ __align__(16) char smem[];
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const int nmaxp = nmax_cap + 1;
+  AbScratch w = carve_ab_scratch(smem, nmaxp);
+  const lmb_sphere sp = spheres[i];
+  const int st = warp_sphere_ab(sp.a_p, sp.n_p, sp.k_p, n_m, wavelength,
+                                nmax_cap, w, ab + size_t(i) * nmaxp * 2,
+                                dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
+                                nmax + i);
+  if (threadIdx.x == 0) status[i] = st;
+}
+
+// ---------------------------------------------------------------------------
+// Staging of per-order records (see lmb_pixel.cuh, struct Quad).
+
+__device__ inline zd rot_i(zd z, int k) {  // z * i^k
+  switch (k & 3) {
+    case 0: return z;
+    case 1: return mk(-z.im, z.re);
+    case 2: return mk(-z.re, -z.im);
+    default: return mk(z.im, -z.re);
+  }
+}
+
+template <typename R, bool kJac>
+__device__ void stage_coef(const zd* ab, const zd* dab, int nmax,
+                           Quad<R>* sm) {
+  constexpr int W = kJac ? 4 : 2;
+  for (int n = threadIdx.x; n <= nmax; n += blockDim.x) {
+    Quad<R> q[4];
+    if (n == 0) {
+      for (int j = 0; j < W; ++j) q[j].x = q[j].y = q[j].z = q[j].w = R(0);
+    } else {
+      const double fn = double(n);
+      const double nn1 = fn * (fn + 1.);
+      const double en = (2. * fn + 1.) / nn1;
+      // alpha = i E_n a_n = en i^{n+1} a_n, beta = E_n b_n = en i^n b_n
+      const zd al = en * rot_i(ab[2 * n], n + 1);
+      const zd be = en * rot_i(ab[2 * n + 1], n);
+      q[0].x = R(al.re); q[0].y = R(al.im); q[0].z = R(be.re); q[0].w = R(be.im);
+      q[1].x = R(nn1 * al.re); q[1].y = R(nn1 * al.im);
+      q[1].z = R(1. + 1. / fn); q[1].w = R(fn);
+      if (kJac) {
+        const zd ala = en * rot_i(dab[4 * n + 0], n + 1);
+        const zd bea = en * rot_i(dab[4 * n + 1], n);
+        const zd aln = en * rot_i(dab[4 * n + 2], n + 1);
+        const zd ben = en * rot_i(dab[4 * n + 3], n);
+        q[2].x = R(ala.re); q[2].y = R(ala.im); q[2].z = R(bea.re); q[2].w = R(bea.im);
+        q[3].x = R(aln.re); q[3].y = R(aln.im); q[3].z = R(ben.re); q[3].w = R(ben.im);
+      }
+    }
+    for (int j = 0; j < W; ++j) sm[W * n + j] = q[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Field / hologram at explicit coordinates, many items, many particles.
+
+template <typename R>
+struct FieldOut;
+template <>
+struct FieldOut<float> {
+  typedef float2 C;
+};
+template <>
+struct FieldOut<double> {
+  typedef double2 C;
+};
+
+template <typename R, bool kHologram>
+__global__ void __launch_bounds__(256)
+k_field(const double* __restrict__ coords, long long npts,
+        const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
+        const zd* __restrict__ ab, const int* __restrict__ nmax, int nmaxp, double k,
+        int flags, void* out) {
+  extern __shared__ __align__(16) char smem[];
+  Quad<R>* coef = reinterpret_cast<Quad<R>*>(smem);
+  const int item = blockIdx.y;
+  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = pix < npts;
+  const bool cart = flags & LMB_CARTESIAN;
+  const bool bohren = flags & LMB_BOHREN;
+  double x = 0., y = 0., z = 0.;
+  if (live) {
+    x = coords[pix];
+    y = coords[npts + pix];
+    z = coords[2 * npts + pix];
+  }
+  cplx<R> e[3];
+  for (int c = 0; c < 3; ++c) e[c] = mk(R(0), R(0));
+  const int pb = item_start[item], pe = item_start[item + 1];
+  for (int p = pb; p < pe; ++p) {
+    const int nm = min(max(nmax[p], 0), nmaxp - 1);
+    __syncthreads();
+    stage_coef<R, false>(ab + size_t(p) * nmaxp * 2, (const zd*)0, nm, coef);
+    __syncthreads();
+    if (live) {
+      const lmb_sphere sp = spheres[p];
+      const Geometry<R> g = geometry<R>(k, x - sp.x_p, y - sp.y_p, z - sp.z_p, z,
+                                        sp.z_p, bohren);
+      const Sums<R> s = order_sum<R>(g, coef, nm);
+      cplx<R> ep[3];
+      epilogue<R>(g, s, cart, ep);
+      for (int c = 0; c < 3; ++c) e[c] = e[c] + ep[c];
+    }
+  }
+  if (!live) return;
+  if (kHologram) {
+    R* o = reinterpret_cast<R*>(out) + (size_t)item * npts;
+    o[pix] = intensity<R>(e);
+  } else {
+    typedef typename FieldOut<R>::C C;
+    C* o = reinterpret_cast<C*>(out) + (size_t)item * 3 * npts;
+    for (int c = 0; c < 3; ++c) {
+      C v;
+      v.x = e[c].re;
+      v.y = e[c].im;
+      o[c * npts + pix] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hologram + 6-column Jacobian, single sphere per item.
+
+__device__ inline void holo_jac_pixel(const Geometry<float>& g,
+                                      const Quad<float>* coef, int nm, float kf,
+                                      float* H, float* dH) {
+  const JacSums<float> A = order_sum_jac<float>(g, coef, nm);
+  cplx<float> e[3], de[6][3];
+  epilogue_jac<float>(g, A, kf, e, de);
+  *H = intensity<float>(e);
+  const cplx<float> et0 = mk(e[0].re + 1.f, e[0].im);
+  for (int j = 0; j < 6; ++j)
+    dH[j] = 2.f * (et0.re * de[j][0].re + et0.im * de[j][0].im +
+                   e[1].re * de[j][1].re + e[1].im * de[j][1].im +
+                   e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+}
+
+__global__ void __launch_bounds__(128)
+k_jacobian(const double* __restrict__ coords, long long npts,
+           const lmb_sphere* __restrict__ spheres, const zd* __restrict__ ab,
+           const zd* __restrict__ dab, const int* __restrict__ nmax, int nmaxp,
+           double k, int flags, double* holo, double* jac) {
+  extern __shared__ __align__(16) char smem[];
+  Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem);
+  const int item = blockIdx.y;
+  const int nm = min(max(nmax[item], 0), nmaxp - 1);
+  stage_coef<float, true>(ab + size_t(item) * nmaxp * 2,
+                          dab + size_t(item) * nmaxp * 4, nm, coef);
+  __syncthreads();
+  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= npts) return;
+  const lmb_sphere sp = spheres[item];
+  const double x = coords[pix], y = coords[npts + pix], z = coords[2 * npts + pix];
+  const Geometry<float> g = geometry<float>(k, x - sp.x_p, y - sp.y_p, z - sp.z_p,
+                                            z, sp.z_p, flags & LMB_BOHREN);
+  float H, dH[6];
+  holo_jac_pixel(g, coef, nm, float(k), &H, dH);
+  if (holo) holo[(size_t)item * npts + pix] = H;
+  double* jo = jac + (size_t)item * 6 * npts;
+  for (int j = 0; j < 6; ++j) jo[j * npts + pix] = dH[j];
+}
+
+// ---------------------------------------------------------------------------
+// Block reduction of NV floats held by every thread; result in red[0..NV-1]
+// of thread 0's view (shared).  Fixed order: deterministic.
+
+template <int NV, int TPB>
+__device__ inline void block_reduce(float* v, float* red /* [TPB/32][NV] */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    float s = v[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    v[j] = s;
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) red[warp * NV + j] = v[j];
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    float s = 0.f;
+    for (int w = 0; w < TPB / 32; ++w) s += red[w * NV + threadIdx.x];
+    red[threadIdx.x] = s;  // safe: each thread reads then writes its own column
+  }
+  __syncthreads();
+}
+
+// VJP: per (item, block) partial sums of g * dH/dp.
+__global__ void __launch_bounds__(128)
+k_vjp(const double* __restrict__ coords, long long npts,
+      const lmb_sphere* __restrict__ spheres, const zd* __restrict__ ab,
+      const zd* __restrict__ dab, const int* __restrict__ nmax, int nmaxp, double k,
+      int flags, const float* __restrict__ gout, double* partial) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ float red[(128 / 32) * 6];
+  Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem);
+  const int item = blockIdx.y;
+  const int nm = min(max(nmax[item], 0), nmaxp - 1);
+  stage_coef<float, true>(ab + size_t(item) * nmaxp * 2,
+                          dab + size_t(item) * nmaxp * 4, nm, coef);
+  __syncthreads();
+  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (pix < npts) {
+    const lmb_sphere sp = spheres[item];
+    const double x = coords[pix], y = coords[npts + pix], z = coords[2 * npts + pix];
+    const Geometry<float> g = geometry<float>(k, x - sp.x_p, y - sp.y_p,
+                                              z - sp.z_p, z, sp.z_p,
+                                              flags & LMB_BOHREN);
+    float H, dH[6];
+    holo_jac_pixel(g, coef, nm, float(k), &H, dH);
+    const float go = gout[(size_t)item * npts + pix];
+    for (int j = 0; j < 6; ++j) acc[j] = go * dH[j];
+  }
+  block_reduce<6, 128>(acc, red);
+  if (threadIdx.x < 6)
+    partial[((size_t)item * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = red[threadIdx.x];
+}
+
+__global__ void k_vjp_reduce(const double* partial, int nblocks, int nitems,
+                             double* grad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nitems * 6) return;
+  const int item = t / 6, j = t % 6;
+  double s = 0.;
+  for (int b = 0; b < nblocks; ++b) s += partial[((size_t)item * nblocks + b) * 6 + j];
+  grad[t] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Batched Levenberg-Marquardt.
+
+enum { FIT_NSUM = 28 };  // f^2, J^T J (21), J^T f (6)
+
+struct EvalPoint {
+  double p[6];    // parameter vector under evaluation
+  int active;     // 1 while an evaluation of this feature is pending
+  int pad;
+};
+
+struct FitCtx {
+  const lmb_feature* features;
+  const float* data;
+  const float* coords;
+  lmb_sphere* params;
+  lmb_fit_result* results;
+  LMState* state;
+  EvalPoint* ev;
+  double* base;        // [nf][6] start values (fixed parameters keep them)
+  zd* ab;              // [nf][nmaxp][2]
+  zd* dab;             // [nf][nmaxp][4]
+  int* nmax;           // [nf]
+  int* tile_begin;     // [nf+1]
+  int2* tiles;         // [max_tiles]
+  double* partial;     // [max_tiles][FIT_NSUM]
+  int* counters;       // [0] tile queue, [1] running, [2] ntiles, [3] overflow
+  long long total_pixels;
+  int nf, nmax_cap, max_tiles, tile_pixels;
+  double n_m, wavelength, k, inv_noise;
+  LMSettings set;
+  int variables, flags, max_iterations;
+};
+
+__device__ inline bool feature_valid(const lmb_feature& ft, long long total) {
+  return ft.npix >= 0 && ft.data_offset >= 0 && ft.data_offset + ft.npix <= total &&
+         (ft.nx == 0 || (ft.nx > 0 && ft.ny > 0 && (long long)ft.nx * ft.ny == ft.npix));
+}
+
+// Tile table and state initialisation; one block.
+__global__ void k_fit_setup(FitCtx c) {
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < c.nf; base += blockDim.x) {
+    const int f = base + threadIdx.x;
+    int nt = 0;
+    if (f < c.nf) {
+      const lmb_feature ft = c.features[f];
+      if (feature_valid(ft, c.total_pixels))
+        nt = ft.npix > 0 ? int((ft.npix + c.tile_pixels - 1) / c.tile_pixels) : 0;
+    }
+    // inclusive scan of nt across the block (Hillis-Steele in shared memory)
+    __shared__ int sc[1024];
+    sc[threadIdx.x] = nt;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+      const int v = threadIdx.x >= o ? sc[threadIdx.x - o] : 0;
+      __syncthreads();
+      sc[threadIdx.x] += v;
+      __syncthreads();
+    }
+    if (f < c.nf) c.tile_begin[f] = carry + sc[threadIdx.x] - nt;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += sc[threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    c.tile_begin[c.nf] = carry;
+    c.counters[2] = carry > c.max_tiles ? 0 : carry;
+    c.counters[3] = carry > c.max_tiles ? 1 : 0;
+    c.counters[0] = 0;
+    c.counters[1] = 0;
+  }
+  __syncthreads();
+  const int ntiles = carry;
+  if (ntiles > c.max_tiles) return;
+  for (int f = threadIdx.x; f < c.nf; f += blockDim.x) {
+    const int tb = c.tile_begin[f];
+    const long long np = c.features[f].npix;
+    for (int t = 0; tb + t < c.tile_begin[f + 1]; ++t)
+      c.tiles[tb + t] = make_int2(f, t * c.tile_pixels);
+    LMState& s = c.state[f];
+    const lmb_sphere p0 = c.params[f];
+    const double pv[6] = {p0.x_p, p0.y_p, p0.z_p, p0.a_p, p0.n_p, p0.k_p};
+    int n = 0;
+    for (int j = 0; j < 6; ++j) {
+      c.base[f * 6 + j] = pv[j];
+      c.ev[f].p[j] = pv[j];
+      if (c.variables & (1 << j)) {
+        s.slot[n] = j;
+        s.x[n] = pv[j];
+        ++n;
+      }
+    }
+    s.n = n;
+    s.phase = LM_PHASE_INIT;
+    s.info = 0;
+    s.iter = s.nfev = s.njev = 0;
+    s.f2_final = 0.;
+    c.ev[f].active = 0;
+    if (n == 0 || np < n || !feature_valid(c.features[f], c.total_pixels)) {
+      // MINPACK's improper input (m < n), or a feature outside the data
+      s.phase = LM_PHASE_DONE;
+      s.info = -1;
+    }
+  }
+}
+
+// Evaluation: persistent CTAs pull tiles from an atomic queue.
+template <int TPB, int PPT>
+__global__ void __launch_bounds__(TPB)
+k_fit_eval(FitCtx c) {
+  extern __shared__ __align__(16) char smem[];
+  Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem);
+  __shared__ float red[(TPB / 32) * FIT_NSUM];
+  __shared__ int s_tile;
+  const int ntiles = c.counters[2];
+  const int nmaxp = c.nmax_cap + 1;
+  const bool bohren = c.flags & LMB_BOHREN;
+  const float kf = float(c.k);
+  const float inv_noise = float(c.inv_noise);
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(c.counters, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= ntiles) break;
+    const int2 tile = c.tiles[t];
+    const int f = tile.x;
+    if (!c.ev[f].active) {
+      __syncthreads();
+      continue;
+    }
+    const int nm = min(max(c.nmax[f], 0), nmaxp - 1);
+    stage_coef<float, true>(c.ab + size_t(f) * nmaxp * 2,
+                            c.dab + size_t(f) * nmaxp * 4, nm, coef);
+    const lmb_feature ft = c.features[f];
+    const EvalPoint ep = c.ev[f];
+    __syncthreads();
+    float acc[FIT_NSUM];
+#pragma unroll
+    for (int j = 0; j < FIT_NSUM; ++j) acc[j] = 0.f;
+    for (int q = 0; q < PPT; ++q) {
+      const long long i = (long long)tile.y + q * TPB + threadIdx.x;
+      if (i >= ft.npix || i >= (long long)tile.y + c.tile_pixels) break;
+      double x, y;
+      if (ft.nx > 0) {
+        const long long row = i / ft.nx;
+        x = ft.x0 + double(i - row * ft.nx);
+        y = ft.y0 + double(row);
+      } else {
+        const float2 xy = reinterpret_cast<const float2*>(c.coords)[ft.data_offset + i];
+        x = xy.x;
+        y = xy.y;
+      }
+      const float d = c.data[ft.data_offset + i];
+      const Geometry<float> g = geometry<float>(c.k, x - ep.p[0], y - ep.p[1],
+                                                -ep.p[2], 0., ep.p[2], bohren);
+      float H, dH[6];
+      holo_jac_pixel(g, coef, nm, kf, &H, dH);
+      const float r = (H - d) * inv_noise;
+      float J[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) J[j] = dH[j] * inv_noise;
+      acc[0] += r * r;
+      int o = 1;
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = a; b < 6; ++b) acc[o++] += J[a] * J[b];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) acc[22 + a] += J[a] * r;
+    }
+    block_reduce<FIT_NSUM, TPB>(acc, red);
+    if (threadIdx.x < FIT_NSUM)
+      c.partial[(size_t)t * FIT_NSUM + threadIdx.x] = red[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+// One warp per feature: gather sums, advance the LM state machine, and
+// compute the Mie coefficients of the next evaluation point.
+__global__ void __launch_bounds__(32)
+k_fit_step(FitCtx c) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ double s_p[6];
+  __shared__ int s_need;
+  const int f = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (f >= c.nf) return;
+  if (c.counters[3]) return;  // tile table overflow: nothing ran
+  LMState* gs = c.state + f;
+  const int phase = gs->phase;
+  if (phase == LM_PHASE_DONE) return;
+  const int nmaxp = c.nmax_cap + 1;
+  if (lane == 0) {
+    s_need = 0;
+    if (phase == LM_PHASE_INIT) {
+      for (int j = 0; j < 6; ++j) s_p[j] = c.base[f * 6 + j];
+      s_need = 1;
+    }
+  }
+  if (phase == LM_PHASE_FIRST || phase == LM_PHASE_TRIAL) {
+    double v[FIT_NSUM];
+    for (int j = 0; j < FIT_NSUM; ++j) v[j] = 0.;
+    const int tb = c.tile_begin[f], te = c.tile_begin[f + 1];
+    for (int t = tb + lane; t < te; t += 32)
+      for (int j = 0; j < FIT_NSUM; ++j) v[j] += c.partial[(size_t)t * FIT_NSUM + j];
+    for (int j = 0; j < FIT_NSUM; ++j)
+      for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+    if (lane == 0) {
+      LMEval ev;
+      ev.f2 = v[0];
+      for (int j = 0; j < 21; ++j) ev.jtj[j] = v[1 + j];
+      for (int j = 0; j < 6; ++j) ev.jtf[j] = v[22 + j];
+      LMState s = *gs;
+      const int done = phase == LM_PHASE_FIRST ? lm_start(s, ev, c.set)
+                                               : lm_after_trial(s, ev, c.set);
+      if (done || s.nfev >= c.max_iterations) {
+        if (!done && s.info == 0) s.info = 5;  // evaluation cap reached
+        s.phase = LM_PHASE_DONE;
+        c.ev[f].active = 0;
+      } else {
+        s.phase = LM_PHASE_TRIAL;
+        for (int j = 0; j < 6; ++j) s_p[j] = c.base[f * 6 + j];
+        for (int a = 0; a < s.n; ++a) s_p[s.slot[a]] = s.x[a] + s.p[a];
+        s_need = 1;
+      }
+      *gs = s;
+    }
+  }
+  __syncwarp();
+  if (!s_need) return;
+  AbScratch w = carve_ab_scratch(smem, nmaxp);
+  const int st = warp_sphere_ab(s_p[3], s_p[4], s_p[5], c.n_m, c.wavelength,
+                                c.nmax_cap, w, c.ab + size_t(f) * nmaxp * 2,
+                                c.dab + size_t(f) * nmaxp * 4, c.nmax + f);
+  if (lane == 0) {
+    if (st != LMB_OK) {
+      gs->phase = LM_PHASE_DONE;
+      gs->info = -3;
+      c.ev[f].active = 0;
+    } else {
+      if (phase == LM_PHASE_INIT) gs->phase = LM_PHASE_FIRST;
+      for (int j = 0; j < 6; ++j) c.ev[f].p[j] = s_p[j];
+      c.ev[f].active = 1;
+      atomicAdd(c.counters + 1, 1);
+    }
+  }
+}
+
+// Results: fitted parameters, uncertainties, redchi; one thread per feature.
+__global__ void k_fit_finalize(FitCtx c) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= c.nf) return;
+  const LMState s = c.state[f];
+  lmb_fit_result r;
+  for (int j = 0; j < 6; ++j) r.dparams[j] = 0.;
+  double pv[6];
+  for (int j = 0; j < 6; ++j) pv[j] = c.base[f * 6 + j];
+  const long long npix = c.features[f].npix;
+  if (c.counters[3]) {
+    r.status = -1;
+    r.success = 0;
+    r.redchi = 0.;
+    r.cost = 0.;
+    r.nfev = r.njev = 0;
+  } else {
+    int info = s.info;
+    if (s.phase != LM_PHASE_DONE && info == 0) info = 5;
+    r.status = lm_scipy_status(info);
+    r.success = r.status > 0;
+    r.nfev = s.nfev;
+    r.njev = s.njev;
+    r.cost = 0.5 * s.f2_final;
+    r.redchi = 0.;
+    if (info > 0 && s.n > 0) {
+      for (int a = 0; a < s.n; ++a) pv[s.slot[a]] = s.x[a];
+      double dp[LM_NV];
+      lm_statistics(s, npix, &r.redchi, dp);
+      for (int a = 0; a < s.n; ++a) r.dparams[s.slot[a]] = dp[a];
+    }
+  }
+  lmb_sphere out;
+  out.x_p = pv[0];
+  out.y_p = pv[1];
+  out.z_p = pv[2];
+  out.a_p = pv[3];
+  out.n_p = pv[4];
+  out.k_p = pv[5];
+  c.params[f] = out;
+  c.results[f] = r;
+}
+
+}  // namespace lmb

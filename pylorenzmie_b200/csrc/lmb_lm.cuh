@@ -1,0 +1,508 @@
+// Levenberg-Marquardt step logic for one feature, in FP64.
+//
+// The reference fits with scipy.optimize.least_squares(method='lm')
+// (analysis/Optimizer.py:104-113, 221), which runs MINPACK lmder: Moré's
+// trust-region Levenberg-Marquardt (J. J. Moré, "The Levenberg-Marquardt
+// algorithm: implementation and theory", Lecture Notes in Mathematics 630
+// (1978); MINPACK-1 user guide, ANL-80-74 (1980)).  This file restates that
+// published algorithm -- the outer/inner loops of lmder, the step-bound
+// update, the convergence tests and the lmpar search for the damping
+// parameter -- for a problem with at most six unknowns, written against
+// the normal equations J^T J, J^T f instead of the QR factors of J:
+//   * qrfac with column pivoting  -> pivoted Cholesky of J^T J (R^T R = P^T J^T J P,
+//                                    the same pivot rule: largest remaining
+//                                    column norm = largest Schur diagonal);
+//   * Q^T f (first n)              -> R^{-T} P^T J^T f;
+//   * qrsolv                        -> Cholesky of R^T R + P^T D^2 P;
+//   * ||R P^T p||                   -> sqrt(p^T R^T R p) in pivoted order.
+// These give the same iterates in exact arithmetic.  The per-pixel sums
+// J^T J, J^T f and f^T f come from the evaluation kernel.
+//
+// Settings follow scipy's call of lmder (scipy/optimize/_lsq/least_squares.py,
+// call_minpack): factor = 100, mode 1 (x_scale='jac': diag from the column
+// norms of J, never decreasing), maxfev = max_nfev.
+#pragma once
+
+#include "lmb_math.cuh"
+
+namespace lmb {
+
+enum { LM_NV = 6 };  // x_p, y_p, z_p, a_p, n_p, k_p
+
+// Packed upper-triangular index of (i, j), i <= j, for a 6x6 symmetric matrix.
+LMB_HD int sym6(int i, int j) {
+  if (i > j) {
+    int t = i;
+    i = j;
+    j = t;
+  }
+  return i * LM_NV - (i * (i - 1)) / 2 + (j - i);
+}
+
+struct LMSettings {
+  double ftol, xtol, gtol, factor;
+  int maxfev;
+};
+
+// Phases of the per-feature state machine.
+enum {
+  LM_PHASE_INIT = 0,       // ab of the start point not yet computed
+  LM_PHASE_FIRST = 1,      // evaluation of the start point pending
+  LM_PHASE_TRIAL = 2,      // evaluation of a trial point pending
+  LM_PHASE_DONE = 3
+};
+
+struct LMState {
+  int n;              // number of free variables
+  int slot[LM_NV];    // parameter slot (0..5) of each free variable
+  int phase, info, iter, nfev, njev, nsing;
+  double x[LM_NV];    // current free-variable values
+  double p[LM_NV];    // step under trial
+  double diag[LM_NV];
+  double acnorm[LM_NV];
+  double jtf[LM_NV];              // J^T f at x (free variables)
+  double jtj[LM_NV * LM_NV];      // J^T J at x (free variables)
+  double r[LM_NV * LM_NV];        // pivoted Cholesky factor, row-major
+  int ipvt[LM_NV];
+  double qtf[LM_NV];
+  double delta, par, fnorm, xnorm, gnorm, pnorm, prered, dirder;
+  double f2_final;
+};
+
+// Sums over the pixels of one feature for one parameter vector.
+struct LMEval {
+  double f2;
+  double jtj[21];  // packed upper over the 6 slots
+  double jtf[6];
+};
+
+LMB_HD double enorm(const double* v, int n) {
+  double s = 0.;
+  for (int i = 0; i < n; ++i) s += v[i] * v[i];
+  return sqrt(s);
+}
+
+// Extract the free-variable normal equations of an evaluation.
+LMB_HD void lm_take(LMState& s, const LMEval& ev) {
+  const int n = s.n;
+  for (int a = 0; a < n; ++a) {
+    s.jtf[a] = ev.jtf[s.slot[a]];
+    for (int b = 0; b < n; ++b) s.jtj[a * LM_NV + b] = ev.jtj[sym6(s.slot[a], s.slot[b])];
+  }
+}
+
+// Pivoted Cholesky of J^T J (the qrfac equivalent), column norms, Q^T f.
+LMB_HD void lm_factor(LMState& s) {
+  const int n = s.n;
+  double w[LM_NV * LM_NV];
+  for (int i = 0; i < n * LM_NV; ++i) w[i] = s.jtj[i];
+  for (int j = 0; j < n; ++j) {
+    s.ipvt[j] = j;
+    const double c = s.jtj[j * LM_NV + j];
+    s.acnorm[j] = sqrt(c > 0. ? c : 0.);
+  }
+  for (int i = 0; i < LM_NV * LM_NV; ++i) s.r[i] = 0.;
+  s.nsing = n;
+  for (int j = 0; j < n; ++j) {
+    int kmax = j;
+    for (int k = j + 1; k < n; ++k)
+      if (w[k * LM_NV + k] > w[kmax * LM_NV + kmax]) kmax = k;
+    if (kmax != j) {
+      for (int i = 0; i < n; ++i) {
+        double t = w[i * LM_NV + j];
+        w[i * LM_NV + j] = w[i * LM_NV + kmax];
+        w[i * LM_NV + kmax] = t;
+      }
+      for (int i = 0; i < n; ++i) {
+        double t = w[j * LM_NV + i];
+        w[j * LM_NV + i] = w[kmax * LM_NV + i];
+        w[kmax * LM_NV + i] = t;
+      }
+      for (int i = 0; i < j; ++i) {  // rows of R already formed
+        double t = s.r[i * LM_NV + j];
+        s.r[i * LM_NV + j] = s.r[i * LM_NV + kmax];
+        s.r[i * LM_NV + kmax] = t;
+      }
+      int t = s.ipvt[j];
+      s.ipvt[j] = s.ipvt[kmax];
+      s.ipvt[kmax] = t;
+    }
+    const double d = w[j * LM_NV + j];
+    if (!(d > 0.)) {
+      s.nsing = j;
+      break;
+    }
+    const double rjj = sqrt(d);
+    s.r[j * LM_NV + j] = rjj;
+    for (int k = j + 1; k < n; ++k) s.r[j * LM_NV + k] = w[j * LM_NV + k] / rjj;
+    for (int i = j + 1; i < n; ++i)
+      for (int k = j + 1; k < n; ++k)
+        w[i * LM_NV + k] -= s.r[j * LM_NV + i] * s.r[j * LM_NV + k];
+  }
+  // R^T qtf = P^T J^T f on the nonsingular block; zero beyond it
+  for (int j = 0; j < n; ++j) {
+    if (j >= s.nsing) {
+      s.qtf[j] = 0.;
+      continue;
+    }
+    double sum = s.jtf[s.ipvt[j]];
+    for (int i = 0; i < j; ++i) sum -= s.r[i * LM_NV + j] * s.qtf[i];
+    s.qtf[j] = sum / s.r[j * LM_NV + j];
+  }
+}
+
+// qrsolv equivalent: S = chol(R^T R + D_p^2) (pivoted order, D_p[j] =
+// dg[ipvt[j]]), solve S^T S z = R^T qtb, x[ipvt[j]] = z[j].
+LMB_HD void lm_qrsolv(const LMState& s, const double* dg, double* x,
+                      double* sm, double* sdiag) {
+  const int n = s.n;
+  double m[LM_NV * LM_NV];
+  for (int i = 0; i < n; ++i)
+    for (int j = i; j < n; ++j) {
+      double sum = 0.;
+      for (int k = 0; k <= i; ++k) sum += s.r[k * LM_NV + i] * s.r[k * LM_NV + j];
+      m[i * LM_NV + j] = sum;
+    }
+  for (int j = 0; j < n; ++j) {
+    const double d = dg[s.ipvt[j]];
+    m[j * LM_NV + j] += d * d;
+  }
+  for (int i = 0; i < LM_NV * LM_NV; ++i) sm[i] = 0.;
+  int nsing = n;
+  for (int j = 0; j < n; ++j) {
+    double d = m[j * LM_NV + j];
+    for (int k = 0; k < j; ++k) d -= sm[k * LM_NV + j] * sm[k * LM_NV + j];
+    if (!(d > 0.)) {
+      nsing = j;
+      break;
+    }
+    const double sjj = sqrt(d);
+    sm[j * LM_NV + j] = sjj;
+    for (int i = j + 1; i < n; ++i) {
+      double e = m[j * LM_NV + i];
+      for (int k = 0; k < j; ++k) e -= sm[k * LM_NV + j] * sm[k * LM_NV + i];
+      sm[j * LM_NV + i] = e / sjj;
+    }
+  }
+  for (int j = 0; j < n; ++j) sdiag[j] = j < nsing ? sm[j * LM_NV + j] : 0.;
+  // rhs = R^T qtb
+  double z[LM_NV];
+  for (int j = 0; j < n; ++j) {
+    double sum = 0.;
+    for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * s.qtf[i];
+    z[j] = sum;
+  }
+  for (int j = 0; j < n; ++j) {  // S^T y = rhs
+    if (j >= nsing) {
+      z[j] = 0.;
+      continue;
+    }
+    double sum = z[j];
+    for (int i = 0; i < j; ++i) sum -= sm[i * LM_NV + j] * z[i];
+    z[j] = sum / sm[j * LM_NV + j];
+  }
+  for (int j = nsing - 1; j >= 0; --j) {  // S z = y
+    double sum = z[j];
+    for (int i = j + 1; i < nsing; ++i) sum -= sm[j * LM_NV + i] * z[i];
+    z[j] = sum / sm[j * LM_NV + j];
+  }
+  for (int j = 0; j < n; ++j) x[s.ipvt[j]] = z[j];
+}
+
+// lmpar: damping parameter and the step x (the step is p = -x).
+LMB_HD void lm_par(LMState& s, double* x) {
+  const int n = s.n;
+  const double dwarf = 2.2250738585072014e-308;
+  const double p1 = 0.1, p001 = 0.001;
+  double wa1[LM_NV], wa2[LM_NV], sm[LM_NV * LM_NV], sdiag[LM_NV];
+  // Gauss-Newton direction
+  for (int j = 0; j < n; ++j) wa1[j] = j < s.nsing ? s.qtf[j] : 0.;
+  for (int j = s.nsing - 1; j >= 0; --j) {
+    wa1[j] /= s.r[j * LM_NV + j];
+    const double t = wa1[j];
+    for (int i = 0; i < j; ++i) wa1[i] -= s.r[i * LM_NV + j] * t;
+  }
+  for (int j = 0; j < n; ++j) x[s.ipvt[j]] = wa1[j];
+  int iter = 0;
+  for (int j = 0; j < n; ++j) wa2[j] = s.diag[j] * x[j];
+  double dxnorm = enorm(wa2, n);
+  double fp = dxnorm - s.delta;
+  if (fp <= p1 * s.delta) {
+    s.par = 0.;
+    return;
+  }
+  // lower bound
+  double parl = 0.;
+  if (s.nsing >= n) {
+    for (int j = 0; j < n; ++j) {
+      const int l = s.ipvt[j];
+      wa1[j] = s.diag[l] * (wa2[l] / dxnorm);
+    }
+    for (int j = 0; j < n; ++j) {
+      double sum = 0.;
+      for (int i = 0; i < j; ++i) sum += s.r[i * LM_NV + j] * wa1[i];
+      wa1[j] = (wa1[j] - sum) / s.r[j * LM_NV + j];
+    }
+    const double t = enorm(wa1, n);
+    parl = ((fp / s.delta) / t) / t;
+  }
+  // upper bound
+  for (int j = 0; j < n; ++j) {
+    double sum = 0.;
+    for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * s.qtf[i];
+    wa1[j] = sum / s.diag[s.ipvt[j]];
+  }
+  const double gnorm = enorm(wa1, n);
+  double paru = gnorm / s.delta;
+  if (paru == 0.) paru = dwarf / (s.delta < p1 ? s.delta : p1);
+  double par = s.par;
+  if (par < parl) par = parl;
+  if (par > paru) par = paru;
+  if (par == 0.) par = gnorm / dxnorm;
+  for (;;) {
+    ++iter;
+    if (par == 0.) par = dwarf > p001 * paru ? dwarf : p001 * paru;
+    const double t = sqrt(par);
+    double dg[LM_NV];
+    for (int j = 0; j < n; ++j) dg[j] = t * s.diag[j];
+    lm_qrsolv(s, dg, x, sm, sdiag);
+    for (int j = 0; j < n; ++j) wa2[j] = s.diag[j] * x[j];
+    dxnorm = enorm(wa2, n);
+    const double temp = fp;
+    fp = dxnorm - s.delta;
+    if (fabs(fp) <= p1 * s.delta || (parl == 0. && fp <= temp && temp < 0.) ||
+        iter == 10)
+      break;
+    // Newton correction: solve S^T w = D P^T x / ||D x||
+    for (int j = 0; j < n; ++j) {
+      const int l = s.ipvt[j];
+      wa1[j] = s.diag[l] * (wa2[l] / dxnorm);
+    }
+    for (int j = 0; j < n; ++j) {
+      wa1[j] /= sdiag[j];
+      const double tj = wa1[j];
+      for (int i = j + 1; i < n; ++i) wa1[i] -= sm[j * LM_NV + i] * tj;
+    }
+    const double tn = enorm(wa1, n);
+    const double parc = ((fp / s.delta) / tn) / tn;
+    if (fp > 0.) parl = parl > par ? parl : par;
+    if (fp < 0.) paru = paru < par ? paru : par;
+    par = parl > par + parc ? parl : par + parc;
+  }
+  s.par = par;
+}
+
+// Inner loop head: choose the next trial step.  Writes s.p.
+LMB_HD void lm_trial(LMState& s) {
+  const int n = s.n;
+  double x[LM_NV];
+  lm_par(s, x);
+  double wa3[LM_NV];
+  for (int j = 0; j < n; ++j) {
+    s.p[j] = -x[j];
+    wa3[j] = s.diag[j] * s.p[j];
+  }
+  s.pnorm = enorm(wa3, n);
+  if (s.iter == 1 && s.pnorm < s.delta) s.delta = s.pnorm;
+  // predicted reduction from ||R P^T p||
+  for (int j = 0; j < n; ++j) wa3[j] = 0.;
+  for (int j = 0; j < n; ++j) {
+    const double t = s.p[s.ipvt[j]];
+    for (int i = 0; i <= j; ++i) wa3[i] += s.r[i * LM_NV + j] * t;
+  }
+  const double temp1 = enorm(wa3, n) / s.fnorm;
+  const double temp2 = (sqrt(s.par) * s.pnorm) / s.fnorm;
+  s.prered = temp1 * temp1 + temp2 * temp2 / 0.5;
+  s.dirder = -(temp1 * temp1 + temp2 * temp2);
+}
+
+// Outer loop body after a new Jacobian at x: scaling, gradient test, trial.
+// Returns nonzero when the fit has terminated.
+LMB_HD int lm_outer(LMState& s, const LMSettings& set) {
+  const int n = s.n;
+  s.njev += 1;
+  lm_factor(s);
+  if (s.iter == 1) {
+    for (int j = 0; j < n; ++j) s.diag[j] = s.acnorm[j] == 0. ? 1. : s.acnorm[j];
+    double wa3[LM_NV];
+    for (int j = 0; j < n; ++j) wa3[j] = s.diag[j] * s.x[j];
+    s.xnorm = enorm(wa3, n);
+    s.delta = set.factor * s.xnorm;
+    if (s.delta == 0.) s.delta = set.factor;
+  }
+  s.gnorm = 0.;
+  if (s.fnorm != 0.) {
+    for (int j = 0; j < n; ++j) {
+      const int l = s.ipvt[j];
+      if (s.acnorm[l] == 0.) continue;
+      double sum = 0.;
+      for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * (s.qtf[i] / s.fnorm);
+      const double g = fabs(sum / s.acnorm[l]);
+      if (g > s.gnorm) s.gnorm = g;
+    }
+  }
+  if (s.gnorm <= set.gtol) {
+    s.info = 4;
+    return 1;
+  }
+  for (int j = 0; j < n; ++j)
+    if (s.acnorm[j] > s.diag[j]) s.diag[j] = s.acnorm[j];
+  lm_trial(s);
+  return 0;
+}
+
+// First evaluation (start point with its Jacobian).  Returns nonzero when
+// the fit has terminated.
+LMB_HD int lm_start(LMState& s, const LMEval& ev, const LMSettings& set) {
+  s.nfev = 1;
+  s.njev = 0;
+  s.info = 0;
+  s.f2_final = ev.f2;
+  if (!(ev.f2 <= 1.7976931348623157e308)) {  // non-finite residuals
+    s.info = -2;
+    return 1;
+  }
+  s.fnorm = sqrt(ev.f2);
+  s.par = 0.;
+  s.iter = 1;
+  lm_take(s, ev);
+  return lm_outer(s, set);
+}
+
+// Evaluation of the trial point x + p (value and Jacobian there).
+// Returns nonzero when the fit has terminated.
+LMB_HD int lm_after_trial(LMState& s, const LMEval& ev, const LMSettings& set) {
+  const int n = s.n;
+  const double epsmch = 2.220446049250313e-16;
+  s.nfev += 1;
+  const double fnorm1 = sqrt(ev.f2);
+  double actred = -1.;
+  if (0.1 * fnorm1 < s.fnorm) actred = 1. - (fnorm1 / s.fnorm) * (fnorm1 / s.fnorm);
+  double ratio = 0.;
+  if (s.prered != 0.) ratio = actred / s.prered;
+  if (ratio <= 0.25) {
+    double temp;
+    if (actred >= 0.)
+      temp = 0.5;
+    else
+      temp = 0.5 * s.dirder / (s.dirder + 0.5 * actred);
+    if (0.1 * fnorm1 >= s.fnorm || temp < 0.1) temp = 0.1;
+    const double pn = s.pnorm / 0.1;
+    s.delta = temp * (s.delta < pn ? s.delta : pn);
+    s.par = s.par / temp;
+  } else if (s.par == 0. || ratio >= 0.75) {
+    s.delta = s.pnorm / 0.5;
+    s.par = 0.5 * s.par;
+  }
+  const bool success = ratio >= 1e-4;
+  if (success) {
+    double wa2[LM_NV];
+    for (int j = 0; j < n; ++j) {
+      s.x[j] = s.x[j] + s.p[j];
+      wa2[j] = s.diag[j] * s.x[j];
+    }
+    s.xnorm = enorm(wa2, n);
+    s.fnorm = fnorm1;
+    s.f2_final = ev.f2;
+    s.iter += 1;
+    lm_take(s, ev);
+  }
+  const bool fconv = fabs(actred) <= set.ftol && s.prered <= set.ftol && 0.5 * ratio <= 1.;
+  if (fconv) s.info = 1;
+  if (s.delta <= set.xtol * s.xnorm) s.info = fconv ? 3 : 2;
+  if (s.info != 0) return 1;
+  if (s.nfev >= set.maxfev) s.info = 5;
+  if (fabs(actred) <= epsmch && s.prered <= epsmch && 0.5 * ratio <= 1.) s.info = 6;
+  if (s.delta <= epsmch * s.xnorm) s.info = 7;
+  if (s.gnorm <= epsmch) s.info = 8;
+  if (s.info != 0) return 1;
+  if (success) return lm_outer(s, set);
+  lm_trial(s);
+  return 0;
+}
+
+// scipy's status for a MINPACK info (FROM_MINPACK_TO_COMMON); the stringent
+// tolerance exits 6/7/8 are reported as the ftol/xtol/gtol successes they
+// refine.  Negative values are this library's own failures.
+LMB_HD int lm_scipy_status(int info) {
+  switch (info) {
+    case 1: return 2;
+    case 2: return 3;
+    case 3: return 4;
+    case 4: return 1;
+    case 5: return 0;
+    case 6: return 2;
+    case 7: return 3;
+    case 8: return 1;
+    default: return info < 0 ? info : -1;
+  }
+}
+
+// Symmetric eigen-decomposition by cyclic Jacobi rotations (n <= 6).
+// a is overwritten; w gets eigenvalues, v (row-major) eigenvectors in columns.
+LMB_HD void jacobi_eigh(double* a, int n, double* w, double* v) {
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) v[i * LM_NV + j] = i == j ? 1. : 0.;
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    double off = 0., tot = 0.;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const double t = a[i * LM_NV + j] * a[i * LM_NV + j];
+        tot += t;
+        if (i != j) off += t;
+      }
+    if (off <= 1e-30 * tot || off == 0.) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[p * LM_NV + q];
+        if (apq == 0.) continue;
+        const double app = a[p * LM_NV + p], aqq = a[q * LM_NV + q];
+        const double theta = (aqq - app) / (2. * apq);
+        const double t = (theta >= 0. ? 1. : -1.) /
+                         (fabs(theta) + sqrt(theta * theta + 1.));
+        const double c = 1. / sqrt(t * t + 1.), sn = t * c;
+        for (int k = 0; k < n; ++k) {
+          const double akp = a[k * LM_NV + p], akq = a[k * LM_NV + q];
+          a[k * LM_NV + p] = c * akp - sn * akq;
+          a[k * LM_NV + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = a[p * LM_NV + k], aqk = a[q * LM_NV + k];
+          a[p * LM_NV + k] = c * apk - sn * aqk;
+          a[q * LM_NV + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = v[k * LM_NV + p], vkq = v[k * LM_NV + q];
+          v[k * LM_NV + p] = c * vkp - sn * vkq;
+          v[k * LM_NV + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < n; ++i) w[i] = a[i * LM_NV + i];
+}
+
+// redchi and uncertainties of Optimizer._statistics (analysis/Optimizer.py:
+// 262-278): pcov = pinv(J^T J) keeping singular values of J above
+// eps * max(npix, n) * s_max; d = sqrt(redchi * diag(pcov)).
+LMB_HD void lm_statistics(const LMState& s, long long npix, double* redchi,
+                          double* dp) {
+  const int n = s.n;
+  const double ndeg = double(npix - n);
+  *redchi = s.f2_final / ndeg;
+  double a[LM_NV * LM_NV], v[LM_NV * LM_NV], w[LM_NV];
+  for (int i = 0; i < LM_NV * LM_NV; ++i) a[i] = s.jtj[i];
+  jacobi_eigh(a, n, w, v);
+  double wmax = 0.;
+  for (int i = 0; i < n; ++i) if (w[i] > wmax) wmax = w[i];
+  const double big = double(npix > n ? npix : n);
+  const double thr = 2.220446049250313e-16 * big;
+  const double thr2 = thr * thr * wmax;
+  for (int i = 0; i < n; ++i) {
+    double c = 0.;
+    for (int k = 0; k < n; ++k)
+      if (w[k] > thr2 && w[k] > 0.) c += v[i * LM_NV + k] * v[i * LM_NV + k] / w[k];
+    dp[i] = sqrt(*redchi * c);
+  }
+}
+
+}  // namespace lmb

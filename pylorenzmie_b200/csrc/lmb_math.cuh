@@ -1,0 +1,108 @@
+// Small complex and math helpers shared by the kernels.
+//
+// Everything here is __host__ __device__ so that the same arithmetic can be
+// compiled for the CPU test harness (tests/cpu_harness), which checks the
+// kernels' own math against the FP64 oracle without a GPU.
+#pragma once
+
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define LMB_HD __host__ __device__ __forceinline__
+#else
+#define LMB_HD inline
+#endif
+
+namespace lmb {
+
+template <typename T>
+struct cplx {
+  T re, im;
+};
+
+template <typename T>
+LMB_HD cplx<T> mk(T re, T im) {
+  cplx<T> z;
+  z.re = re;
+  z.im = im;
+  return z;
+}
+template <typename T>
+LMB_HD cplx<T> operator+(cplx<T> a, cplx<T> b) { return mk(a.re + b.re, a.im + b.im); }
+template <typename T>
+LMB_HD cplx<T> operator-(cplx<T> a, cplx<T> b) { return mk(a.re - b.re, a.im - b.im); }
+template <typename T>
+LMB_HD cplx<T> operator-(cplx<T> a) { return mk(-a.re, -a.im); }
+template <typename T>
+LMB_HD cplx<T> operator*(cplx<T> a, cplx<T> b) {
+  return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+template <typename T>
+LMB_HD cplx<T> operator*(T s, cplx<T> a) { return mk(s * a.re, s * a.im); }
+template <typename T>
+LMB_HD cplx<T> operator*(cplx<T> a, T s) { return mk(s * a.re, s * a.im); }
+template <typename T>
+LMB_HD cplx<T> operator+(cplx<T> a, T s) { return mk(a.re + s, a.im); }
+template <typename T>
+LMB_HD cplx<T> operator+(T s, cplx<T> a) { return mk(a.re + s, a.im); }
+template <typename T>
+LMB_HD cplx<T> operator-(T s, cplx<T> a) { return mk(s - a.re, -a.im); }
+template <typename T>
+LMB_HD cplx<T> operator-(cplx<T> a, T s) { return mk(a.re - s, a.im); }
+template <typename T>
+LMB_HD cplx<T> conj(cplx<T> a) { return mk(a.re, -a.im); }
+// multiply by i
+template <typename T>
+LMB_HD cplx<T> mul_i(cplx<T> a) { return mk(-a.im, a.re); }
+template <typename T>
+LMB_HD T norm2(cplx<T> a) { return a.re * a.re + a.im * a.im; }
+
+// Complex division by Smith's method (R. L. Smith, CACM 5, 435 (1962)),
+// the scaling numpy applies to complex128 division.
+template <typename T>
+LMB_HD cplx<T> operator/(cplx<T> a, cplx<T> b) {
+  T ar = b.re < T(0) ? -b.re : b.re;
+  T ai = b.im < T(0) ? -b.im : b.im;
+  if (ar >= ai) {
+    T rat = b.im / b.re;
+    T scl = T(1) / (b.re + b.im * rat);
+    return mk((a.re + a.im * rat) * scl, (a.im - a.re * rat) * scl);
+  } else {
+    T rat = b.re / b.im;
+    T scl = T(1) / (b.im + b.re * rat);
+    return mk((a.re * rat + a.im) * scl, (a.im * rat - a.re) * scl);
+  }
+}
+template <typename T>
+LMB_HD cplx<T> operator/(T s, cplx<T> b) { return mk(s, T(0)) / b; }
+template <typename T>
+LMB_HD cplx<T> operator/(cplx<T> a, T s) { return mk(a.re / s, a.im / s); }
+
+// e^{i t}
+LMB_HD cplx<double> cis(double t) {
+  double s, c;
+#if defined(__CUDA_ARCH__)
+  sincos(t, &s, &c);
+#else
+  s = sin(t);
+  c = cos(t);
+#endif
+  return mk(c, s);
+}
+LMB_HD cplx<float> cis(float t) {
+  float s, c;
+#if defined(__CUDA_ARCH__)
+  sincosf(t, &s, &c);
+#else
+  s = sinf(t);
+  c = cosf(t);
+#endif
+  return mk(c, s);
+}
+
+LMB_HD float lsqrt(float x) { return sqrtf(x); }
+LMB_HD double lsqrt(double x) { return sqrt(x); }
+LMB_HD float labs_(float x) { return fabsf(x); }
+LMB_HD double labs_(double x) { return fabs(x); }
+
+}  // namespace lmb

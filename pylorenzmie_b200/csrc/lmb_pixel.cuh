@@ -1,0 +1,454 @@
+// Per-pixel Lorenz-Mie partial-wave sum, its Jacobian, and the hologram.
+//
+// Follows theory/LorenzMie.py:183-342 (LorenzMie.lorenzmie):
+//   geometry from kdr with kz flipped (:221-237); Riccati-Bessel starting
+//   values with the sign(kz) convention (:249-251); for n = 1..nmax the
+//   Wiscombe pi_n/tau_n, xi_n = (2n-1) xi_{n-1}/kr - xi_{n-2},
+//   D_n = n xi_n/kr - xi_{n-1} and the vector-spherical-harmonic sums
+//   (:272-317); geometric factors restored at the end (:322-325); Cartesian
+//   projection (:331-340); phase exp(-i k z_p) (:157-158); hologram
+//   |E + x|^2 (:131-133).
+//
+// Two reformulations keep FP32 accurate without changing the result:
+//  * xi_n = e^{i sigma kr} h_n, where h_n obeys the same real-coefficient
+//    recurrence from h_{-1} = 1, h_0 = -i sigma.  The pure phase
+//    e^{i(sigma kr - k z_p)} is applied once per pixel.  For the default
+//    convention (sigma = sign(kz)) its argument equals
+//    sign(kz) krho^2 / (kr + |kz|) - k z, which is free of the cancellation
+//    between kr and k z_p (both ~10^2 rad) that FP32 cannot resolve.
+//  * The order-n coefficients are pre-multiplied by the prefactor:
+//    alpha_n = i E_n a_n, beta_n = E_n b_n, E_n = i^n (2n+1)/(n(n+1)), and
+//    the sums are regrouped as
+//      S0 = sum pi (n(n+1) alpha h),
+//      S1 = sum tau (alpha Dh) - pi (beta h),
+//      S2 = sum pi (alpha Dh) - tau (beta h).
+//
+//  * The Wiscombe recurrence is carried in s = 1 - |cos(theta)| and
+//    Delta_n = pi_n - pi_{n-1}:
+//      tau_n = pi_{n-1} - n Delta_n + n s pi_n,
+//      Delta_{n+1} = c_n Delta_n - (1 + c_n) s pi_n,  c_n = 1 + 1/n,
+//      pi_{n+1} = pi_n + Delta_{n+1},
+//    which is the reference's swisc/twisc update with mu = 1 - s.  s is
+//    formed as krho^2 / (kr (kr + |kz|)), so the angle near the optical
+//    axis keeps its relative precision (FP32 cos(theta) near 1 does not,
+//    and pi_n is very sensitive there).  For cos(theta) < 0 the parities
+//    pi_n(-mu) = (-1)^{n-1} pi_n(mu), tau_n(-mu) = (-1)^n tau_n(mu) are
+//    folded into h_n (h~_n = (-1)^{n-1} h_n obeys the recurrence with kr
+//    negated), which leaves a sign on some of the summed components.
+//
+// The Jacobian is forward mode.  In the order loop it carries tangents in kr
+// of the phase-reduced h_n (the differentiated recurrence, which starts
+// from zero because h_{-1}, h_0 are constants: this keeps the small
+// derivative of the slowly varying h_n at full relative precision), in
+// cos(theta) (differentiated Wiscombe recurrence), and in the particle's
+// a_p and n_p (through d alpha_n, d beta_n from the FP64 coefficient kernel).
+// The per-pixel epilogue is evaluated in dual numbers over (kx, ky, kz).
+// d/dk_p = i d/dn_p because a_n, b_n are holomorphic in the relative index.
+// On the optical axis (krho = 0) phi is taken as 0 with zero derivative,
+// the safe branch of theory/jaxLorenzMie.py:170-175.
+#pragma once
+
+#include "lmb_math.cuh"
+
+namespace lmb {
+
+// Per-order record staged in shared memory by the kernels.
+//   c0 = (alpha.re, alpha.im, beta.re, beta.im)
+//   c1 = (n(n+1) alpha.re, n(n+1) alpha.im, 1 + 1/n, n)
+// and, for the Jacobian, the a_p and n_p derivatives of alpha and beta:
+//   c2 = d/da_p (alpha, beta), c3 = d/dn_p (alpha, beta).
+template <typename R>
+struct Quad {
+  R x, y, z, w;
+};
+
+template <typename R>
+struct Geometry {
+  R kr, ikr, mu, sint, cosp, sinp, krho;
+  R s1mu;           // 1 - |cos(theta)|, to full relative precision
+  R smu;            // sign of cos(theta) (+1 when cos(theta) == 0)
+  R ikrs;           // smu / kr: the recurrence coefficient's scale
+  R sigma;          // +1, -1, or 0 (pixel in the particle's plane)
+  cplx<R> phase;    // e^{i(sigma kr - k z_p)}
+  cplx<R> hm1, h0;  // h_{-1}, h_0
+};
+
+// Geometry of one pixel relative to one particle.
+//   dx, dy, dzc: coordinate minus particle position (pixels, FP64)
+//   z: the pixel's own z coordinate; zp: the particle's z
+LMB_HD double reduce_2pi(double t) { return remainder(t, 6.283185307179586); }
+
+template <typename R>
+LMB_HD Geometry<R> geometry(double k, double dx, double dy, double dzc,
+                            double z, double zp, bool bohren) {
+  Geometry<R> g;
+  const R kx = R(k * dx);
+  const R ky = R(k * dy);
+  const R kz = R(-k * dzc);
+  const R krho2 = kx * kx + ky * ky;
+  const R krho = lsqrt(krho2);
+  const R kr = lsqrt(krho2 + kz * kz);
+  const R ikr = R(1) / kr;
+  g.kr = kr;
+  g.ikr = ikr;
+  g.krho = krho;
+  g.mu = kz * ikr;
+  g.sint = krho * ikr;
+  g.s1mu = krho2 / (kr * (kr + labs_(kz)));
+  g.smu = kz < R(0) ? R(-1) : R(1);
+  g.ikrs = g.smu * ikr;
+  if (krho > R(0)) {
+    const R ikrho = R(1) / krho;
+    g.cosp = kx * ikrho;
+    g.sinp = ky * ikrho;
+  } else {
+    g.cosp = R(1);
+    g.sinp = R(0);
+  }
+  const R s = kz > R(0) ? R(1) : (kz < R(0) ? R(-1) : R(0));
+  const R sigma = bohren ? s : -s;
+  g.sigma = sigma;
+  if (sigma != R(0)) {
+    g.hm1 = mk(R(1), R(0));
+    g.h0 = mk(R(0), -sigma);
+    if (sigma == s) {
+      // sign(kz) (kr - |kz|) - k z, with kr - |kz| = krho^2/(kr + |kz|)
+      R arg = s * krho2 / (kr + labs_(kz));
+      if (z != 0.) arg += R(reduce_2pi(-k * z));
+      g.phase = cis(arg);
+    } else {
+      const double kr64 = k * sqrt(dx * dx + dy * dy + dzc * dzc);
+      g.phase = cis(R(reduce_2pi(double(sigma) * kr64 - k * zp)));
+    }
+  } else {
+    // kz == 0: real standing-wave start, xi_{-1} = cos kr, xi_0 = sin kr
+    const double kr64 = k * sqrt(dx * dx + dy * dy + dzc * dzc);
+    const cplx<R> e = cis(R(reduce_2pi(kr64)));
+    g.hm1 = mk(e.re, R(0));
+    g.h0 = mk(e.im, R(0));
+    g.phase = cis(R(reduce_2pi(-k * zp)));
+  }
+  g.h0 = g.smu * g.h0;  // h~_0 = sign(mu) h_0
+  return g;
+}
+
+template <typename R>
+struct Sums {
+  cplx<R> s0, s1, s2;
+};
+
+// The partial-wave sum for the field value only.
+// coef: per-order records (2 Quads per order, index n*2 + {0,1}).
+template <typename R>
+LMB_HD Sums<R> order_sum(const Geometry<R>& g, const Quad<R>* coef,
+                         int nmax) {
+  Sums<R> acc;
+  acc.s0 = mk(R(0), R(0));
+  acc.s1 = acc.s0;
+  acc.s2 = acc.s0;
+  R pim1 = R(0), pi = R(1), del = R(1);
+  cplx<R> h2 = g.hm1, h1 = g.h0;
+  const R sv = g.s1mu, ikr = g.ikrs;
+#pragma unroll 2
+  for (int n = 1; n <= nmax; ++n) {
+    const Quad<R> c0 = coef[2 * n];
+    const Quad<R> c1 = coef[2 * n + 1];
+    const R fn = c1.w;
+    const R spi = sv * pi;
+    const R tau = pim1 - fn * del + fn * spi;
+    const R a2 = (fn + fn - R(1)) * ikr;
+    const cplx<R> h = mk(a2 * h1.re - h2.re, a2 * h1.im - h2.im);
+    const R a1 = fn * ikr;
+    const cplx<R> dh = mk(a1 * h.re - h1.re, a1 * h.im - h1.im);
+    // X = alpha dh, Y = beta h, Z = n(n+1) alpha h
+    const cplx<R> X = mk(c0.x * dh.re - c0.y * dh.im, c0.x * dh.im + c0.y * dh.re);
+    const cplx<R> Y = mk(c0.z * h.re - c0.w * h.im, c0.z * h.im + c0.w * h.re);
+    const cplx<R> Z = mk(c1.x * h.re - c1.y * h.im, c1.x * h.im + c1.y * h.re);
+    acc.s0.re += pi * Z.re;
+    acc.s0.im += pi * Z.im;
+    acc.s1.re += tau * X.re - pi * Y.re;
+    acc.s1.im += tau * X.im - pi * Y.im;
+    acc.s2.re += pi * X.re - tau * Y.re;
+    acc.s2.im += pi * X.im - tau * Y.im;
+    del = c1.z * del - (c1.z + R(1)) * spi;
+    pim1 = pi;
+    pi = pi + del;
+    h2 = h1;
+    h1 = h;
+  }
+  acc.s2 = g.smu * acc.s2;
+  return acc;
+}
+
+// Restore the geometric factors and (optionally) project onto Cartesian
+// axes; multiply by the phase.  Returns the field of one particle.
+template <typename R>
+LMB_HD void epilogue(const Geometry<R>& g, const Sums<R>& s, bool cartesian,
+                     cplx<R>* e) {
+  const R ikr = g.ikr;
+  const cplx<R> es0 = (g.cosp * g.sint * ikr * ikr) * s.s0;
+  const cplx<R> es1 = (g.cosp * ikr) * s.s1;
+  const cplx<R> es2 = (g.sinp * ikr) * s.s2;
+  cplx<R> c0, c1, c2;
+  if (cartesian) {
+    c0 = (g.sint * g.cosp) * es0 + (g.mu * g.cosp) * es1 - g.sinp * es2;
+    c1 = (g.sint * g.sinp) * es0 + (g.mu * g.sinp) * es1 + g.cosp * es2;
+    c2 = g.mu * es0 - g.sint * es1;
+  } else {
+    c0 = es0;
+    c1 = es1;
+    c2 = es2;
+  }
+  e[0] = g.phase * c0;
+  e[1] = g.phase * c1;
+  e[2] = g.phase * c2;
+}
+
+// ---------------------------------------------------------------------------
+// Jacobian
+
+template <typename R>
+struct JacSums {
+  cplx<R> s[3];   // value
+  cplx<R> t[3];   // d/dkr of the phase-reduced sums
+  cplx<R> u[3];   // d/dmu
+  cplx<R> a[3];   // d/da_p
+  cplx<R> p[3];   // d/dn_p
+};
+
+// coef: 4 Quads per order (index n*4 + {0..3}), see Quad above.
+template <typename R>
+LMB_HD JacSums<R> order_sum_jac(const Geometry<R>& g, const Quad<R>* coef,
+                                int nmax) {
+  JacSums<R> A;
+  const cplx<R> zero = mk(R(0), R(0));
+  for (int c = 0; c < 3; ++c) {
+    A.s[c] = zero;
+    A.t[c] = zero;
+    A.u[c] = zero;
+    A.a[c] = zero;
+    A.p[c] = zero;
+  }
+  // pi, Delta and their derivatives with respect to s = 1 - |mu|
+  R pim1 = R(0), pi = R(1), del = R(1);
+  R dpim1 = R(0), dpi = R(0), ddel = R(0);
+  cplx<R> h2 = g.hm1, h1 = g.h0;
+  cplx<R> hp2 = mk(R(0), R(0)), hp1 = hp2;  // d h~/dkr
+  const R sv = g.s1mu, ikr = g.ikrs, ikr2 = g.ikrs * g.ikr;
+  for (int n = 1; n <= nmax; ++n) {
+    const Quad<R> c0 = coef[4 * n];
+    const Quad<R> c1 = coef[4 * n + 1];
+    const Quad<R> c2 = coef[4 * n + 2];
+    const Quad<R> c3 = coef[4 * n + 3];
+    const R fn = c1.w;
+    const R cn = c1.z;
+    const R spi = sv * pi;
+    const R tau = pim1 - fn * del + fn * spi;
+    const R dspi = pi + sv * dpi;
+    const R dtau = dpim1 - fn * ddel + fn * dspi;
+    const R a2 = (fn + fn - R(1)) * ikr;
+    const cplx<R> h = mk(a2 * h1.re - h2.re, a2 * h1.im - h2.im);
+    const R a1 = fn * ikr;
+    const cplx<R> dh = mk(a1 * h.re - h1.re, a1 * h.im - h1.im);
+    const R nn1 = fn * (fn + R(1));
+    // d/dkr of h~_n = (2n-1) ikr h~_{n-1} - h~_{n-2} and of dh
+    const cplx<R> hp = mk(a2 * hp1.re - (fn + fn - R(1)) * ikr2 * h1.re - hp2.re,
+                          a2 * hp1.im - (fn + fn - R(1)) * ikr2 * h1.im - hp2.im);
+    const cplx<R> dhp = mk(a1 * hp.re - fn * ikr2 * h.re - hp1.re,
+                           a1 * hp.im - fn * ikr2 * h.im - hp1.im);
+    const cplx<R> al = mk(c0.x, c0.y), be = mk(c0.z, c0.w);
+    const cplx<R> al1 = mk(c1.x, c1.y);
+    const cplx<R> ala = mk(c2.x, c2.y), bea = mk(c2.z, c2.w);
+    const cplx<R> aln = mk(c3.x, c3.y), ben = mk(c3.z, c3.w);
+    // value: X = alpha dh, Y = beta h, Z = n(n+1) alpha h
+    const cplx<R> X = al * dh, Y = be * h, Z = al1 * h;
+    A.s[0] = A.s[0] + pi * Z;
+    A.s[1] = A.s[1] + tau * X - pi * Y;
+    A.s[2] = A.s[2] + pi * X - tau * Y;
+    // s tangent: same X, Y, Z with dpi/ds, dtau/ds
+    A.u[0] = A.u[0] + dpi * Z;
+    A.u[1] = A.u[1] + dtau * X - dpi * Y;
+    A.u[2] = A.u[2] + dpi * X - dtau * Y;
+    // kr tangent: h -> hp, dh -> dhp
+    const cplx<R> Xk = al * dhp, Yk = be * hp, Zk = al1 * hp;
+    A.t[0] = A.t[0] + pi * Zk;
+    A.t[1] = A.t[1] + tau * Xk - pi * Yk;
+    A.t[2] = A.t[2] + pi * Xk - tau * Yk;
+    // a_p: n(n+1) d alpha is formed from d alpha
+    const cplx<R> Xa = ala * dh, Ya = bea * h, Za = nn1 * (ala * h);
+    A.a[0] = A.a[0] + pi * Za;
+    A.a[1] = A.a[1] + tau * Xa - pi * Ya;
+    A.a[2] = A.a[2] + pi * Xa - tau * Ya;
+    const cplx<R> Xn = aln * dh, Yn = ben * h, Zn = nn1 * (aln * h);
+    A.p[0] = A.p[0] + pi * Zn;
+    A.p[1] = A.p[1] + tau * Xn - pi * Yn;
+    A.p[2] = A.p[2] + pi * Xn - tau * Yn;
+    const R deln = cn * del - (cn + R(1)) * spi;
+    const R ddeln = cn * ddel - (cn + R(1)) * dspi;
+    pim1 = pi;
+    pi = pi + deln;
+    del = deln;
+    dpim1 = dpi;
+    dpi = dpi + ddeln;
+    ddel = ddeln;
+    h2 = h1;
+    h1 = h;
+    hp2 = hp1;
+    hp1 = hp;
+  }
+  // Undo the parity folding (identity when cos(theta) >= 0) and turn the
+  // s tangent into d/dmu: d/dmu = -sign(mu) d/ds on pi~, tau~.
+  const R sg = g.smu;
+  A.s[2] = sg * A.s[2];
+  A.a[2] = sg * A.a[2];
+  A.p[2] = sg * A.p[2];
+  A.t[2] = sg * A.t[2];
+  A.u[0] = (-sg) * A.u[0];
+  A.u[1] = (-sg) * A.u[1];
+  A.u[2] = -A.u[2];
+  return A;
+}
+
+// Dual numbers over the three displacement coordinates (kx, ky, kz).
+template <typename R>
+struct dr3 {
+  R v, g[3];
+};
+template <typename R>
+struct dc3 {
+  cplx<R> v, g[3];
+};
+template <typename R>
+LMB_HD dr3<R> dmul(dr3<R> a, dr3<R> b) {
+  dr3<R> r;
+  r.v = a.v * b.v;
+  for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+  return r;
+}
+template <typename R>
+LMB_HD dc3<R> dmul(dc3<R> a, dr3<R> b) {
+  dc3<R> r;
+  r.v = b.v * a.v;
+  for (int i = 0; i < 3; ++i) r.g[i] = b.v * a.g[i] + b.g[i] * a.v;
+  return r;
+}
+template <typename R>
+LMB_HD dc3<R> dmul(dc3<R> a, dc3<R> b) {
+  dc3<R> r;
+  r.v = a.v * b.v;
+  for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+  return r;
+}
+template <typename R>
+LMB_HD dc3<R> dadd(dc3<R> a, dc3<R> b) {
+  dc3<R> r;
+  r.v = a.v + b.v;
+  for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] + b.g[i];
+  return r;
+}
+template <typename R>
+LMB_HD dc3<R> dsub(dc3<R> a, dc3<R> b) {
+  dc3<R> r;
+  r.v = a.v - b.v;
+  for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] - b.g[i];
+  return r;
+}
+
+// Field of one particle and its derivatives with respect to the particle
+// parameters, in the order x_p, y_p, z_p, a_p, n_p, k_p:
+//   e[c]        field component c (Cartesian)
+//   de[j][c]    d e[c] / d param_j
+template <typename R>
+LMB_HD void epilogue_jac(const Geometry<R>& g, const JacSums<R>& A, R k,
+                         cplx<R>* e, cplx<R> (*de)[3]) {
+  const R ikr = g.ikr, mu = g.mu, st = g.sint, cp = g.cosp, sp = g.sinp;
+  // d kr / d(kx, ky, kz)
+  const R krg[3] = {st * cp, st * sp, mu};
+  dr3<R> IKR, MU, ST, CP, SP;
+  IKR.v = ikr;
+  MU.v = mu;
+  ST.v = st;
+  CP.v = cp;
+  SP.v = sp;
+  for (int i = 0; i < 3; ++i) IKR.g[i] = -ikr * ikr * krg[i];
+  MU.g[0] = -mu * krg[0] * ikr;
+  MU.g[1] = -mu * krg[1] * ikr;
+  MU.g[2] = st * st * ikr;
+  ST.g[0] = cp * mu * mu * ikr;
+  ST.g[1] = sp * mu * mu * ikr;
+  ST.g[2] = -st * mu * ikr;
+  if (g.krho > R(0)) {
+    const R ik = R(1) / g.krho;
+    CP.g[0] = sp * sp * ik;
+    CP.g[1] = -cp * sp * ik;
+    SP.g[0] = -cp * sp * ik;
+    SP.g[1] = cp * cp * ik;
+  } else {
+    CP.g[0] = CP.g[1] = SP.g[0] = SP.g[1] = R(0);
+  }
+  CP.g[2] = SP.g[2] = R(0);
+  // phase-reduced sums as duals: S' = t dkr + u dmu
+  dc3<R> S[3];
+  for (int c = 0; c < 3; ++c) {
+    S[c].v = A.s[c];
+    for (int i = 0; i < 3; ++i) S[c].g[i] = krg[i] * A.t[c] + MU.g[i] * A.u[c];
+  }
+  // The phase e^{i(sigma kr - k z_p)}: its kz tangent also carries the
+  // explicit -k z_p (kz = k (z_p - z)), so that d/dz_p = k d/dkz.  The
+  // combined rate sigma mu - 1 equals -(1 - |mu|) when sigma = sign(mu),
+  // which is formed without cancellation.
+  dc3<R> PH;
+  PH.v = g.phase;
+  {
+    const cplx<R> ip = g.sigma * mul_i(g.phase);
+    PH.g[0] = krg[0] * ip;
+    PH.g[1] = krg[1] * ip;
+    const R rate = (g.sigma != R(0) && g.sigma == g.smu) ? -g.s1mu
+                                                          : g.sigma * mu - R(1);
+    PH.g[2] = rate * mul_i(g.phase);
+  }
+  // geometric factors
+  const dr3<R> G0 = dmul(dmul(CP, ST), dmul(IKR, IKR));
+  const dr3<R> G1 = dmul(CP, IKR);
+  const dr3<R> G2 = dmul(SP, IKR);
+  const dc3<R> es0 = dmul(S[0], G0), es1 = dmul(S[1], G1), es2 = dmul(S[2], G2);
+  const dc3<R> c0 = dsub(dadd(dmul(es0, dmul(ST, CP)), dmul(es1, dmul(MU, CP))),
+                         dmul(es2, SP));
+  const dc3<R> c1 = dadd(dadd(dmul(es0, dmul(ST, SP)), dmul(es1, dmul(MU, SP))),
+                         dmul(es2, CP));
+  const dc3<R> c2 = dsub(dmul(es0, MU), dmul(es1, ST));
+  const dc3<R> E[3] = {dmul(c0, PH), dmul(c1, PH), dmul(c2, PH)};
+  // material sums share the value geometry
+  const R g0 = G0.v, g1 = G1.v, g2 = G2.v;
+  for (int c = 0; c < 3; ++c) {
+    e[c] = E[c].v;
+    // kx = k (x - x_p), ky = k (y - y_p), kz = k (z_p - z)
+    de[0][c] = (-k) * E[c].g[0];
+    de[1][c] = (-k) * E[c].g[1];
+    de[2][c] = k * E[c].g[2];
+  }
+  cplx<R> ma[3], mn[3];
+  {
+    const cplx<R> a0 = g0 * A.a[0], a1 = g1 * A.a[1], a2 = g2 * A.a[2];
+    const cplx<R> n0 = g0 * A.p[0], n1 = g1 * A.p[1], n2 = g2 * A.p[2];
+    ma[0] = (st * cp) * a0 + (mu * cp) * a1 - sp * a2;
+    ma[1] = (st * sp) * a0 + (mu * sp) * a1 + cp * a2;
+    ma[2] = mu * a0 - st * a1;
+    mn[0] = (st * cp) * n0 + (mu * cp) * n1 - sp * n2;
+    mn[1] = (st * sp) * n0 + (mu * sp) * n1 + cp * n2;
+    mn[2] = mu * n0 - st * n1;
+  }
+  for (int c = 0; c < 3; ++c) {
+    de[3][c] = g.phase * ma[c];
+    de[4][c] = g.phase * mn[c];
+    de[5][c] = mul_i(de[4][c]);
+  }
+}
+
+// Hologram from the total scattered field: |E + x|^2 = |E|^2 + 2 Re(E_x) + 1
+template <typename R>
+LMB_HD R intensity(const cplx<R>* e) {
+  return norm2(e[0]) + norm2(e[1]) + norm2(e[2]) + R(2) * e[0].re + R(1);
+}
+
+}  // namespace lmb

@@ -1,0 +1,202 @@
+// CPU build of the kernels' own arithmetic, for tests without a GPU.
+//
+// Compiles the __host__ __device__ headers of pylorenzmie_b200/csrc with g++
+// so that tests/test_cpu_harness.py can check, on the CPU, the Mie
+// recurrences, the per-pixel sums (FP32 and FP64), the forward-mode
+// Jacobian and the Levenberg-Marquardt state machine against the FP64
+// oracle and scipy.  Test infrastructure only: the library never calls it.
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "lmb_lm.cuh"
+#include "lmb_mie.cuh"
+#include "lmb_pixel.cuh"
+
+using namespace lmb;
+
+#define API extern "C"
+
+// ab: [cap+1][2] complex (4 doubles per n), dab: [cap+1][4] complex.
+API int h_sphere_ab(double a_p, double n_p, double k_p, double n_m, double lam,
+                int cap, double* ab, double* dab, int* nmax) {
+  MieScalars s = mie_setup(a_p, n_p, k_p, n_m, lam);
+  *nmax = s.nmax;
+  if (s.nmax > cap) return 3;
+  std::vector<zd> d1in(s.nmax + 1), d1inz(s.nmax + 1), zeta(s.nmax + 1),
+      zetax(s.nmax + 1);
+  std::vector<double> d1m(s.nmax + 1), d1mx(s.nmax + 1), psi(s.nmax + 1),
+      psix(s.nmax + 1);
+  mie_d1_inside(s, d1in.data(), d1inz.data());
+  mie_d1_medium(s, d1m.data(), d1mx.data());
+  mie_upward(s, d1m.data(), d1mx.data(), psi.data(), psix.data(), zeta.data(),
+             zetax.data());
+  memset(ab, 0, sizeof(double) * 4 * (cap + 1));
+  if (dab) memset(dab, 0, sizeof(double) * 8 * (cap + 1));
+  for (int n = 1; n <= s.nmax; ++n) {
+    zd out[2], dout[4];
+    mie_coefficient(s, n, d1in.data(), d1inz.data(), psi.data(), psix.data(),
+                    zeta.data(), zetax.data(), out, dab ? dout : 0);
+    ab[4 * n + 0] = out[0].re;
+    ab[4 * n + 1] = out[0].im;
+    ab[4 * n + 2] = out[1].re;
+    ab[4 * n + 3] = out[1].im;
+    if (dab)
+      for (int j = 0; j < 4; ++j) {
+        dab[8 * n + 2 * j] = dout[j].re;
+        dab[8 * n + 2 * j + 1] = dout[j].im;
+      }
+  }
+  return 0;
+}
+
+static zd rot_i(zd z, int k) {
+  switch (k & 3) {
+    case 0: return z;
+    case 1: return mk(-z.im, z.re);
+    case 2: return mk(-z.re, -z.im);
+    default: return mk(z.im, -z.re);
+  }
+}
+
+template <typename R>
+static void stage(const double* ab, const double* dab, int nmax, Quad<R>* q,
+                  int w) {
+  for (int n = 0; n <= nmax; ++n) {
+    Quad<R> r[4];
+    memset(r, 0, sizeof(r));
+    if (n > 0) {
+      const double fn = n, nn1 = fn * (fn + 1.), en = (2. * fn + 1.) / nn1;
+      const zd a = mk(ab[4 * n], ab[4 * n + 1]), b = mk(ab[4 * n + 2], ab[4 * n + 3]);
+      const zd al = en * rot_i(a, n + 1), be = en * rot_i(b, n);
+      r[0] = Quad<R>{R(al.re), R(al.im), R(be.re), R(be.im)};
+      r[1] = Quad<R>{R(nn1 * al.re), R(nn1 * al.im), R(1. + 1. / fn), R(fn)};
+      if (w == 4) {
+        zd d[4];
+        for (int j = 0; j < 4; ++j) d[j] = mk(dab[8 * n + 2 * j], dab[8 * n + 2 * j + 1]);
+        const zd ala = en * rot_i(d[0], n + 1), bea = en * rot_i(d[1], n);
+        const zd aln = en * rot_i(d[2], n + 1), ben = en * rot_i(d[3], n);
+        r[2] = Quad<R>{R(ala.re), R(ala.im), R(bea.re), R(bea.im)};
+        r[3] = Quad<R>{R(aln.re), R(aln.im), R(ben.re), R(ben.im)};
+      }
+    }
+    for (int j = 0; j < w; ++j) q[w * n + j] = r[j];
+  }
+}
+
+// Field of one sphere at coords [3][npts]; out: [3][npts] complex (re, im).
+template <typename R>
+static void field_one(const double* coords, long long npts, const double* p,
+                      const double* ab, int nmax, double k, int flags,
+                      double* out) {
+  std::vector<Quad<R>> q(2 * (nmax + 1));
+  stage<R>(ab, 0, nmax, q.data(), 2);
+  for (long long i = 0; i < npts; ++i) {
+    const double x = coords[i], y = coords[npts + i], z = coords[2 * npts + i];
+    Geometry<R> g = geometry<R>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
+    Sums<R> s = order_sum<R>(g, q.data(), nmax);
+    cplx<R> e[3];
+    epilogue<R>(g, s, flags & 1, e);
+    for (int c = 0; c < 3; ++c) {
+      out[2 * (c * npts + i)] = e[c].re;
+      out[2 * (c * npts + i) + 1] = e[c].im;
+    }
+  }
+}
+
+API void h_field(const double* coords, long long npts, const double* p,
+             const double* ab, int nmax, double k, int flags, int fp64,
+             double* out) {
+  if (fp64)
+    field_one<double>(coords, npts, p, ab, nmax, k, flags, out);
+  else
+    field_one<float>(coords, npts, p, ab, nmax, k, flags, out);
+}
+
+// Hologram and Jacobian of one sphere: holo [npts], jac [6][npts].
+template <typename R>
+static void jac_one(const double* coords, long long npts, const double* p,
+                    const double* ab, const double* dab, int nmax, double k,
+                    int flags, double* holo, double* jac) {
+  std::vector<Quad<R>> q(4 * (nmax + 1));
+  stage<R>(ab, dab, nmax, q.data(), 4);
+  for (long long i = 0; i < npts; ++i) {
+    const double x = coords[i], y = coords[npts + i], z = coords[2 * npts + i];
+    Geometry<R> g = geometry<R>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
+    JacSums<R> A = order_sum_jac<R>(g, q.data(), nmax);
+    cplx<R> e[3], de[6][3];
+    epilogue_jac<R>(g, A, R(k), e, de);
+    holo[i] = intensity<R>(e);
+    const cplx<R> et0 = mk(e[0].re + R(1), e[0].im);
+    for (int j = 0; j < 6; ++j)
+      jac[j * npts + i] = 2 * (et0.re * de[j][0].re + et0.im * de[j][0].im +
+                               e[1].re * de[j][1].re + e[1].im * de[j][1].im +
+                               e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+  }
+}
+
+API void h_jacobian(const double* coords, long long npts, const double* p,
+                const double* ab, const double* dab, int nmax, double k,
+                int flags, int fp64, double* holo, double* jac) {
+  if (fp64)
+    jac_one<double>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac);
+  else
+    jac_one<float>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac);
+}
+
+// Levenberg-Marquardt state machine driven from Python.
+struct HLM {
+  LMState s;
+  LMSettings set;
+  int started;
+  int done;
+};
+
+API void* h_lm_new(int n, const int* slots, const double* x0, double ftol,
+               double xtol, double gtol, double factor, int maxfev) {
+  HLM* h = (HLM*)calloc(1, sizeof(HLM));
+  h->s.n = n;
+  for (int a = 0; a < n; ++a) {
+    h->s.slot[a] = slots[a];
+    h->s.x[a] = x0[a];
+  }
+  h->set.ftol = ftol;
+  h->set.xtol = xtol;
+  h->set.gtol = gtol;
+  h->set.factor = factor;
+  h->set.maxfev = maxfev;
+  return h;
+}
+
+API void h_lm_free(void* p) { free(p); }
+
+// Feed the evaluation of the point last requested.  Returns 1 when done;
+// otherwise writes the next point (free variables) to xnext.
+API int h_lm_feed(void* p, double f2, const double* jtj21, const double* jtf6,
+              double* xnext) {
+  HLM* h = (HLM*)p;
+  LMEval ev;
+  ev.f2 = f2;
+  for (int j = 0; j < 21; ++j) ev.jtj[j] = jtj21[j];
+  for (int j = 0; j < 6; ++j) ev.jtf[j] = jtf6[j];
+  int done = h->started ? lm_after_trial(h->s, ev, h->set) : lm_start(h->s, ev, h->set);
+  h->started = 1;
+  h->done = done;
+  if (!done)
+    for (int a = 0; a < h->s.n; ++a) xnext[a] = h->s.x[a] + h->s.p[a];
+  return done;
+}
+
+API void h_lm_result(void* p, long long npix, double* x, int* info, int* nfev,
+                 int* njev, double* redchi, double* dp) {
+  HLM* h = (HLM*)p;
+  for (int a = 0; a < h->s.n; ++a) x[a] = h->s.x[a];
+  *info = h->s.info;
+  *nfev = h->s.nfev;
+  *njev = h->s.njev;
+  lm_statistics(h->s, npix, redchi, dp);
+}
+
+API int h_sym6(int i, int j) { return sym6(i, j); }
+

@@ -1,0 +1,119 @@
+'''GPU parity of the device Levenberg-Marquardt fit against the reference.
+
+The reference fit (tests/golden/fit.npz) is the reference Optimizer run on
+a seeded 201x201 hologram (config: a_p=0.75 um, n_p=1.42, z_p=200 px,
+noise 0.05, start perturbed by 5 % in a_p, 0.02 in n_p, 10 px in z_p).
+The device fit must land within a_p 1 nm, n_p 1e-4, z_p 0.02 px (and
+x_p, y_p 0.02 px) of it.
+'''
+import numpy as np
+import pandas as pd
+import pytest
+
+from oracle import field as ofield, fit as ofit
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+TOL = {'x_p': 0.02, 'y_p': 0.02, 'z_p': 0.02, 'a_p': 1e-3, 'n_p': 1e-4,
+       'k_p': 1e-4}
+
+
+def make_optimizer(start, shape):
+    from pylorenzmie_b200 import LorenzMie, Optimizer, Instrument, Sphere
+    inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
+    s = Sphere(a_p=start[3], n_p=start[4], k_p=start[5])
+    s.r_p = start[:3]
+    model = LorenzMie(coordinates=LorenzMie.meshgrid(shape), particle=s,
+                      instrument=inst)
+    return Optimizer(model=model)
+
+
+def test_fit_matches_reference(golden_fit):
+    from pylorenzmie_b200 import Hologram
+    shape = tuple(golden_fit['shape'])
+    opt = make_optimizer(golden_fit['start'], shape)
+    result = opt.optimize(Hologram(golden_fit['data'].reshape(shape)))
+    ref = dict(zip(golden_fit['keys'], golden_fit['values']))
+    assert isinstance(result, pd.Series)
+    assert list(result.index) == list(golden_fit['keys'])
+    assert bool(result['success'])
+    assert result['npix'] == shape[0] * shape[1]
+    for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p'):
+        assert abs(result[k] - ref[k]) <= TOL[k], (k, result[k], ref[k])
+        assert abs(result['d' + k] / ref['d' + k] - 1) < 1e-2, k
+    assert abs(result['redchi'] / ref['redchi'] - 1) < 1e-4
+    assert opt._result.nfev == int(golden_fit['nfev'])
+    assert opt._result.status == int(golden_fit['status'])
+    # the model is left at the fitted values
+    assert abs(opt.model.particle.a_p - result['a_p']) < 1e-12
+    assert 'a_p' in opt.report()
+
+
+def _render(seed, shape, p):
+    rng = np.random.default_rng(seed)
+    c = ofield.meshgrid(shape)
+    h = ofield.hologram(c, [dict(zip(KEYS, p))], ofield.DEFAULT_INSTRUMENT)
+    return h + rng.normal(0., 0.05, h.shape)
+
+
+def test_fit_batch_matches_oracle():
+    '''16 features of mixed crop sizes in one device call vs the oracle fit
+    (the reference algorithm, scipy lm + FD Jacobian) of each.'''
+    from pylorenzmie_b200 import Hologram
+    rng = np.random.default_rng(7)
+    holos, starts, oracle = [], [], []
+    for i in range(16):
+        s = int(rng.choice([41, 61, 81, 101]))
+        c = (s - 1) / 2.
+        truth = [c + rng.uniform(-2, 2), c + rng.uniform(-2, 2),
+                 rng.uniform(150., 250.), rng.uniform(0.5, 1.0),
+                 rng.uniform(1.38, 1.6), 0.]
+        data = _render(100 + i, (s, s), truth)
+        start = list(truth)
+        start[2] += 15.
+        start[3] *= 1.05
+        start[4] += 0.03
+        holos.append(Hologram(data.reshape(s, s)))
+        starts.append(start)
+        oracle.append(ofit.fit(data, ofield.meshgrid((s, s)),
+                               dict(zip(KEYS, start)),
+                               ofield.DEFAULT_INSTRUMENT))
+    opt = make_optimizer(starts[0], (8, 8))
+    df = opt.optimize_batch(holos, starts=np.array(starts))
+    assert len(df) == 16
+    for i in range(16):
+        o = oracle[i]
+        if not o['success']:
+            continue
+        assert df['success'][i], i
+        for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p'):
+            assert abs(df[k][i] - o[k]) <= TOL[k], (i, k, df[k][i], o[k])
+
+
+def test_fit_edge_cases():
+    from pylorenzmie_b200 import Hologram
+    opt = make_optimizer([4., 4., 150., 0.75, 1.45, 0.], (8, 8))
+    # empty batch
+    df = opt.optimize_batch([], starts=np.zeros((0, 6)))
+    assert len(df) == 0
+    # fewer pixels than variables: MINPACK's improper input
+    tiny = Hologram(np.ones((2, 2)))
+    with pytest.raises(ValueError):
+        opt.optimize(tiny)
+    # non-finite residuals at the start point
+    bad = np.ones((16, 16))
+    bad[3, 3] = np.nan
+    with pytest.raises(ValueError):
+        opt.optimize(Hologram(bad))
+    # in a batch both are reported per feature, the good one still fits
+    good = _render(3, (41, 41), [20., 20., 200., 0.75, 1.45, 0.])
+    df = opt.optimize_batch(
+        [tiny, Hologram(bad), Hologram(good.reshape(41, 41))],
+        starts=np.array([[1., 1., 150., .75, 1.45, 0.],
+                         [8., 8., 150., .75, 1.45, 0.],
+                         [20., 20., 210., .78, 1.47, 0.]]))
+    assert list(df['status'][:2]) == [-1, -2]
+    assert not df['success'][0] and not df['success'][1]
+    assert df['success'][2]
+    assert abs(df['a_p'][2] - 0.75) < 0.02
