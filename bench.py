@@ -1,0 +1,466 @@
+'''Benchmark: batched Levenberg-Marquardt fits of 201x201 hologram crops.
+
+A step fits one batch of B = 256 single-sphere features (201x201 crops,
+a_p = 0.75 um, n_p = 1.42, z_p = 200 px, noise 0.05, start perturbed by
+5 % / +0.02 / +10 px) with the device-resident fitter (FP64 Mie
+coefficients, FP32 per-pixel sums, analytic Jacobian, MINPACK LM steps on
+the device).  Inputs are synthetic (seeded; see pylorenzmie_b200.workloads).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  ``value`` is whole-job features/s with the
+inputs resident in HBM; ``e2e`` is the same metric through the public API
+(Optimizer.optimize_batch on host numpy crops: packing, host-to-device
+copies, the fit and the device-to-host read of the results inside the
+timed region).  ``--impl reference`` times the reference algorithm (the
+FP64 numpy oracle with scipy's lm fit, all host cores) on a bounded sample
+of the same workload.  Multi-GPU runs (torchrun) shard features across
+ranks with no data-path collective (weak scaling).
+'''
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'features fitted/s (LM, 201² crops)'
+UNIT = 'features/s'
+BATCH = 256
+SHAPE = (201, 201)
+ROTATE = 4  # distinct input batches cycled through (4 x 41 MB > 126 MB L2)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--batch', type=int, default=BATCH)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-extras', action='store_true')
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get('RANK', 0)),
+            int(os.environ.get('WORLD_SIZE', 1)),
+            int(os.environ.get('LOCAL_RANK', 0)))
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference algorithm (oracle) on the host cores
+
+def cpu_fit_rate(nfeat, seed=0):
+    '''features/s of the oracle fit over a spawn pool of all host cores.'''
+    import multiprocessing as mp
+    import numpy as np
+    from pylorenzmie_b200 import workloads
+    from oracle import bench_tasks
+    cores = os.cpu_count() or 1
+    truth, start = workloads.batch_201(nfeat, seed)
+    # one thread per worker process: BLAS/OpenMP threads would oversubscribe
+    for var in ('OMP_NUM_THREADS', 'MKL_NUM_THREADS', 'OPENBLAS_NUM_THREADS'):
+        os.environ[var] = '1'
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(cores) as pool:
+        data = pool.starmap(bench_tasks.render_201,
+                            [(truth[i], 1000 + i) for i in range(nfeat)])
+        t0 = time.perf_counter()
+        res = pool.starmap(bench_tasks.fit_201,
+                           [(data[i], start[i]) for i in range(nfeat)])
+        dt = time.perf_counter() - t0
+    ok = float(np.mean([r['success'] for r in res]))
+    return nfeat / dt, cores, dt, ok
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    sample = max(cores, 8)
+    for _ in range(max(args.warmup, 0)):
+        cpu_fit_rate(sample, seed=7)
+    rates, times = [], []
+    for k in range(args.steps):
+        r, cores, dt, ok = cpu_fit_rate(sample, seed=100 + k)
+        rates.append(r)
+        times.append(dt)
+    value = sample * len(times) / sum(times)
+    line = {
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'impl': 'reference',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': 1e3 * sum(times) / len(times),
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic (seeded)',
+        'config': {'workload': f'LM fit of 201x201 single-sphere crops, '
+                               f'{sample} features per step on the host',
+                   'global_batch': sample, 'crop': '201x201',
+                   'parallelism': f'{cores} host processes'},
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores,
+                         'kind': 'port',
+                         'sample': f'{sample} features per step x '
+                                   f'{args.steps} steps, oracle FP64 model '
+                                   '+ scipy lm (FD Jacobian)'},
+        'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# clocks under load (NVML, read only)
+
+class ClockSampler:
+    REASONS = {0x1: 'gpu_idle', 0x2: 'applications_clocks_setting',
+               0x4: 'sw_power_cap', 0x8: 'hw_slowdown', 0x10: 'sync_boost',
+               0x20: 'sw_thermal_slowdown', 0x40: 'hw_thermal_slowdown',
+               0x80: 'hw_power_brake_slowdown'}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], 0, None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(
+                self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(
+                    self.h, nv.NVML_CLOCK_SM))
+                self.reasons |= int(
+                    nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def start(self):
+        if self.nv is not None:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+
+    def stop(self):
+        if self.nv is not None:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': self.max_mhz,
+                    'reasons': ['unavailable']}
+        return {'sm_mhz': statistics.median(self.samples),
+                'sm_max_mhz': self.max_mhz,
+                'reasons': [v for k, v in self.REASONS.items()
+                            if self.reasons & k],
+                'samples': len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+
+def b200_arm(args):
+    rank, world, local = dist_env()
+    cpu_base = None
+    if (rank == 0 and world == 1 and not args.no_cpu_baseline):
+        # before the first GPU call: the pool uses spawn anyway
+        cores = os.cpu_count() or 1
+        sample = min(max(2 * cores, 8), 64)
+        rate, cores, dt, ok = cpu_fit_rate(sample, seed=3)
+        cpu_base = {'value': rate, 'unit': UNIT, 'cores': cores,
+                    'kind': 'port',
+                    'sample': f'{sample} features of the same workload, '
+                              f'oracle FP64 model + scipy lm (FD Jacobian), '
+                              f'{dt:.1f} s wall on {cores} processes'}
+
+    import ctypes
+    import numpy as np
+    import torch
+    import torch.distributed as tdist
+    from pylorenzmie_b200 import _native, workloads, Hologram, Optimizer, \
+        LorenzMie, Instrument
+    from pylorenzmie_b200.analysis import _fit
+
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    if world > 1:
+        from datetime import timedelta
+        tdist.init_process_group('nccl', timeout=timedelta(seconds=120),
+                                 device_id=dev)
+
+    def barrier():
+        if world > 1:
+            tdist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    lib = _native.load()
+    inst = Instrument()
+    variables = ['x_p', 'y_p', 'z_p', 'a_p', 'n_p']
+    B = args.batch
+    npix = SHAPE[0] * SHAPE[1]
+
+    # device-resident inputs: ROTATE distinct batches
+    batches = []
+    for r in range(ROTATE):
+        seed = 1000 * rank + r
+        truth, start = workloads.batch_201(B, seed)
+        data = workloads.render(truth, SHAPE, seed=seed, device=dev)
+        items = [(data[i].cpu().numpy(), (0., 0., SHAPE[0], SHAPE[1]), None)
+                 for i in range(B)]
+        packed = _fit.PackedFeatures(items)
+        d_feat, d_data, d_coords, d_params = _fit.upload(packed, start, dev)
+        cap = _fit.fit_capacity(start, inst.n_m, inst.wavelength)
+        batches.append(dict(packed=packed, start=start, truth=truth,
+                            d_feat=d_feat, d_data=d_data,
+                            d_params0=d_params.clone(), d_params=d_params,
+                            cap=cap))
+
+    def step(i, stats=False):
+        b = batches[i % ROTATE]
+        b['d_params'].copy_(b['d_params0'])
+        return _fit.fit_device(b['d_feat'], b['d_data'], None, b['d_params'],
+                               B, npix * B, inst, variables, None, b['cap'],
+                               b['start'], stats)
+
+    peak = ctypes.c_double()
+    _native.check(lib.lmb_measure_fp32_peak(ctypes.byref(peak),
+                                            torch.cuda.current_stream().cuda_stream),
+                  'lmb_measure_fp32_peak')
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    stats = []
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        _, fs = step(i, stats=True)
+        stats.append(fs)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks.stop()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * B * args.steps / (ms * 1e-3)
+
+    # results of the last timed step: converged?
+    res = step(args.steps - 1)[0]
+    resv = res[:B * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
+        _native.RESULT_DTYPE)
+    success = float(resv['success'].mean())
+    nfev = float(resv['nfev'].mean())
+
+    eval_ms = sum(s.eval_ms for s in stats)
+    launches = sum(s.eval_launches for s in stats)
+    pixels = sum(s.pixels for s in stats)
+    porders = sum(s.pixel_orders for s in stats)
+    flop_per_launch = (292. * porders + 476. * pixels) / launches
+    avg_ms = eval_ms / launches
+    achieved = flop_per_launch / (avg_ms * 1e-3) / 1e12
+    peak_tf = peak.value / 1e12
+    traffic = None
+    tfile = ROOT / 'profiles' / 'traffic.json'
+    if tfile.exists():
+        try:
+            t = json.loads(tfile.read_text()).get('k_fit_eval')
+            if t:
+                traffic = t['bytes_per_launch_full_batch']
+        except Exception:
+            traffic = None
+    roofline = {'bound': 'fp32', 'achieved': achieved, 'peak': peak_tf,
+                'unit': 'TFLOP/s', 'frac': achieved / peak_tf,
+                'traffic': traffic, 'kernel': 'k_fit_eval',
+                'peak_source': 'measured FP32 FMA throughput of this GPU '
+                               '(lmb_measure_fp32_peak, same run); '
+                               'MEASURED_PEAKS.json has no FP32 CUDA-core '
+                               'figure',
+                'flop_per_launch': flop_per_launch,
+                'avg_launch_ms': avg_ms,
+                'work': '292 FLOP per pixel-order + 476 FLOP per pixel '
+                        '(value + 6-column Jacobian + normal equations)'}
+    gpu_launches = sum(s.kernel_launches for s in stats)
+
+    # end to end through the public API with host crops
+    opt = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1)),
+                                    instrument=inst, device=dev))
+    host_sets = []
+    for r in range(ROTATE):
+        b = batches[r]
+        holos = [Hologram(b['packed'].data[i * npix:(i + 1) * npix]
+                          .reshape(SHAPE).astype(np.float64))
+                 for i in range(B)]
+        host_sets.append((holos, b['start']))
+    for i in range(max(args.warmup, 1)):
+        opt.optimize_batch(host_sets[i % ROTATE][0],
+                           starts=host_sets[i % ROTATE][1])
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        df = opt.optimize_batch(host_sets[i % ROTATE][0],
+                                starts=host_sets[i % ROTATE][1])
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    h2d = B * npix * 4 + B * 40 + B * 48
+    d2h = B * 48 + B * _native.RESULT_DTYPE.itemsize
+    e2e = {'value': world * B * args.steps / e2e_s, 'unit': UNIT,
+           'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+           'api': 'Optimizer.optimize_batch(list[Hologram], starts)'}
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = run_extras(dev, inst, value)
+
+    if world > 1:
+        tdist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic (seeded); rendered by the FP64 kernel + N(0, 0.05)',
+        'config': {'workload': 'batched LM fit, 201x201 single-sphere crops '
+                               '(a_p 0.75 um, n_p 1.42, z_p 200 px, start '
+                               '+5%/+0.02/+10 px), FP64 Mie coefficients + '
+                               'FP32 sums + analytic Jacobian',
+                   'global_batch': B * world, 'per_gpu_batch': B,
+                   'crop': '201x201', 'parallelism': f'features sharded '
+                   f'over {world} GPU(s), no collective',
+                   'l2': f'{ROTATE} rotating input batches '
+                         f'({ROTATE * B * npix * 4 / 1e6:.0f} MB) > 126 MB L2'},
+        'fit_quality': {'success_fraction': success, 'mean_nfev': nfev},
+        'roofline': roofline,
+        'cpu_baseline': cpu_base,
+        'e2e': e2e,
+        'gpu_launches': gpu_launches,
+        'clocks': clocks.summary(),
+        'extras': extras,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_extras(dev, inst, chosen_value):
+    '''Secondary figures on one GPU: the plain-FP64 path, hologram Mpx/s of
+    a full frame, and mixed-crop batched fits.'''
+    import numpy as np
+    import torch
+    from scipy.optimize import least_squares
+    from pylorenzmie_b200 import workloads, LorenzMie, Hologram, Optimizer
+    from pylorenzmie_b200.analysis import _fit
+    out = {}
+
+    # plain FP64: FP64 field kernel + forward-difference Jacobian + host LM,
+    # one feature at a time (the reference Optimizer's loop on our kernel)
+    nplain = 8
+    truth, start = workloads.batch_201(nplain, 77)
+    data = workloads.render(truth, SHAPE, seed=77, device=dev).cpu().numpy()
+    model = LorenzMie(coordinates=LorenzMie.meshgrid(SHAPE), instrument=inst,
+                      double_precision=True, device=dev)
+    names = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')
+
+    def plain_fit(d, s):
+        def resid(v):
+            model.properties = dict(zip(names, v))
+            return (model.hologram() - d) / inst.noise
+        model.particle = workloads.spheres(s)[0]
+        return least_squares(resid, s[:5], method='lm', ftol=1e-4, xtol=1e-6,
+                             gtol=1e-6, max_nfev=2000, diff_step=1e-5,
+                             x_scale='jac')
+    plain_fit(data[0].ravel().astype(float), start[0])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(nplain):
+        plain_fit(data[i].ravel().astype(float), start[i])
+    plain = nplain / (time.perf_counter() - t0)
+    out['plain_fp64_gpu'] = {
+        'value': plain, 'unit': UNIT,
+        'method': 'FP64 field kernel + forward-difference Jacobian + host '
+                  'scipy lm, one feature at a time',
+        'chosen_over_plain': chosen_value / plain}
+
+    # hologram throughput of a 1280x1024 frame with 16 spheres
+    p = workloads.frame(seed=5)
+    while p.shape[0] < 16:
+        p = np.vstack([p, workloads.frame(seed=5 + p.shape[0])])[:16]
+    for fp64 in (False, True):
+        m = LorenzMie(coordinates=LorenzMie.meshgrid((1024, 1280)),
+                      particle=workloads.spheres(p), instrument=inst,
+                      double_precision=fp64, device=dev)
+        m.hologram(device=True)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 10
+        e0.record()
+        for _ in range(reps):
+            m.hologram(device=True)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / reps * 1e-3
+        out['frame_fp64' if fp64 else 'frame_fp32'] = {
+            'value': 1280 * 1024 * p.shape[0] / sec / 1e6,
+            'unit': 'Mpx/s (pixel-particles)', 'spheres': int(p.shape[0]),
+            'ms_per_frame': sec * 1e3}
+
+    # mixed crop sizes 51..301, 256 features per launch
+    sides, truth, start = workloads.mixed_crops(256, seed=9)
+    holos = []
+    for i in range(256):
+        s = int(sides[i])
+        d = workloads.render(truth[i:i + 1], (s, s), seed=i, device=dev)[0]
+        holos.append(Hologram(d.cpu().numpy().astype(np.float64)))
+    opt = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1)),
+                                    instrument=inst, device=dev))
+    opt.optimize_batch(holos, starts=start)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        df = opt.optimize_batch(holos, starts=start)
+    torch.cuda.synchronize()
+    out['mixed_crops_e2e'] = {
+        'value': 256 * reps / (time.perf_counter() - t0), 'unit': UNIT,
+        'success_fraction': float(df['success'].mean()),
+        'mean_pixels': float(np.mean(sides.astype(float) ** 2))}
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

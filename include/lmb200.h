@@ -92,7 +92,7 @@ int lmb_layered_ab(const double *radii, const double *indices, int nlayers,
  *   coords      [3][npts] FP64 (x row, y row, z row)
  *   spheres     [nparticles] positions; ab/nmax as from lmb_sphere_ab
  *               (or lmb_layered_ab) for the same particles
- *   item_start  [nitems+1] host int array: particles of item i are
+ *   item_start  [nitems+1] int: particles of item i are
  *               item_start[i] .. item_start[i+1]-1 (CSR)
  *   k           wave number in the medium, rad/pixel (Instrument.wavenumber)
  *   out         [nitems][3][npts] complex64 (FP32) or complex128 (LMB_FP64)
@@ -177,6 +177,22 @@ typedef struct lmb_fit_result {
   int nfev, njev;
 } lmb_fit_result;
 
+/*
+ * Optional measurements of one lmb_fit_batch call (host struct).  When
+ * requested, the call records CUDA events around each evaluation launch on
+ * its stream and counts the work done on the device.
+ */
+typedef struct lmb_fit_stats {
+  double eval_ms;        /* summed device time of the evaluation launches */
+  double total_ms;       /* device time from the first to the last launch */
+  double pixels;         /* pixels evaluated, summed over launches */
+  double pixel_orders;   /* pixels x partial-wave orders evaluated */
+  int eval_launches;     /* evaluation kernel launches */
+  int kernel_launches;   /* all kernels the call launched */
+  int iterations;        /* evaluation/step rounds */
+  int pad;
+} lmb_fit_stats;
+
 /* Scratch bytes lmb_fit_batch needs for these sizes. */
 size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
                                int nmax_cap);
@@ -193,9 +209,12 @@ size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
  *   coords   packed float32 (x, y) pairs for explicit-pixel features, or NULL
  *   params   [nfeatures] in: start values, out: fitted values
  *   results  [nfeatures]
+ *   settings host pointer
  *   workspace / workspace_bytes: scratch of lmb_fit_workspace_bytes(...)
+ *   stats    optional host pointer (NULL: no measurement)
  * The call returns once every feature has terminated (or
  * max_iterations evaluations have run); it synchronizes the stream.
+ * Features whose pixels fall outside [0, total_pixels) end with status -1.
  */
 int lmb_fit_batch(const lmb_feature *features, int nfeatures,
                   long long total_pixels, const float *data,
@@ -203,7 +222,7 @@ int lmb_fit_batch(const lmb_feature *features, int nfeatures,
                   double wavelength, double magnification, double noise,
                   int nmax_cap, const lmb_fit_settings *settings,
                   lmb_fit_result *results, void *workspace,
-                  size_t workspace_bytes, void *stream);
+                  size_t workspace_bytes, lmb_fit_stats *stats, void *stream);
 
 /*
  * Measured FP32 fused-multiply-add throughput of the current device in

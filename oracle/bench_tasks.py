@@ -1,0 +1,26 @@
+'''Oracle tasks for the CPU baseline of bench.py (test infrastructure).
+
+Module-level functions so that a ``spawn`` process pool can run them: one
+renders a 201x201 single-sphere hologram with the FP64 oracle plus noise,
+the other runs the reference fitting algorithm (scipy least_squares lm with
+a forward-difference Jacobian, Optimizer defaults) on it.
+'''
+import numpy as np
+
+from .field import hologram, meshgrid, DEFAULT_INSTRUMENT
+from .fit import fit
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+
+
+def render_201(truth, seed):
+    shape = (201, 201)
+    rng = np.random.default_rng(seed)
+    h = hologram(meshgrid(shape), [dict(zip(KEYS, truth))],
+                 DEFAULT_INSTRUMENT)
+    return h + rng.normal(0., 0.05, h.shape)
+
+
+def fit_201(data, start):
+    return fit(data, meshgrid((201, 201)), dict(zip(KEYS, start)),
+               DEFAULT_INSTRUMENT)

@@ -42,6 +42,14 @@ class FitSettings(ctypes.Structure):
                 ('flags', ctypes.c_int), ('max_iterations', ctypes.c_int)]
 
 
+class FitStats(ctypes.Structure):
+    _fields_ = [('eval_ms', ctypes.c_double), ('total_ms', ctypes.c_double),
+                ('pixels', ctypes.c_double), ('pixel_orders', ctypes.c_double),
+                ('eval_launches', ctypes.c_int),
+                ('kernel_launches', ctypes.c_int),
+                ('iterations', ctypes.c_int), ('pad', ctypes.c_int)]
+
+
 class LMBError(RuntimeError):
     '''A non-zero status from the CUDA library.'''
 
@@ -73,7 +81,8 @@ _SIGNATURES = {
                               _vp, _vp, _vp, _sz, _vp]),
     'lmb_fit_workspace_bytes': (_sz, [_i, _ll, _i]),
     'lmb_fit_batch': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _d, _d, _d, _d, _i,
-                           ctypes.POINTER(FitSettings), _vp, _vp, _sz, _vp]),
+                           ctypes.POINTER(FitSettings), _vp, _vp, _sz,
+                           ctypes.POINTER(FitStats), _vp]),
     'lmb_measure_fp32_peak': (_i, [ctypes.POINTER(_d), _vp]),
 }
 

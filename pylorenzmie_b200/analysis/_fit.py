@@ -80,36 +80,81 @@ class PackedFeatures:
         return n
 
 
-def _to_device(a, dev):
-    t = torch.from_numpy(np.ascontiguousarray(a))
-    if t.numel() == 0:
-        return t.to(dev)
-    return t.pin_memory().to(dev, non_blocking=True)
+_TORCH_DTYPE = {'<f4': torch.float32, '<f8': torch.float64,
+                '|u1': torch.uint8, '<i4': torch.int32, '<i8': torch.int64}
 
 
-def fit_packed(packed, starts, instrument, variables, settings=None,
-               device=None, nmax_cap=None):
-    '''Fit every packed feature; returns (params (B, 6), results record
-    array with dparams, redchi, cost, status, success, nfev, njev).'''
+class _Staging:
+    '''Reusable pinned host buffer for host-to-device copies (allocating
+    pinned memory on every call would cost more than the copy).'''
+
+    def __init__(self):
+        self.buf = None
+
+    def take(self, nbytes):
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8,
+                                   pin_memory=True)
+        return self.buf
+
+
+_staging = _Staging()
+
+
+def _to_device(arrays, dev):
+    '''Copy numpy arrays to the device through one pinned staging buffer
+    and one host-to-device transfer; returns device tensors (same dtypes).'''
+    arrays = [np.ascontiguousarray(a) for a in arrays]
+    sizes = [(a.nbytes + 255) // 256 * 256 for a in arrays]
+    total = sum(sizes)
+    stage = _staging.take(total)
+    host = stage.numpy()
+    off = 0
+    for a, n in zip(arrays, sizes):
+        host[off:off + a.nbytes] = a.view(np.uint8).reshape(-1)
+        off += n
+    dbuf = torch.empty(max(total, 1), dtype=torch.uint8, device=dev)
+    dbuf[:total].copy_(stage[:total], non_blocking=True)
+    out, off = [], 0
+    for a, n in zip(arrays, sizes):
+        out.append(dbuf[off:off + a.nbytes].view(_TORCH_DTYPE[a.dtype.str]))
+        off += n
+    # the staging buffer is reused by the next call: wait for this copy
+    torch.cuda.current_stream(dev).synchronize()
+    return out
+
+
+def upload(packed, starts, device=None):
+    '''Device copies of a packed batch: (features, data, coords, params).'''
     dev = get_device(device)
+    starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
+    arrays = [packed.features.view(np.uint8), packed.data, starts]
+    if packed.coords is not None:
+        arrays.append(packed.coords)
+    t = _to_device(arrays, dev)
+    d_feat, d_data, d_params = t[0], t[1], t[2]
+    d_coords = t[3] if packed.coords is not None else None
+    return d_feat, d_data, d_coords, d_params
+
+
+def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
+               instrument, variables, settings=None, nmax_cap=None,
+               starts_host=None, stats=False):
+    '''Run lmb_fit_batch on device-resident inputs.  d_params is updated in
+    place with the fitted values; returns (results tensor (B*80 uint8),
+    FitStats or None).'''
+    dev = d_data.device
     lib = _native.load()
     settings = dict(DEFAULT_SETTINGS if settings is None else settings)
-    starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
-    B = starts.shape[0]
-    res = np.zeros(B, dtype=_native.RESULT_DTYPE)
-    if B == 0:
-        return starts.copy(), res
     n_m = float(instrument.n_m)
     lam = float(instrument.wavelength)
-    cap = nmax_cap or fit_capacity(starts, n_m, lam)
-    d_data = _to_device(packed.data, dev)
-    d_feat = _to_device(packed.features.view(np.uint8), dev)
-    d_coords = (_to_device(packed.coords, dev) if packed.coords is not None
-                else None)
-    d_params = _to_device(starts, dev)
-    d_res = torch.empty(B * _native.RESULT_DTYPE.itemsize, dtype=torch.uint8,
-                        device=dev)
-    nbytes = lib.lmb_fit_workspace_bytes(B, packed.total, cap)
+    if nmax_cap is None:
+        sh = (starts_host if starts_host is not None
+              else d_params.view(torch.float64).reshape(-1, 6).cpu().numpy())
+        nmax_cap = fit_capacity(sh, n_m, lam)
+    d_res = torch.empty(max(nfeatures, 1) * _native.RESULT_DTYPE.itemsize,
+                        dtype=torch.uint8, device=dev)
+    nbytes = lib.lmb_fit_workspace_bytes(nfeatures, total_pixels, nmax_cap)
     ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     st = _native.FitSettings()
     st.ftol = float(settings.get('ftol', 1e-4) or 0.)
@@ -120,11 +165,33 @@ def fit_packed(packed, starts, instrument, variables, settings=None,
     st.variables = variable_mask(variables)
     st.flags = _native.LMB_BOHREN
     st.max_iterations = st.max_nfev
+    fs = _native.FitStats() if stats else None
     _native.check(lib.lmb_fit_batch(
-        ptr(d_feat), B, packed.total, ptr(d_data), ptr(d_coords),
+        ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
         ptr(d_params), n_m, lam, float(instrument.magnification),
-        float(instrument.noise), cap, st, ptr(d_res), ptr(ws), nbytes,
-        stream_handle(dev)), 'lmb_fit_batch')
-    params = d_params.cpu().numpy()
-    res = d_res.cpu().numpy().view(_native.RESULT_DTYPE).copy()
-    return params, res
+        float(instrument.noise), nmax_cap, st, ptr(d_res), ptr(ws), nbytes,
+        fs, stream_handle(dev)), 'lmb_fit_batch')
+    return d_res, fs
+
+
+def fit_packed(packed, starts, instrument, variables, settings=None,
+               device=None, nmax_cap=None, stats=False):
+    '''Fit every packed feature; returns (params (B, 6), results record
+    array with dparams, redchi, cost, status, success, nfev, njev) and,
+    when stats, the FitStats of the call.'''
+    starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
+    B = starts.shape[0]
+    if B == 0:
+        res = np.zeros(0, dtype=_native.RESULT_DTYPE)
+        return (starts.copy(), res, None) if stats else (starts.copy(), res)
+    d_feat, d_data, d_coords, d_params = upload(packed, starts, device)
+    if nmax_cap is None:
+        nmax_cap = fit_capacity(starts, float(instrument.n_m),
+                                float(instrument.wavelength))
+    d_res, fs = fit_device(d_feat, d_data, d_coords, d_params, B,
+                           packed.total, instrument, variables, settings,
+                           nmax_cap, starts, stats)
+    params = d_params.view(torch.float64).reshape(B, 6).cpu().numpy()
+    res = d_res[:B * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
+        _native.RESULT_DTYPE).copy()
+    return (params, res, fs) if stats else (params, res)

@@ -4,6 +4,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <vector>
+
 #include "lmb200.h"
 #include "lmb_kernels.cuh"
 
@@ -63,7 +65,7 @@ FitLayout fit_layout(int nf, long long total_pixels, int nmax_cap) {
   L.tile_begin = take(sizeof(int) * (nf + 1));
   L.tiles = take(sizeof(int2) * size_t(L.max_tiles));
   L.partial = take(sizeof(double) * FIT_NSUM * size_t(L.max_tiles));
-  L.counters = take(sizeof(int) * 8);
+  L.counters = take(sizeof(int) * 16);
   L.total = align_up(off, 256);
   return L;
 }
@@ -244,7 +246,7 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
                   double wavelength, double magnification, double noise,
                   int nmax_cap, const lmb_fit_settings* settings,
                   lmb_fit_result* results, void* workspace,
-                  size_t workspace_bytes, void* stream) {
+                  size_t workspace_bytes, lmb_fit_stats* stats, void* stream) {
   if (nfeatures < 0 || total_pixels < 0 || bad_cap(nmax_cap) || !settings)
     return LMB_ERR_ARG;
   if (nfeatures == 0) return LMB_OK;
@@ -272,6 +274,7 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
   c.tiles = reinterpret_cast<int2*>(ws + L.tiles);
   c.partial = reinterpret_cast<double*>(ws + L.partial);
   c.counters = reinterpret_cast<int*>(ws + L.counters);
+  c.work = reinterpret_cast<unsigned long long*>(ws + L.counters + 8 * sizeof(int));
   c.total_pixels = total_pixels;
   c.nf = nfeatures;
   c.nmax_cap = nmax_cap;
@@ -302,29 +305,87 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
   LMB_CK(smem_attr((const void*)eval, coef_smem));
   const int egrid = persistent_grid((const void*)eval, kFitTPB, coef_smem);
 
-  k_fit_setup<<<1, 1024, 0, st>>>(c);
-  LMB_CK(cudaGetLastError());
-  k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
-  LMB_CK(cudaGetLastError());
-  for (int it = 0; it < c.max_iterations; ++it) {
-    LMB_CK(cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st));
-    eval<<<egrid, kFitTPB, coef_smem, st>>>(c);
-    LMB_CK(cudaGetLastError());
-    LMB_CK(cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st));
+  // Optional timing: one event pair per evaluation launch, plus the span.
+  std::vector<cudaEvent_t> ev;
+  auto mark = [&](void) -> cudaError_t {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r != cudaSuccess) return r;
+    ev.push_back(e);
+    return cudaEventRecord(e, st);
+  };
+  auto release = [&]() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    ev.clear();
+  };
+  int launches = 0, evals = 0, iterations = 0;
+  int status = LMB_OK;
+  do {
+    if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+    k_fit_setup<<<1, 1024, 0, st>>>(c);
     k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
-    LMB_CK(cudaGetLastError());
-    int running = 0;
-    LMB_CK(cudaMemcpyAsync(&running, c.counters + 1, sizeof(int),
-                           cudaMemcpyDeviceToHost, st));
-    LMB_CK(cudaStreamSynchronize(st));
-    if (running == 0) break;
-  }
-  k_fit_finalize<<<(nfeatures + 127) / 128, 128, 0, st>>>(c);
-  LMB_CK(cudaGetLastError());
+    launches += 2;
+    if (cudaGetLastError() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+    for (int it = 0; it < c.max_iterations; ++it) {
+      if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) {
+        status = LMB_ERR_CUDA;
+        break;
+      }
+      if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+      eval<<<egrid, kFitTPB, coef_smem, st>>>(c);
+      if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+      cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
+      k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
+      launches += 2;
+      ++evals;
+      ++iterations;
+      if (cudaGetLastError() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+      int running = 0;
+      if (cudaMemcpyAsync(&running, c.counters + 1, sizeof(int),
+                          cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess) {
+        status = LMB_ERR_CUDA;
+        break;
+      }
+      if (running == 0) break;
+    }
+    if (status != LMB_OK) break;
+    k_fit_finalize<<<(nfeatures + 127) / 128, 128, 0, st>>>(c);
+    launches += 1;
+    if (cudaGetLastError() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+    if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+  } while (0);
   int overflow = 0;
-  LMB_CK(cudaMemcpyAsync(&overflow, c.counters + 3, sizeof(int),
-                         cudaMemcpyDeviceToHost, st));
-  LMB_CK(cudaStreamSynchronize(st));
+  unsigned long long work[2] = {0ull, 0ull};
+  if (status == LMB_OK) {
+    if (cudaMemcpyAsync(&overflow, c.counters + 3, sizeof(int),
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(work, c.work, sizeof(work), cudaMemcpyDeviceToHost,
+                        st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      status = LMB_ERR_CUDA;
+  }
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    if (status == LMB_OK && ev.size() >= 2) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev.front(), ev.back());
+      stats->total_ms = ms;
+      // events: [span start] then pairs around each evaluation, then end
+      for (size_t q = 1; q + 1 < ev.size(); q += 2) {
+        float e = 0.f;
+        cudaEventElapsedTime(&e, ev[q], ev[q + 1]);
+        stats->eval_ms += e;
+      }
+    }
+    stats->pixels = double(work[0]);
+    stats->pixel_orders = double(work[1]);
+    stats->eval_launches = evals;
+    stats->kernel_launches = launches;
+    stats->iterations = iterations;
+  }
+  release();
+  if (status != LMB_OK) return status;
   return overflow ? LMB_ERR_WORKSPACE : LMB_OK;
 }
 

@@ -355,6 +355,7 @@ struct FitCtx {
   int2* tiles;         // [max_tiles]
   double* partial;     // [max_tiles][FIT_NSUM]
   int* counters;       // [0] tile queue, [1] running, [2] ntiles, [3] overflow
+  unsigned long long* work;  // [0] pixels, [1] pixel-orders evaluated
   long long total_pixels;
   int nf, nmax_cap, max_tiles, tile_pixels;
   double n_m, wavelength, k, inv_noise;
@@ -401,6 +402,8 @@ __global__ void k_fit_setup(FitCtx c) {
     c.counters[3] = carry > c.max_tiles ? 1 : 0;
     c.counters[0] = 0;
     c.counters[1] = 0;
+    c.work[0] = 0ull;
+    c.work[1] = 0ull;
   }
   __syncthreads();
   const int ntiles = carry;
@@ -504,6 +507,12 @@ k_fit_eval(FitCtx c) {
     block_reduce<FIT_NSUM, TPB>(acc, red);
     if (threadIdx.x < FIT_NSUM)
       c.partial[(size_t)t * FIT_NSUM + threadIdx.x] = red[threadIdx.x];
+    if (threadIdx.x == 0) {
+      long long np = ft.npix - tile.y;
+      if (np > c.tile_pixels) np = c.tile_pixels;
+      atomicAdd(c.work, (unsigned long long)np);
+      atomicAdd(c.work + 1, (unsigned long long)np * (unsigned long long)nm);
+    }
     __syncthreads();
   }
 }

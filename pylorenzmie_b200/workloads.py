@@ -1,0 +1,115 @@
+'''Seeded synthetic workloads of the benchmark configurations.
+
+No public dataset is involved: every input is drawn from a seeded
+``numpy.random.default_rng`` with the shapes and distributions below, and
+holograms are rendered with the FP64 per-pixel kernel plus Gaussian noise
+of sigma = 0.05 (the instrument's noise).
+
+* single_201  -- one 201x201 crop: a_p = 0.75 um, n_p = 1.42, k_p = 0,
+  x_p, y_p = 100 + U(-2, 2) px, z_p = 200 px; start perturbed by 5 % in
+  a_p, +0.02 in n_p and +10 px in z_p.  ``batch_201`` stacks B of them.
+* frame       -- a 1280x1024 frame with 1..16 spheres (seeded count),
+  a_p ~ U(0.4, 3.0) um, n_p ~ U(1.38, 1.70), k_p ~ U(0, 1e-3),
+  z_p ~ U(50, 600) px constrained to z_p >= a_p/magnification + 10 px so
+  that the focal plane never cuts through a sphere, positions uniform
+  over the frame.
+* mixed_crops -- B features of square odd crops of side U{51, 53, .., 301}
+  with single_201's parameters centred on the crop; start perturbed by
+  5 % in a_p, +0.03 in n_p and +15 px in z_p.
+* large       -- crops of 401x401 with a_p ~ U(3, 6) um, n_p ~ U(1.4, 2.0),
+  z_p ~ U(200, 600) px.
+'''
+import numpy as np
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+NOISE = 0.05
+
+
+def batch_201(B, seed=0):
+    '''Truth and start parameters (B, 6) for 201x201 crops.'''
+    rng = np.random.default_rng(seed)
+    truth = np.zeros((B, 6))
+    truth[:, 0] = 100. + rng.uniform(-2., 2., B)
+    truth[:, 1] = 100. + rng.uniform(-2., 2., B)
+    truth[:, 2] = 200.
+    truth[:, 3] = 0.75
+    truth[:, 4] = 1.42
+    start = truth.copy()
+    start[:, 3] *= 1.05
+    start[:, 4] += 0.02
+    start[:, 2] += 10.
+    return truth, start
+
+
+def mixed_crops(B, seed=0):
+    '''Crop sides (B,), truth and start (B, 6) for mixed crop sizes.'''
+    rng = np.random.default_rng(seed)
+    sides = 2 * rng.integers(25, 151, B) + 1          # 51 .. 301, odd
+    truth = np.zeros((B, 6))
+    c = (sides - 1) / 2.
+    truth[:, 0] = c + rng.uniform(-2., 2., B)
+    truth[:, 1] = c + rng.uniform(-2., 2., B)
+    truth[:, 2] = 200.
+    truth[:, 3] = 0.75
+    truth[:, 4] = 1.42
+    start = truth.copy()
+    start[:, 3] *= 1.05
+    start[:, 4] += 0.03
+    start[:, 2] += 15.
+    return sides, truth, start
+
+
+def frame(seed=0, shape=(1024, 1280), magnification=0.048):
+    '''Sphere parameters (n, 6) of one frame.'''
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 17))
+    p = np.zeros((n, 6))
+    p[:, 3] = rng.uniform(0.4, 3.0, n)
+    p[:, 4] = rng.uniform(1.38, 1.70, n)
+    p[:, 5] = rng.uniform(0., 1e-3, n)
+    zmin = p[:, 3] / magnification + 10.
+    p[:, 2] = np.maximum(rng.uniform(50., 600., n), zmin)
+    p[:, 0] = rng.uniform(0., shape[1], n)
+    p[:, 1] = rng.uniform(0., shape[0], n)
+    return p
+
+
+def large(B, seed=0, side=401):
+    rng = np.random.default_rng(seed)
+    p = np.zeros((B, 6))
+    c = (side - 1) / 2.
+    p[:, 0] = c + rng.uniform(-2., 2., B)
+    p[:, 1] = c + rng.uniform(-2., 2., B)
+    p[:, 2] = rng.uniform(200., 600., B)
+    p[:, 3] = rng.uniform(3., 6., B)
+    p[:, 4] = rng.uniform(1.4, 2.0, B)
+    return p
+
+
+def spheres(params):
+    '''Sphere objects from a (n, 6) parameter array.'''
+    from .theory import Sphere
+    out = []
+    for row in np.atleast_2d(params):
+        s = Sphere(a_p=row[3], n_p=row[4], k_p=row[5])
+        s.r_p = row[:3]
+        out.append(s)
+    return out
+
+
+def render(params, shape, seed=0, instrument=None, device=None,
+           noise=NOISE):
+    '''Noisy holograms (B, ny, nx) float32 of one sphere each, rendered by
+    the FP64 kernel on the device; same crop shape for the whole batch.'''
+    import torch
+    from .theory import LorenzMie, Instrument
+    inst = instrument or Instrument()
+    m = LorenzMie(coordinates=LorenzMie.meshgrid(shape), instrument=inst,
+                  double_precision=True, device=device)
+    lists = [[s] for s in spheres(params)]
+    h = m.batch_hologram(lists, device=True)
+    g = torch.Generator(device=h.device)
+    g.manual_seed(int(seed))
+    h = h + noise * torch.randn(h.shape, generator=g, device=h.device,
+                                dtype=h.dtype)
+    return h.float().reshape(len(lists), *shape)

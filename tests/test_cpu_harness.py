@@ -1,0 +1,152 @@
+'''The kernels' own arithmetic, compiled for the CPU (tests/cpu_harness),
+against the FP64 oracle and scipy.
+
+This checks, without a GPU, the exact code the sm_100a kernels run: the
+FP64 Mie recurrences with tangents, the per-pixel sums in FP32 and FP64,
+the forward-mode Jacobian, and the Levenberg-Marquardt state machine
+(restated MINPACK lmder) against scipy's least_squares(method='lm').
+'''
+import ctypes
+
+import numpy as np
+import pytest
+from scipy.optimize import least_squares
+
+from oracle import mie, field, fit
+from tests.cpu_harness.loader import Harness, ptr
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+K = field.wavenumber(1.34, 0.447, 0.048)
+
+
+@pytest.fixture(scope='module')
+def h():
+    return Harness()
+
+
+def test_sphere_ab_and_tangents(h, golden_ab):
+    for i, case in enumerate(golden_ab['cases']):
+        ab, dab = h.sphere_ab(*case, deriv=True)
+        ref = golden_ab[f'ab_{i}']
+        assert ab.shape == ref.shape
+        assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max() + 1e-300
+    # tangents against central differences of the oracle
+    for (a, n, k) in [(0.75, 1.45, 0.), (1.5, 1.59, 0.002), (0.4, 1.38, 0.)]:
+        ab, dab = h.sphere_ab(a, n, k, 1.34, 0.447, deriv=True)
+        da, dn = 1e-6 * a, 1e-6
+        fa = (mie.mie_coefficients(a + da, n, k, 1.34, 0.447) -
+              mie.mie_coefficients(a - da, n, k, 1.34, 0.447)) / (2 * da)
+        fn = (mie.mie_coefficients(a, n + dn, k, 1.34, 0.447) -
+              mie.mie_coefficients(a, n - dn, k, 1.34, 0.447)) / (2 * dn)
+        assert np.abs(dab[:, :2] - fa).max() < 1e-6 * np.abs(fa).max()
+        assert np.abs(dab[:, 2:] - fn).max() < 1e-6 * np.abs(fn).max()
+
+
+@pytest.mark.parametrize('name', ['torch64', 'cupy128', 'pair96', 'absorb48',
+                                  'below40', 'sph_nb32', 'sph_b32',
+                                  'cart_nb32', 'big64'])
+@pytest.mark.parametrize('fp64', [0, 1])
+def test_pixel_sums(h, golden_holo, name, fp64):
+    shape = tuple(golden_holo[name + '_shape'])
+    cart, bohren = (bool(v) for v in golden_holo[name + '_flags'])
+    c = field.coordinates3(field.meshgrid(shape))
+    E = np.zeros((3, c.shape[1]), complex)
+    for p in golden_holo[name + '_particles']:
+        ab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447)
+        E += h.field(c, p[:3], ab, K, cart, bohren, fp64)
+    holo = np.sum(np.abs(E + np.array([[1], [0], [0]])) ** 2, axis=0)
+    err = np.abs(holo - golden_holo[name + '_holo']).max()
+    assert err <= (1e-11 if fp64 else 2e-5), err
+    if name + '_field' in golden_holo:
+        ferr = np.abs(E - golden_holo[name + '_field']).max()
+        assert ferr <= (1e-11 if fp64 else 2e-5), ferr
+
+
+@pytest.mark.parametrize('shape,p', [
+    ((48, 48), [20.3, 25.7, 120., 0.9, 1.6, 0.01]),
+    ((40, 40), [20., 20., -130., 0.6, 1.5, 0.]),
+    ((33, 33), [16., 16., 80., 1.0, 1.4, 0.]),
+])
+@pytest.mark.parametrize('fp64', [0, 1])
+def test_jacobian(h, shape, p, fp64):
+    c = field.coordinates3(field.meshgrid(shape))
+    ab, dab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447, deriv=True)
+    H, J = h.jacobian(c, p[:3], ab, dab, K, True, fp64)
+    inst = field.DEFAULT_INSTRUMENT
+    h0 = field.hologram(c, [dict(zip(KEYS, p))], inst)
+    assert np.abs(H - h0).max() < (1e-11 if fp64 else 2e-5)
+    for j in range(6):
+        step = 1e-5 * max(abs(p[j]), 1e-2) if j < 5 else 1e-7
+        pp, pm = list(p), list(p)
+        pp[j] += step
+        pm[j] -= step
+        fd = (field.hologram(c, [dict(zip(KEYS, pp))], inst) -
+              field.hologram(c, [dict(zip(KEYS, pm))], inst)) / (2 * step)
+        err = np.abs(J[j] - fd).max() / np.abs(fd).max()
+        assert err < (1e-5 if fp64 else 3e-4), (KEYS[j], err)
+
+
+def _lm_run(h, model, data, variables, p0, noise=0.05):
+    lib = h.lib
+    slots = np.array(variables, dtype=np.int32)
+    x0 = np.array([p0[j] for j in variables])
+    hd = lib.h_lm_new(len(variables), ptr(slots, ctypes.POINTER(ctypes.c_int)),
+                      ptr(x0), 1e-4, 1e-6, 1e-6, 100., 2000)
+    p = np.array(p0, float)
+    xn = np.zeros(6)
+    while True:
+        H, J = model(p)
+        r = (H - data) / noise
+        Jn = J / noise
+        jtj = np.array([Jn[a] @ Jn[b] for a in range(6) for b in range(a, 6)])
+        done = lib.h_lm_feed(hd, float(r @ r), ptr(jtj),
+                             ptr(np.ascontiguousarray(Jn @ r)), ptr(xn))
+        if done:
+            break
+        p = np.array(p0, float)
+        for a, j in enumerate(variables):
+            p[j] = xn[a]
+    x = np.zeros(6)
+    info, nfev, njev = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rc, dp = ctypes.c_double(), np.zeros(6)
+    lib.h_lm_result(hd, data.size, ptr(x), ctypes.byref(info),
+                    ctypes.byref(nfev), ctypes.byref(njev), ctypes.byref(rc),
+                    ptr(dp))
+    lib.h_lm_free(hd)
+    n = len(variables)
+    return x[:n], info.value, nfev.value, njev.value, rc.value, dp[:n]
+
+
+@pytest.mark.parametrize('variables', [[0, 1, 2, 3, 4], [0, 1, 2, 3, 4, 5],
+                                       [2, 3, 4], [3, 4]])
+def test_lm_state_machine_matches_scipy(h, golden_fit, variables):
+    '''Same residuals and Jacobian in, same iterates out: the device LM
+    logic follows MINPACK lmder as scipy runs it.'''
+    shape = tuple(golden_fit['shape'])
+    c = field.coordinates3(field.meshgrid(shape))
+    data = golden_fit['data']
+    start = golden_fit['start']
+
+    def model(p):
+        ab, dab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447, deriv=True)
+        return h.jacobian(c, p[:3], ab, dab, K, True, 1)
+
+    x, info, nfev, njev, redchi, dp = _lm_run(h, model, data, variables,
+                                              start)
+    base = np.array(start, float)
+
+    def params(v):
+        q = base.copy()
+        q[variables] = v
+        return q
+    res = least_squares(lambda v: (model(params(v))[0] - data) / 0.05,
+                        base[variables],
+                        jac=lambda v: model(params(v))[1][variables].T / 0.05,
+                        method='lm', ftol=1e-4, xtol=1e-6, gtol=1e-6,
+                        max_nfev=2000, x_scale='jac')
+    rc, sdp = fit.statistics(res, data.size)
+    np.testing.assert_allclose(x, res.x, rtol=1e-9, atol=1e-9)
+    assert nfev == res.nfev and njev == res.njev
+    assert {1: 2, 2: 3, 3: 4, 4: 1}[info] == res.status
+    assert abs(redchi - rc) < 1e-9 * rc
+    np.testing.assert_allclose(dp, sdp, rtol=1e-6)

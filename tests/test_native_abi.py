@@ -1,0 +1,94 @@
+'''The C-ABI library: it loads without a GPU, exports every entry point that
+include/lmb200.h declares, and its struct layouts match the host mirror.
+No compute runs here (only calls that return before touching CUDA).'''
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from pylorenzmie_b200 import _native, build
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = '\n'.join(p.read_text() for p in sorted((ROOT / 'include').glob('*.h')))
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    return sorted(set(re.findall(r'\b(lmb_\w+)\s*\(', text)))
+
+
+@pytest.fixture(scope='module')
+def lib():
+    return _native.load()
+
+
+def test_library_is_in_tree_and_sm100a(lib):
+    path = _native.library_path()
+    assert path.exists() and path.parent == ROOT / 'pylorenzmie_b200' / '_lib'
+    cmd = build.command()
+    assert 'arch=compute_100a,code=sm_100a' in ' '.join(cmd)
+
+
+def test_exports_every_declared_symbol(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 12
+    out = subprocess.run(['nm', '-D', '--defined-only',
+                          str(_native.library_path())],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r' T (\w+)', out))
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    for s in syms:
+        getattr(lib, s)
+    assert set(_native.symbols()) <= set(syms)
+
+
+def test_version_and_status_strings(lib):
+    assert lib.lmb_version() == 100
+    for st in range(6):
+        assert isinstance(_native.status_string(st), str)
+    assert 'workspace' in _native.status_string(_native.LMB_ERR_WORKSPACE)
+
+
+def test_struct_layouts():
+    assert _native.SPHERE_DTYPE.itemsize == 48
+    assert _native.FEATURE_DTYPE.itemsize == 40
+    assert _native.RESULT_DTYPE.itemsize == 80
+    assert ctypes.sizeof(_native.FitSettings) == 48
+    assert ctypes.sizeof(_native.FitStats) == 48
+
+
+def test_argument_checks_without_gpu(lib):
+    # these return before any CUDA call
+    assert lib.lmb_sphere_ab(None, 0, 1.34, 0.447, 10, None, None, None,
+                             None, None) == _native.LMB_OK
+    assert lib.lmb_sphere_ab(None, 1, 1.34, 0.447, 0, None, None, None,
+                             None, None) == _native.LMB_ERR_ARG
+    assert lib.lmb_sphere_ab(None, 1, 1.34, 0.447, 10, None, None, None,
+                             None, None) == _native.LMB_ERR_ARG
+    assert lib.lmb_hologram(None, 0, None, None, 0, None, None, 10, 1., 3,
+                            None, None) == _native.LMB_OK
+    assert lib.lmb_hologram(None, 10, None, None, 1, None, None, 10, 1., 3,
+                            None, None) == _native.LMB_ERR_ARG
+    assert lib.lmb_jacobian(None, 0, None, 0, None, None, None, 10, 1., 3,
+                            None, None, None) == _native.LMB_OK
+    st = _native.FitSettings()
+    assert lib.lmb_fit_batch(None, 0, 0, None, None, None, 1.34, 0.447,
+                             0.048, 0.05, 10, st, None, None, 0, None,
+                             None) == _native.LMB_OK
+    assert lib.lmb_fit_batch(None, 2, 10, None, None, None, 1.34, 0.447,
+                             0.048, 0.05, 10, st, None, None, 0, None,
+                             None) == _native.LMB_ERR_ARG
+
+
+def test_workspace_sizes(lib):
+    a = lib.lmb_fit_workspace_bytes(256, 256 * 201 * 201, 40)
+    b = lib.lmb_fit_workspace_bytes(512, 512 * 201 * 201, 40)
+    assert 0 < a < b
+    assert a % 256 == 0
+    assert lib.lmb_fit_workspace_bytes(0, 0, 40) == 0
+    assert lib.lmb_vjp_workspace_bytes(1000, 2) == 8 * 2 * 6 * 8
+    assert lib.lmb_vjp_workspace_bytes(0, 2) == 0
