@@ -225,6 +225,42 @@ int lmb_fit_batch(const lmb_feature *features, int nfeatures,
                   size_t workspace_bytes, lmb_fit_stats *stats, void *stream);
 
 /*
+ * lmb_fit_batch for callers that cannot allocate device memory.  No
+ * counterpart in the reference (its fits run on the host).
+ *
+ * Who needs it: cudaMalloc and cudaFree synchronize the device and can
+ * fail under memory pressure, so a caller that runs inside a real-time
+ * acquisition loop, or that owns all of its device memory through another
+ * allocator (a framework's caching allocator, an instrument vendor's SDK)
+ * and may not allocate outside it, cannot obtain a workspace for each call.
+ * This entry point takes the same inputs and outputs as lmb_fit_batch but
+ * no workspace: its scratch is a file-scope device array of
+ * LMB_FIT_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU which loads the
+ * library holds until the process exits.  It calls no cudaMalloc, cudaFree
+ * or other allocating routine and takes no stats.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  Requests whose lmb_fit_workspace_bytes
+ * exceed LMB_FIT_NOALLOC_SCRATCH_BYTES are rejected with
+ * LMB_ERR_WORKSPACE before anything is launched (about 700 features of
+ * 201x201 pixels fit at the capacity a 0.75 um sphere needs).  All calls share the one array, which keeps the
+ * last call's contents; the fit re-initializes every counter, state and
+ * table it reads, and the counters are zeroed again at each call.  Calls
+ * from this process are serialized by a lock, but calls whose work could
+ * overlap on the GPU (for example from another thread that bypasses this
+ * entry point's return) would race on the array.
+ */
+#define LMB_FIT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int lmb_fit_batch_noalloc(const lmb_feature *features, int nfeatures,
+                          long long total_pixels, const float *data,
+                          const float *coords, lmb_sphere *params,
+                          double n_m, double wavelength, double magnification,
+                          double noise, int nmax_cap,
+                          const lmb_fit_settings *settings,
+                          lmb_fit_result *results, void *stream);
+
+/*
  * Measured FP32 fused-multiply-add throughput of the current device in
  * FLOP/s (2 per FMA), for roofline reporting.  Runs a short kernel.
  */

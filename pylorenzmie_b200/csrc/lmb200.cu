@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "lmb200.h"
@@ -438,4 +439,62 @@ extern "C" int lmb_measure_fp32_peak(double* flops, void* stream) {
   LMB_CK(cudaGetLastError());
   *flops = best;
   return best > 0. ? LMB_OK : LMB_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// lmb_fit_batch_noalloc: the batched fit with its scratch in a static device
+// array instead of a caller workspace, for callers that cannot allocate
+// device memory (declaration and contract in include/lmb200.h).
+
+namespace {
+
+static __device__ __align__(256) unsigned char
+    g_fit_scratch[LMB_FIT_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_lock;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_fit_scratch on the current device, looked up once per
+// device (the host-side symbol is not a device address).
+int scratch_address(void** out) {
+  int dev = -1;
+  LMB_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return LMB_ERR_ARG;
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    LMB_CK(cudaGetSymbolAddress(&p, g_fit_scratch));
+    if (!p) return LMB_ERR_CUDA;
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" int lmb_fit_batch_noalloc(const lmb_feature* features, int nfeatures,
+                                     long long total_pixels, const float* data,
+                                     const float* coords, lmb_sphere* params,
+                                     double n_m, double wavelength,
+                                     double magnification, double noise,
+                                     int nmax_cap,
+                                     const lmb_fit_settings* settings,
+                                     lmb_fit_result* results, void* stream) {
+  if (nfeatures < 0 || total_pixels < 0 || bad_cap(nmax_cap) || !settings)
+    return LMB_ERR_ARG;
+  std::lock_guard<std::mutex> hold(g_noalloc_lock);
+  void* scratch = nullptr;
+  const int st = scratch_address(&scratch);
+  if (st != LMB_OK) return st;
+  if (nfeatures == 0) return LMB_OK;
+  const FitLayout L = fit_layout(nfeatures, total_pixels, nmax_cap);
+  if (L.total > size_t(LMB_FIT_NOALLOC_SCRATCH_BYTES)) return LMB_ERR_WORKSPACE;
+  // counters must start at zero; the setup kernel writes them too
+  LMB_CK(cudaMemsetAsync(reinterpret_cast<char*>(scratch) + L.counters, 0,
+                         sizeof(int) * 16, as_stream(stream)));
+  return lmb_fit_batch(features, nfeatures, total_pixels, data, coords, params,
+                       n_m, wavelength, magnification, noise, nmax_cap,
+                       settings, results, scratch,
+                       size_t(LMB_FIT_NOALLOC_SCRATCH_BYTES), nullptr, stream);
 }
