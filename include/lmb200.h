@@ -163,7 +163,19 @@ typedef struct lmb_fit_settings {
   int variables;   /* bit j set = parameter j of (x_p,y_p,z_p,a_p,n_p,k_p) free */
   int flags;       /* LMB_BOHREN */
   int max_iterations; /* hard cap on evaluations per call, >= 1 */
+  int tile_config;    /* launch shape of the evaluation kernel, 0 = default;
+                         see lmb_fit_tile_config */
+  int reserved;
 } lmb_fit_settings;
+
+/*
+ * Launch shapes of the fit's evaluation kernel (threads per CTA, pixels per
+ * thread, minimum resident CTAs per SM), for lmb_fit_settings.tile_config.
+ * Returns LMB_ERR_ARG past the last index.  The autotuner of the Python
+ * package times them per problem class.
+ */
+int lmb_fit_tile_config(int index, int *threads, int *pixels_per_thread,
+                        int *min_blocks);
 
 /* Per-feature fit result (Optimizer.result, analysis/Optimizer.py:166-186). */
 typedef struct lmb_fit_result {

@@ -39,7 +39,8 @@ class FitSettings(ctypes.Structure):
     _fields_ = [('ftol', ctypes.c_double), ('xtol', ctypes.c_double),
                 ('gtol', ctypes.c_double), ('factor', ctypes.c_double),
                 ('max_nfev', ctypes.c_int), ('variables', ctypes.c_int),
-                ('flags', ctypes.c_int), ('max_iterations', ctypes.c_int)]
+                ('flags', ctypes.c_int), ('max_iterations', ctypes.c_int),
+                ('tile_config', ctypes.c_int), ('reserved', ctypes.c_int)]
 
 
 class FitStats(ctypes.Structure):
@@ -80,6 +81,8 @@ _SIGNATURES = {
     'lmb_hologram_vjp': (_i, [_vp, _ll, _vp, _i, _vp, _vp, _vp, _i, _d, _i,
                               _vp, _vp, _vp, _sz, _vp]),
     'lmb_fit_workspace_bytes': (_sz, [_i, _ll, _i]),
+    'lmb_fit_tile_config': (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i),
+                                 ctypes.POINTER(_i)]),
     'lmb_fit_batch': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _d, _d, _d, _d, _i,
                            ctypes.POINTER(FitSettings), _vp, _vp, _sz,
                            ctypes.POINTER(FitStats), _vp]),

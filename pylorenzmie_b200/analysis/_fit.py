@@ -35,17 +35,23 @@ def fit_capacity(starts, n_m, wavelength):
 
 class PackedFeatures:
     '''Crops packed for the device: float32 data, lmb_feature records and
-    optional float32 (x, y) coordinates for non-grid pixel sets.'''
+    optional float32 (x, y) coordinates for non-grid pixel sets.
+
+    The crops are not copied here: ``write_data`` converts them straight
+    into a destination buffer (the pinned staging buffer of ``upload``),
+    in parallel over features; ``data`` builds a host copy on demand.
+    '''
 
     def __init__(self, items):
-        '''items: list of (data (npix,) or (ny, nx), grid) where grid is
-        (x0, y0, ny, nx) or None with explicit coords (2, npix).'''
+        '''items: list of (data, grid, coords): data (npix,) or (ny, nx);
+        grid (x0, y0, ny, nx), or None with explicit coords (2, npix).'''
         feats = np.zeros(len(items), dtype=_native.FEATURE_DTYPE)
-        chunks, cchunks = [], []
+        self._sources = []
+        cchunks = []
         off = 0
         explicit = any(it[1] is None for it in items)
         for i, (data, grid, coords) in enumerate(items):
-            d = np.ascontiguousarray(np.ravel(data), dtype=np.float32)
+            d = np.asarray(data)
             n = d.size
             if grid is not None:
                 x0, y0, ny, nx = grid
@@ -54,7 +60,7 @@ class PackedFeatures:
                 feats[i] = (x0, y0, nx, ny, n, off)
             else:
                 feats[i] = (0., 0., 0, 0, n, off)
-            chunks.append(d)
+            self._sources.append(d)
             if explicit:
                 if grid is None:
                     c = np.asarray(coords, dtype=np.float32)[:2].T
@@ -66,22 +72,60 @@ class PackedFeatures:
                 cchunks.append(np.ascontiguousarray(c))
             off += n
         self.features = feats
-        self.data = (np.concatenate(chunks) if chunks
-                     else np.zeros(0, np.float32))
         self.coords = (np.concatenate(cchunks).reshape(-1)
                        if explicit and cchunks else None)
         self.total = off
+        self._data = None
+
+    def write_data(self, out):
+        '''Convert every crop into the float32 array ``out`` (total,).'''
+        offs = self.features['data_offset']
+
+        def work(lo, hi):
+            for i in range(lo, hi):
+                src = self._sources[i]
+                n = src.size
+                np.copyto(out[offs[i]:offs[i] + n], src.reshape(-1),
+                          casting='unsafe')
+        nf = len(self._sources)
+        pool = _pool()
+        if pool is None or self.total < (1 << 20) or nf < 4:
+            work(0, nf)
+            return out
+        nthreads = pool._max_workers
+        step = (nf + nthreads - 1) // nthreads
+        futs = [pool.submit(work, lo, min(lo + step, nf))
+                for lo in range(0, nf, step)]
+        for f in futs:
+            f.result()
+        return out
+
+    @property
+    def data(self):
+        if self._data is None:
+            self._data = self.write_data(np.empty(self.total, np.float32))
+        return self._data
 
     @property
     def h2d_bytes(self):
-        n = self.data.nbytes + self.features.nbytes
+        n = self.total * 4 + self.features.nbytes
         if self.coords is not None:
             n += self.coords.nbytes
         return n
 
 
-_TORCH_DTYPE = {'<f4': torch.float32, '<f8': torch.float64,
-                '|u1': torch.uint8, '<i4': torch.int32, '<i8': torch.int64}
+_POOL = None
+
+
+def _pool():
+    '''Thread pool for packing (numpy releases the GIL while copying).'''
+    global _POOL
+    if _POOL is None:
+        import os
+        from concurrent.futures import ThreadPoolExecutor
+        n = min(16, os.cpu_count() or 1)
+        _POOL = ThreadPoolExecutor(max_workers=n) if n > 1 else False
+    return _POOL or None
 
 
 class _Staging:
@@ -101,45 +145,42 @@ class _Staging:
 _staging = _Staging()
 
 
-def _to_device(arrays, dev):
-    '''Copy numpy arrays to the device through one pinned staging buffer
-    and one host-to-device transfer; returns device tensors (same dtypes).'''
-    arrays = [np.ascontiguousarray(a) for a in arrays]
-    sizes = [(a.nbytes + 255) // 256 * 256 for a in arrays]
+def upload(packed, starts, device=None):
+    '''Device copies of a packed batch: (features, data, coords, params).
+    The crops are converted to float32 directly into the pinned staging
+    buffer and everything crosses to the device in one copy.'''
+    dev = get_device(device)
+    starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
+    pieces = [packed.features.view(np.uint8), None, starts]
+    if packed.coords is not None:
+        pieces.append(packed.coords)
+    nbytes = [packed.features.nbytes, packed.total * 4, starts.nbytes]
+    if packed.coords is not None:
+        nbytes.append(packed.coords.nbytes)
+    sizes = [(n + 255) // 256 * 256 for n in nbytes]
     total = sum(sizes)
     stage = _staging.take(total)
     host = stage.numpy()
-    off = 0
-    for a, n in zip(arrays, sizes):
-        host[off:off + a.nbytes] = a.view(np.uint8).reshape(-1)
-        off += n
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    for k, a in enumerate(pieces):
+        if a is None:
+            packed.write_data(host[offs[k]:offs[k] + nbytes[k]].view(np.float32))
+        else:
+            host[offs[k]:offs[k] + nbytes[k]] = a.view(np.uint8).reshape(-1)
     dbuf = torch.empty(max(total, 1), dtype=torch.uint8, device=dev)
     dbuf[:total].copy_(stage[:total], non_blocking=True)
-    out, off = [], 0
-    for a, n in zip(arrays, sizes):
-        out.append(dbuf[off:off + a.nbytes].view(_TORCH_DTYPE[a.dtype.str]))
-        off += n
+    dtypes = [torch.uint8, torch.float32, torch.float64, torch.float32]
+    out = [dbuf[offs[k]:offs[k] + nbytes[k]].view(dtypes[k])
+           for k in range(len(pieces))]
     # the staging buffer is reused by the next call: wait for this copy
     torch.cuda.current_stream(dev).synchronize()
-    return out
-
-
-def upload(packed, starts, device=None):
-    '''Device copies of a packed batch: (features, data, coords, params).'''
-    dev = get_device(device)
-    starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
-    arrays = [packed.features.view(np.uint8), packed.data, starts]
-    if packed.coords is not None:
-        arrays.append(packed.coords)
-    t = _to_device(arrays, dev)
-    d_feat, d_data, d_params = t[0], t[1], t[2]
-    d_coords = t[3] if packed.coords is not None else None
-    return d_feat, d_data, d_coords, d_params
+    d_coords = out[3] if packed.coords is not None else None
+    return out[0], out[1], d_coords, out[2]
 
 
 def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
                instrument, variables, settings=None, nmax_cap=None,
-               starts_host=None, stats=False):
+               starts_host=None, stats=False, tile_config=0):
     '''Run lmb_fit_batch on device-resident inputs.  d_params is updated in
     place with the fitted values; returns (results tensor (B*80 uint8),
     FitStats or None).'''
@@ -165,6 +206,7 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
     st.variables = variable_mask(variables)
     st.flags = _native.LMB_BOHREN
     st.max_iterations = st.max_nfev
+    st.tile_config = int(tile_config)
     fs = _native.FitStats() if stats else None
     _native.check(lib.lmb_fit_batch(
         ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),

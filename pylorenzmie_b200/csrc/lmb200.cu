@@ -33,14 +33,30 @@ inline cudaError_t smem_attr(const void* fn, size_t bytes) {
 
 inline bool bad_cap(int nmax_cap) { return nmax_cap < 1 || nmax_cap > LMB_NMAX_LIMIT; }
 
-// Fit-evaluation launch shape: TPB threads, PPT pixels per thread.
-constexpr int kFitTPB = 128;
-constexpr int kFitPPT = 4;
-constexpr int kFitTile = kFitTPB * kFitPPT;
+// Fit-evaluation launch shapes: TPB threads, PPT pixels per thread and a
+// minimum of MINB resident CTAs per SM (which caps registers per thread).
+// Every shape covers a 512-pixel tile, so the tile table and the workspace
+// do not depend on the choice.  Index 0 is the default.
+constexpr int kFitTile = 512;
+struct EvalShape {
+  int tpb, ppt, minb;
+  void (*fn)(FitCtx);
+};
+const EvalShape kEvalShapes[] = {
+    {128, 4, 4, k_fit_eval<128, 4, 4>},
+    {128, 4, 5, k_fit_eval<128, 4, 5>},
+    {128, 4, 6, k_fit_eval<128, 4, 6>},
+    {256, 2, 2, k_fit_eval<256, 2, 2>},
+    {256, 2, 3, k_fit_eval<256, 2, 3>},
+    {64, 8, 8, k_fit_eval<64, 8, 8>},
+    {64, 8, 10, k_fit_eval<64, 8, 10>},
+    {512, 1, 1, k_fit_eval<512, 1, 1>},
+};
+constexpr int kNumEvalShapes = int(sizeof(kEvalShapes) / sizeof(kEvalShapes[0]));
 
 struct FitLayout {
-  size_t state, ev, base, ab, dab, nmax, tile_begin, tiles, partial, counters,
-      total;
+  size_t state, ev, base, ab, dab, coef32, nmax, tile_begin, tiles, partial,
+      counters, total;
   int max_tiles;
 };
 
@@ -62,6 +78,7 @@ FitLayout fit_layout(int nf, long long total_pixels, int nmax_cap) {
   L.base = take(sizeof(double) * 6 * nf);
   L.ab = take(sizeof(zd) * 2 * nmaxp * nf);
   L.dab = take(sizeof(zd) * 4 * nmaxp * nf);
+  L.coef32 = take(sizeof(Quad<float>) * 4 * nmaxp * nf);
   L.nmax = take(sizeof(int) * nf);
   L.tile_begin = take(sizeof(int) * (nf + 1));
   L.tiles = take(sizeof(int2) * size_t(L.max_tiles));
@@ -235,6 +252,15 @@ int lmb_hologram_vjp(const double* coords, long long npts,
   return LMB_OK;
 }
 
+int lmb_fit_tile_config(int index, int* threads, int* pixels_per_thread,
+                        int* min_blocks) {
+  if (index < 0 || index >= kNumEvalShapes) return LMB_ERR_ARG;
+  if (threads) *threads = kEvalShapes[index].tpb;
+  if (pixels_per_thread) *pixels_per_thread = kEvalShapes[index].ppt;
+  if (min_blocks) *min_blocks = kEvalShapes[index].minb;
+  return LMB_OK;
+}
+
 size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
                                int nmax_cap) {
   if (nfeatures <= 0 || total_pixels < 0 || bad_cap(nmax_cap)) return 0;
@@ -270,6 +296,7 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
   c.base = reinterpret_cast<double*>(ws + L.base);
   c.ab = reinterpret_cast<zd*>(ws + L.ab);
   c.dab = reinterpret_cast<zd*>(ws + L.dab);
+  c.coef32 = reinterpret_cast<Quad<float>*>(ws + L.coef32);
   c.nmax = reinterpret_cast<int*>(ws + L.nmax);
   c.tile_begin = reinterpret_cast<int*>(ws + L.tile_begin);
   c.tiles = reinterpret_cast<int2*>(ws + L.tiles);
@@ -301,10 +328,13 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
 
   const size_t ab_smem = ab_scratch_bytes(nmax_cap + 1);
   const size_t coef_smem = sizeof(Quad<float>) * 4 * (size_t(nmax_cap) + 1);
-  auto eval = k_fit_eval<kFitTPB, kFitPPT>;
+  const int shape_index = settings->tile_config;
+  if (shape_index < 0 || shape_index >= kNumEvalShapes) return LMB_ERR_ARG;
+  const EvalShape shape = kEvalShapes[shape_index];
+  auto eval = shape.fn;
   LMB_CK(smem_attr((const void*)k_fit_step, ab_smem));
   LMB_CK(smem_attr((const void*)eval, coef_smem));
-  const int egrid = persistent_grid((const void*)eval, kFitTPB, coef_smem);
+  const int egrid = persistent_grid((const void*)eval, shape.tpb, coef_smem);
 
   // Optional timing: one event pair per evaluation launch, plus the span.
   std::vector<cudaEvent_t> ev;
@@ -333,7 +363,7 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
         break;
       }
       if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-      eval<<<egrid, kFitTPB, coef_smem, st>>>(c);
+      eval<<<egrid, shape.tpb, coef_smem, st>>>(c);
       if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
       cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
       k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);

@@ -350,6 +350,7 @@ struct FitCtx {
   double* base;        // [nf][6] start values (fixed parameters keep them)
   zd* ab;              // [nf][nmaxp][2]
   zd* dab;             // [nf][nmaxp][4]
+  Quad<float>* coef32; // [nf][nmaxp][4] FP32 per-order records of the eval point
   int* nmax;           // [nf]
   int* tile_begin;     // [nf+1]
   int2* tiles;         // [max_tiles]
@@ -441,8 +442,8 @@ __global__ void k_fit_setup(FitCtx c) {
 }
 
 // Evaluation: persistent CTAs pull tiles from an atomic queue.
-template <int TPB, int PPT>
-__global__ void __launch_bounds__(TPB)
+template <int TPB, int PPT, int MINB>
+__global__ void __launch_bounds__(TPB, MINB)
 k_fit_eval(FitCtx c) {
   extern __shared__ __align__(16) char smem[];
   Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem);
@@ -465,8 +466,11 @@ k_fit_eval(FitCtx c) {
       continue;
     }
     const int nm = min(max(c.nmax[f], 0), nmaxp - 1);
-    stage_coef<float, true>(c.ab + size_t(f) * nmaxp * 2,
-                            c.dab + size_t(f) * nmaxp * 4, nm, coef);
+    {
+      const float4* src = reinterpret_cast<const float4*>(c.coef32 + size_t(f) * nmaxp * 4);
+      float4* dst = reinterpret_cast<float4*>(coef);
+      for (int i = threadIdx.x; i < 4 * (nm + 1); i += TPB) dst[i] = src[i];
+    }
     const lmb_feature ft = c.features[f];
     const EvalPoint ep = c.ev[f];
     __syncthreads();
@@ -574,6 +578,11 @@ k_fit_step(FitCtx c) {
   const int st = warp_sphere_ab(s_p[3], s_p[4], s_p[5], c.n_m, c.wavelength,
                                 c.nmax_cap, w, c.ab + size_t(f) * nmaxp * 2,
                                 c.dab + size_t(f) * nmaxp * 4, c.nmax + f);
+  if (st == LMB_OK)
+    stage_coef<float, true>(c.ab + size_t(f) * nmaxp * 2,
+                            c.dab + size_t(f) * nmaxp * 4,
+                            min(c.nmax[f], nmaxp - 1),
+                            c.coef32 + size_t(f) * nmaxp * 4);
   if (lane == 0) {
     if (st != LMB_OK) {
       gs->phase = LM_PHASE_DONE;
