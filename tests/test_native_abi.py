@@ -57,7 +57,7 @@ def test_struct_layouts():
     assert _native.SPHERE_DTYPE.itemsize == 48
     assert _native.FEATURE_DTYPE.itemsize == 40
     assert _native.RESULT_DTYPE.itemsize == 80
-    assert ctypes.sizeof(_native.FitSettings) == 48
+    assert ctypes.sizeof(_native.FitSettings) == 56
     assert ctypes.sizeof(_native.FitStats) == 48
 
 
