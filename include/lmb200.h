@@ -237,6 +237,29 @@ int lmb_fit_batch(const lmb_feature *features, int nfeatures,
                   size_t workspace_bytes, lmb_fit_stats *stats, void *stream);
 
 /*
+ * lmb_fit_batch for multilayer (core-shell) spheres: the free parameters
+ * are the outer radius a_p and the outer layer's index n_p + i k_p (with
+ * the position); every inner radius keeps its fraction of a_p.  Layered
+ * particles have no live fitting path in the reference (their coefficients
+ * are lib/obsolete/sphere_coefficients.py:65-220).
+ *   nlayers          layers per sphere (1..8; 1 = lmb_fit_batch)
+ *   layer_fractions  [nfeatures][nlayers-1] inner radii / a_p, ascending
+ *   layer_indices    [nfeatures][nlayers-1][2] inner layer indices (re, im)
+ * Workspace: lmb_fit_workspace_bytes as for lmb_fit_batch.
+ */
+int lmb_fit_batch_layered(const lmb_feature *features, int nfeatures,
+                          long long total_pixels, const float *data,
+                          const float *coords, lmb_sphere *params, int nlayers,
+                          const double *layer_fractions,
+                          const double *layer_indices, double n_m,
+                          double wavelength, double magnification,
+                          double noise, int nmax_cap,
+                          const lmb_fit_settings *settings,
+                          lmb_fit_result *results, void *workspace,
+                          size_t workspace_bytes, lmb_fit_stats *stats,
+                          void *stream);
+
+/*
  * lmb_fit_batch for callers that cannot allocate device memory.  No
  * counterpart in the reference (its fits run on the host).
  *

@@ -39,7 +39,9 @@ def fit(data, coordinates, particle, instrument, variables=DEFAULT_VARIABLES,
     '''One LM fit; returns a dict shaped like ``Optimizer.result``.
 
     ``data``: (npts,) normalized intensities; ``coordinates``: (2|3, npts);
-    ``particle``: dict with the six particle keys (start values);
+    ``particle``: dict with the six particle keys (start values), plus
+    'fractions' and 'core_indices' for a multilayer sphere whose inner radii
+    keep their fractions of the fitted outer radius a_p;
     ``instrument``: dict with n_m, wavelength, magnification, noise.
     ``jac``: optional callable p -> (npts, nvar) dH/dp (not divided by
     noise), standing in for the analytic-Jacobian slot
@@ -53,6 +55,11 @@ def fit(data, coordinates, particle, instrument, variables=DEFAULT_VARIABLES,
     def params(values):
         p = dict(base)
         p.update(zip(variables, values))
+        if 'fractions' in p:  # multilayer: outer radius and index vary
+            frac = np.asarray(p['fractions'], dtype=float)
+            p['layers'] = (np.append(frac * p['a_p'], p['a_p']),
+                           np.append(np.asarray(p['core_indices'], complex),
+                                     p['n_p'] + 1j * p.get('k_p', 0.)))
         return p
 
     def residuals(values):

@@ -8,5 +8,6 @@ reference interface.  Importing the package does not touch the GPU.
 __version__ = '0.1.0'
 
 from .lib import meshgrid, LMObject  # noqa: F401
-from .theory import Particle, Sphere, Instrument, LorenzMie  # noqa: F401
+from .theory import (Particle, Sphere, LayeredSphere, Instrument,  # noqa: F401
+                     LorenzMie)
 from .analysis import Hologram, Mask, Optimizer  # noqa: F401

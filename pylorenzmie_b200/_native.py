@@ -81,6 +81,10 @@ _SIGNATURES = {
     'lmb_hologram_vjp': (_i, [_vp, _ll, _vp, _i, _vp, _vp, _vp, _i, _d, _i,
                               _vp, _vp, _vp, _sz, _vp]),
     'lmb_fit_workspace_bytes': (_sz, [_i, _ll, _i]),
+    'lmb_fit_batch_layered': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _i, _vp, _vp,
+                                   _d, _d, _d, _d, _i,
+                                   ctypes.POINTER(FitSettings), _vp, _vp, _sz,
+                                   ctypes.POINTER(FitStats), _vp]),
     'lmb_fit_tile_config': (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i),
                                  ctypes.POINTER(_i)]),
     'lmb_fit_batch': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _d, _d, _d, _d, _i,

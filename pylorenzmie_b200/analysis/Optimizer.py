@@ -193,7 +193,8 @@ class Optimizer(LMObject):
                            getattr(part, 'k_p', 0.)]])
         params, res = _fit.fit_packed(packed, start, self.model.instrument,
                                       self.variables, self.settings,
-                                      device=self.model.device)
+                                      device=self.model.device,
+                                      layers=_fit.layers_of([part]))
         status = int(res['status'][0])
         if status == -1:
             raise ValueError("Method 'lm' doesn't work when the number of "
@@ -266,14 +267,20 @@ class Optimizer(LMObject):
         '''Fit one sphere per hologram, all on the device in one call.
 
         holograms : list of Hologram (crops; any sizes)
-        particles : list of Sphere start values, or
-        starts    : array (B, 6) of x_p, y_p, z_p, a_p, n_p, k_p
+        particles : list of Sphere (or LayeredSphere, one layer count)
+                    start values; the layer structure of layered spheres
+                    is kept, their outer radius and index are fitted
+        starts    : array (B, 6) of x_p, y_p, z_p, a_p, n_p, k_p (overrides
+                    the particles' start values)
         Returns a DataFrame, one row per feature, with the columns of
         ``result`` plus ``status`` and ``nfev``.
         '''
         if not self._device_fit_ok() and not (
                 set(self.variables) <= set(PARAM_KEYS)):
             raise ValueError('optimize_batch fits sphere parameters only')
+        layers = None
+        if particles is not None:
+            layers = _fit.layers_of(list(particles))
         if starts is None:
             if particles is None:
                 raise ValueError('give particles or starts')
@@ -284,7 +291,7 @@ class Optimizer(LMObject):
         packed = _fit.PackedFeatures(items)
         params, res = _fit.fit_packed(packed, starts, self.model.instrument,
                                       self.variables, self.settings,
-                                      device=self.model.device)
+                                      device=self.model.device, layers=layers)
         return batch_frame(params, res, packed, self.variables)
 
 

@@ -24,13 +24,39 @@ def variable_mask(variables):
     return mask
 
 
-def fit_capacity(starts, n_m, wavelength):
+def fit_capacity(starts, n_m, wavelength, layers=None):
     '''Partial-wave capacity for fits that start at ``starts`` (B, 6): room
     for a_p to grow 25 % and n_p by 0.25 during the fit.'''
     a = starts[:, 3] * 1.25
     n = starts[:, 4] + 0.25
     k = starts[:, 5]
-    return K.nmax_cap_for(a, n, k, n_m, wavelength, margin=4)
+    if layers is None:
+        return K.nmax_cap_for(a, n, k, n_m, wavelength, margin=4)
+    _, frac, idx = layers
+    best = 0
+    for i in range(starts.shape[0]):
+        radii = np.append(frac[i] * a[i], a[i])
+        ind = np.append(idx[i], n[i] + 1j * k[i])
+        best = max(best, K.wiscombe_yang_layers(radii, ind, n_m, wavelength))
+    cap = best + 4
+    if cap > _native.LMB_NMAX_LIMIT:
+        raise ValueError(f'a sphere needs {best} partial-wave orders; the '
+                         f'limit is {_native.LMB_NMAX_LIMIT}')
+    return cap
+
+
+def layers_of(particles):
+    '''(nlayers, fractions (B, L-1), inner indices (B, L-1) complex) of a
+    list of LayeredSphere particles with one layer count, or None.'''
+    if not particles or not K.is_layered(particles[0]):
+        return None
+    L = particles[0].nlayers
+    if any(not K.is_layered(p) or p.nlayers != L for p in particles):
+        raise ValueError('a batch fits spheres with one layer count')
+    frac = np.array([p.fractions for p in particles], dtype=float)
+    idx = np.array([p.core_indices for p in particles], dtype=complex)
+    return L, frac.reshape(len(particles), L - 1), \
+        idx.reshape(len(particles), L - 1)
 
 
 class PackedFeatures:
@@ -180,7 +206,7 @@ def upload(packed, starts, device=None):
 
 def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
                instrument, variables, settings=None, nmax_cap=None,
-               starts_host=None, stats=False, tile_config=0):
+               starts_host=None, stats=False, tile_config=0, layers=None):
     '''Run lmb_fit_batch on device-resident inputs.  d_params is updated in
     place with the fitted values; returns (results tensor (B*80 uint8),
     FitStats or None).'''
@@ -208,16 +234,31 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
     st.max_iterations = st.max_nfev
     st.tile_config = int(tile_config)
     fs = _native.FitStats() if stats else None
-    _native.check(lib.lmb_fit_batch(
+    if layers is None:
+        _native.check(lib.lmb_fit_batch(
+            ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
+            ptr(d_params), n_m, lam, float(instrument.magnification),
+            float(instrument.noise), nmax_cap, st, ptr(d_res), ptr(ws),
+            nbytes, fs, stream_handle(dev)), 'lmb_fit_batch')
+        return d_res, fs
+    L, frac, idx = layers
+    d_frac = torch.from_numpy(np.ascontiguousarray(frac, dtype=np.float64)
+                              ).to(dev)
+    ind = np.zeros((nfeatures, L - 1, 2))
+    ind[..., 0] = np.real(idx)
+    ind[..., 1] = np.imag(idx)
+    d_ind = torch.from_numpy(ind).to(dev)
+    _native.check(lib.lmb_fit_batch_layered(
         ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
-        ptr(d_params), n_m, lam, float(instrument.magnification),
-        float(instrument.noise), nmax_cap, st, ptr(d_res), ptr(ws), nbytes,
-        fs, stream_handle(dev)), 'lmb_fit_batch')
+        ptr(d_params), L, ptr(d_frac), ptr(d_ind), n_m, lam,
+        float(instrument.magnification), float(instrument.noise), nmax_cap,
+        st, ptr(d_res), ptr(ws), nbytes, fs, stream_handle(dev)),
+        'lmb_fit_batch_layered')
     return d_res, fs
 
 
 def fit_packed(packed, starts, instrument, variables, settings=None,
-               device=None, nmax_cap=None, stats=False):
+               device=None, nmax_cap=None, stats=False, layers=None):
     '''Fit every packed feature; returns (params (B, 6), results record
     array with dparams, redchi, cost, status, success, nfev, njev) and,
     when stats, the FitStats of the call.'''
@@ -229,10 +270,10 @@ def fit_packed(packed, starts, instrument, variables, settings=None,
     d_feat, d_data, d_coords, d_params = upload(packed, starts, device)
     if nmax_cap is None:
         nmax_cap = fit_capacity(starts, float(instrument.n_m),
-                                float(instrument.wavelength))
+                                float(instrument.wavelength), layers)
     d_res, fs = fit_device(d_feat, d_data, d_coords, d_params, B,
                            packed.total, instrument, variables, settings,
-                           nmax_cap, starts, stats)
+                           nmax_cap, starts, stats, layers=layers)
     params = d_params.view(torch.float64).reshape(B, 6).cpu().numpy()
     res = d_res[:B * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
         _native.RESULT_DTYPE).copy()

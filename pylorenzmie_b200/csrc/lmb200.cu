@@ -172,10 +172,18 @@ int lmb_layered_ab(const double* radii, const double* indices, int nlayers,
                    int nspheres, double n_m, double wavelength, int nmax_cap,
                    double* ab, double* dab, int* nmax, int* status,
                    void* stream) {
-  (void)radii; (void)indices; (void)nlayers; (void)nspheres; (void)n_m;
-  (void)wavelength; (void)nmax_cap; (void)ab; (void)dab; (void)nmax;
-  (void)status; (void)stream;
-  return LMB_ERR_UNSUPPORTED;
+  if (nspheres < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
+  if (nlayers < 1 || nlayers > LMB_MAX_LAYERS) return LMB_ERR_ARG;
+  if (nspheres == 0) return LMB_OK;
+  if (!radii || !indices || !ab || !nmax || !status) return LMB_ERR_ARG;
+  if (!(wavelength > 0.) || !(n_m > 0.)) return LMB_ERR_ARG;
+  const size_t smem = layered_scratch_bytes(nmax_cap + 1);
+  LMB_CK(smem_attr((const void*)k_layered_ab, smem));
+  k_layered_ab<<<nspheres, 32, smem, as_stream(stream)>>>(
+      radii, indices, nlayers, nspheres, n_m, wavelength, nmax_cap,
+      reinterpret_cast<zd*>(ab), reinterpret_cast<zd*>(dab), nmax, status);
+  LMB_CK(cudaGetLastError());
+  return LMB_OK;
 }
 
 int lmb_field(const double* coords, long long npts, const lmb_sphere* spheres,
@@ -267,13 +275,22 @@ size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
   return fit_layout(nfeatures, total_pixels, nmax_cap).total;
 }
 
-int lmb_fit_batch(const lmb_feature* features, int nfeatures,
-                  long long total_pixels, const float* data,
-                  const float* coords, lmb_sphere* params, double n_m,
-                  double wavelength, double magnification, double noise,
-                  int nmax_cap, const lmb_fit_settings* settings,
-                  lmb_fit_result* results, void* workspace,
-                  size_t workspace_bytes, lmb_fit_stats* stats, void* stream) {
+}  // extern "C"
+
+namespace {
+
+int fit_batch_impl(const lmb_feature* features, int nfeatures,
+                   long long total_pixels, const float* data,
+                   const float* coords, lmb_sphere* params, double n_m,
+                   double wavelength, double magnification, double noise,
+                   int nmax_cap, const lmb_fit_settings* settings,
+                   lmb_fit_result* results, void* workspace,
+                   size_t workspace_bytes, lmb_fit_stats* stats, void* stream,
+                   int nlayers, const double* layer_frac,
+                   const double* layer_index) {
+  if (nlayers < 1 || nlayers > LMB_MAX_LAYERS) return LMB_ERR_ARG;
+  if (nlayers > 1 && nfeatures > 0 && (!layer_frac || !layer_index))
+    return LMB_ERR_ARG;
   if (nfeatures < 0 || total_pixels < 0 || bad_cap(nmax_cap) || !settings)
     return LMB_ERR_ARG;
   if (nfeatures == 0) return LMB_OK;
@@ -304,6 +321,9 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
   c.counters = reinterpret_cast<int*>(ws + L.counters);
   c.work = reinterpret_cast<unsigned long long*>(ws + L.counters + 8 * sizeof(int));
   c.total_pixels = total_pixels;
+  c.nlayers = nlayers;
+  c.layer_frac = layer_frac;
+  c.layer_index = layer_index;
   c.nf = nfeatures;
   c.nmax_cap = nmax_cap;
   c.max_tiles = L.max_tiles;
@@ -326,7 +346,8 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
   c.max_iterations = settings->max_iterations > 0 ? settings->max_iterations : 1;
   if (c.max_iterations > c.set.maxfev) c.max_iterations = c.set.maxfev;
 
-  const size_t ab_smem = ab_scratch_bytes(nmax_cap + 1);
+  const size_t ab_smem = nlayers > 1 ? layered_scratch_bytes(nmax_cap + 1)
+                                     : ab_scratch_bytes(nmax_cap + 1);
   const size_t coef_smem = sizeof(Quad<float>) * 4 * (size_t(nmax_cap) + 1);
   const int shape_index = settings->tile_config;
   if (shape_index < 0 || shape_index >= kNumEvalShapes) return LMB_ERR_ARG;
@@ -418,6 +439,40 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
   release();
   if (status != LMB_OK) return status;
   return overflow ? LMB_ERR_WORKSPACE : LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lmb_fit_batch(const lmb_feature* features, int nfeatures,
+                  long long total_pixels, const float* data,
+                  const float* coords, lmb_sphere* params, double n_m,
+                  double wavelength, double magnification, double noise,
+                  int nmax_cap, const lmb_fit_settings* settings,
+                  lmb_fit_result* results, void* workspace,
+                  size_t workspace_bytes, lmb_fit_stats* stats, void* stream) {
+  return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
+                        n_m, wavelength, magnification, noise, nmax_cap,
+                        settings, results, workspace, workspace_bytes, stats,
+                        stream, 1, nullptr, nullptr);
+}
+
+int lmb_fit_batch_layered(const lmb_feature* features, int nfeatures,
+                          long long total_pixels, const float* data,
+                          const float* coords, lmb_sphere* params, int nlayers,
+                          const double* layer_fractions,
+                          const double* layer_indices, double n_m,
+                          double wavelength, double magnification,
+                          double noise, int nmax_cap,
+                          const lmb_fit_settings* settings,
+                          lmb_fit_result* results, void* workspace,
+                          size_t workspace_bytes, lmb_fit_stats* stats,
+                          void* stream) {
+  return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
+                        n_m, wavelength, magnification, noise, nmax_cap,
+                        settings, results, workspace, workspace_bytes, stats,
+                        stream, nlayers, layer_fractions, layer_indices);
 }
 
 }  // extern "C"

@@ -17,6 +17,7 @@
 #include <stdint.h>
 
 #include "lmb200.h"
+#include "lmb_layered.cuh"
 #include "lmb_lm.cuh"
 #include "lmb_mie.cuh"
 #include "lmb_pixel.cuh"
@@ -105,6 +106,107 @@ __global__ void k_sphere_ab(const lmb_sphere* spheres, int n, double n_m,
                                 nmax_cap, w, ab + size_t(i) * nmaxp * 2,
                                 dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
                                 nmax + i);
+  if (threadIdx.x == 0) status[i] = st;
+}
+
+// ---------------------------------------------------------------------------
+// Multilayer spheres: one warp per sphere.  Lane 0 runs the core and the
+// shells' upward recurrences, lanes 0/1 the two downward D1 recurrences of
+// each shell, lane 1 the medium's recurrences meanwhile; then all lanes form
+// a_n, b_n over n.
+
+__host__ __device__ inline size_t layered_scratch_bytes(int nmaxp) {
+  return 4 * size_t(nmaxp + 1) * sizeof(dz) + ab_scratch_bytes(nmaxp);
+}
+
+// radii [L] ascending (um), idx [L][2] (re, im), core first.
+__device__ int warp_layered_ab(const double* radii, const double* idx, int L,
+                               double n_m, double wavelength, int nmax_cap,
+                               char* scratch, zd* ab, zd* dab, int* nmax_out) {
+  const int lane = threadIdx.x & 31;
+  const int nmaxp = nmax_cap + 1;
+  bool ok = L >= 1 && L <= LMB_MAX_LAYERS;
+  for (int l = 0; ok && l < L; ++l)
+    ok = radii[l] > 0. && (l == 0 || radii[l] > radii[l - 1]) &&
+         isfinite(idx[2 * l]) && isfinite(idx[2 * l + 1]);
+  LayeredScalars s;
+  if (ok) {
+    s = layered_setup(radii, idx, L, n_m, wavelength);
+    ok = s.nmax >= 1 && s.nmax <= nmax_cap && s.x[L - 1] < 1e7;
+  }
+  if (!ok) {
+    for (int n = lane; n < nmaxp; n += 32) {
+      ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
+      if (dab)
+        for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
+    }
+    if (lane == 0) *nmax_out = 0;
+    __syncwarp();
+    return LMB_ERR_NMAX;
+  }
+  dz* d1a = reinterpret_cast<dz*>(scratch);
+  dz* d1b = d1a + (nmaxp + 1);
+  dz* ha = d1b + (nmaxp + 1);
+  dz* hb = ha + (nmaxp + 1);
+  AbScratch w = carve_ab_scratch(reinterpret_cast<char*>(hb + (nmaxp + 1)), nmaxp);
+  MieScalars med;
+  med.k = s.k;
+  med.x = s.x[L - 1];
+  med.n_m = n_m;
+  med.m = s.m[L - 1];
+  med.nmax = s.nmax;
+  if (lane == 0) layered_core(s, d1a, ha, hb);
+  if (lane == 1) {
+    mie_d1_medium(med, w.d1m, w.d1mx);
+    mie_upward(med, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+  }
+  __syncwarp();
+  for (int ii = 1; ii < L; ++ii) {
+    const bool outer = ii == L - 1;
+    if (lane < 2) {
+      dz z;
+      const double xx = lane == 0 ? s.x[ii] : s.x[ii - 1];
+      z.v = xx * s.m[ii];
+      z.s = z.v;
+      z.m = outer ? mk(xx, 0.) : mk(0., 0.);
+      layered_d1_down(z, s.nmax, lane == 0 ? d1a : d1b);
+    }
+    __syncwarp();
+    if (lane == 0) layered_shell_up(s, ii, d1a, d1b, ha, hb);
+    __syncwarp();
+  }
+  for (int n = lane; n < nmaxp; n += 32) {
+    if (n == 0 || n > s.nmax) {
+      ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
+      if (dab)
+        for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
+      continue;
+    }
+    zd out[2], dout[4];
+    layered_coefficient(s, n, ha[n], hb[n], w.psi, w.psix, w.zeta, w.zetax, out,
+                        dab ? dout : (zd*)0);
+    ab[2 * n] = out[0];
+    ab[2 * n + 1] = out[1];
+    if (dab)
+      for (int j = 0; j < 4; ++j) dab[4 * n + j] = dout[j];
+  }
+  if (lane == 0) *nmax_out = s.nmax;
+  __syncwarp();
+  return LMB_OK;
+}
+
+__global__ void k_layered_ab(const double* radii, const double* indices, int L,
+                             int n, double n_m, double wavelength, int nmax_cap,
+                             zd* ab, zd* dab, int* nmax, int* status) {
+  extern __shared__ __align__(16) char smem[];
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const int nmaxp = nmax_cap + 1;
+  const int st = warp_layered_ab(radii + size_t(i) * L, indices + size_t(i) * L * 2,
+                                 L, n_m, wavelength, nmax_cap, smem,
+                                 ab + size_t(i) * nmaxp * 2,
+                                 dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
+                                 nmax + i);
   if (threadIdx.x == 0) status[i] = st;
 }
 
@@ -359,6 +461,9 @@ struct FitCtx {
   unsigned long long* work;  // [0] pixels, [1] pixel-orders evaluated
   long long total_pixels;
   int nf, nmax_cap, max_tiles, tile_pixels;
+  int nlayers;                // 1: homogeneous spheres
+  const double* layer_frac;   // [nf][nlayers-1] inner radii / outer radius
+  const double* layer_index;  // [nf][nlayers-1][2] inner layer indices
   double n_m, wavelength, k, inv_noise;
   LMSettings set;
   int variables, flags, max_iterations;
@@ -574,10 +679,27 @@ k_fit_step(FitCtx c) {
   }
   __syncwarp();
   if (!s_need) return;
-  AbScratch w = carve_ab_scratch(smem, nmaxp);
-  const int st = warp_sphere_ab(s_p[3], s_p[4], s_p[5], c.n_m, c.wavelength,
-                                c.nmax_cap, w, c.ab + size_t(f) * nmaxp * 2,
-                                c.dab + size_t(f) * nmaxp * 4, c.nmax + f);
+  int st;
+  if (c.nlayers > 1) {
+    __shared__ double s_r[LMB_MAX_LAYERS], s_i[2 * LMB_MAX_LAYERS];
+    const int L = c.nlayers;
+    if (lane < L) {
+      const bool outer = lane == L - 1;
+      s_r[lane] = outer ? s_p[3] : c.layer_frac[size_t(f) * (L - 1) + lane] * s_p[3];
+      s_i[2 * lane] = outer ? s_p[4] : c.layer_index[(size_t(f) * (L - 1) + lane) * 2];
+      s_i[2 * lane + 1] =
+          outer ? s_p[5] : c.layer_index[(size_t(f) * (L - 1) + lane) * 2 + 1];
+    }
+    __syncwarp();
+    st = warp_layered_ab(s_r, s_i, L, c.n_m, c.wavelength, c.nmax_cap, smem,
+                         c.ab + size_t(f) * nmaxp * 2, c.dab + size_t(f) * nmaxp * 4,
+                         c.nmax + f);
+  } else {
+    AbScratch w = carve_ab_scratch(smem, nmaxp);
+    st = warp_sphere_ab(s_p[3], s_p[4], s_p[5], c.n_m, c.wavelength, c.nmax_cap,
+                        w, c.ab + size_t(f) * nmaxp * 2, c.dab + size_t(f) * nmaxp * 4,
+                        c.nmax + f);
+  }
   if (st == LMB_OK)
     stage_coef<float, true>(c.ab + size_t(f) * nmaxp * 2,
                             c.dab + size_t(f) * nmaxp * 4,

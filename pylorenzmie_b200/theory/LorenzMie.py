@@ -136,12 +136,16 @@ class LorenzMie(LMObject):
         if len(flat) == 0:
             cap = 1
         else:
-            cap = K.nmax_cap_for(rec['a_p'], rec['n_p'], rec['k_p'], inst.n_m,
-                                 inst.wavelength)
+            cap = max(K.particle_nmax(p, inst.n_m, inst.wavelength)
+                      for p in flat) + 2
+            if cap > K._native.LMB_NMAX_LIMIT:
+                raise ValueError(f'a particle needs {cap - 2} partial-wave '
+                                 f'orders; the limit is '
+                                 f'{K._native.LMB_NMAX_LIMIT}')
         sp = K.spheres_tensor(rec, self.device)
         if len(flat):
-            ab, dab, nmax = K.sphere_ab(sp, inst.n_m, inst.wavelength, cap,
-                                        deriv)
+            ab, dab, nmax = K.particle_ab(flat, sp, inst.n_m,
+                                          inst.wavelength, cap, deriv)
         else:
             ab = torch.zeros((1, 2, 2, 2), dtype=torch.float64,
                              device=self.device)

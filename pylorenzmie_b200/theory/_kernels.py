@@ -151,3 +151,108 @@ def hologram_vjp(coords, spheres, ab, dab, nmax, cap, k, gout, bohren=True):
                                        stream_handle(dev)),
                   'lmb_hologram_vjp')
     return grad
+
+
+def wiscombe_yang_layers(radii, indices, n_m, wavelength):
+    '''Host n_max of one multilayer sphere (radii ascending, complex indices).'''
+    k = 2. * np.pi / wavelength * float(np.real(n_m))
+    x = k * np.asarray(radii, dtype=float)
+    m = np.asarray(indices, dtype=complex) / n_m
+    xl = abs(x[-1])
+    if xl <= 8.:
+        ns = np.floor(xl + 4. * np.cbrt(xl) + 1.)
+    elif xl <= 4200.:
+        ns = np.floor(xl + 4.05 * np.cbrt(xl) + 2.)
+    else:
+        ns = np.floor(xl + 4. * np.cbrt(xl) + 2.)
+    return int(max(ns, np.abs(x * m).max(), np.abs(np.roll(x, -1) * m).max()))
+
+
+def layered_ab(radii, indices, n_m, wavelength, cap, deriv=False, check=True):
+    '''Coefficients of multilayer spheres: radii (n, L), indices (n, L, 2)
+    float64 device tensors; outputs as sphere_ab.'''
+    lib = _native.load()
+    dev = radii.device
+    n, L = radii.shape
+    ab = torch.empty((n, cap + 1, 2, 2), dtype=torch.float64, device=dev)
+    dab = (torch.empty((n, cap + 1, 4, 2), dtype=torch.float64, device=dev)
+           if deriv else None)
+    nmax = torch.empty(n, dtype=torch.int32, device=dev)
+    status = torch.empty(n, dtype=torch.int32, device=dev)
+    _native.check(lib.lmb_layered_ab(ptr(radii), ptr(indices), L, n,
+                                     float(n_m), float(wavelength), cap,
+                                     ptr(ab), ptr(dab), ptr(nmax),
+                                     ptr(status), stream_handle(dev)),
+                  'lmb_layered_ab')
+    if check and n and int(status.max().item()) != _native.LMB_OK:
+        raise ValueError('a layered sphere is invalid or needs more '
+                         f'partial-wave orders than the capacity {cap}')
+    return ab, dab, nmax
+
+
+def is_layered(p):
+    return hasattr(p, 'fractions') and hasattr(p, 'core_indices')
+
+
+def particle_nmax(p, n_m, wavelength):
+    if is_layered(p):
+        return wiscombe_yang_layers(p.radii, p.indices, n_m, wavelength)
+    return int(wiscombe_yang(p.a_p, p.n_p, getattr(p, 'k_p', 0.), n_m,
+                             wavelength))
+
+
+def particle_ab(particles, spheres, n_m, wavelength, cap, deriv=False):
+    '''Coefficients for a list of Sphere / LayeredSphere particles (in
+    order); spheres is their (n, 6) device tensor.'''
+    dev = spheres.device
+    n = len(particles)
+    layered = [i for i, p in enumerate(particles) if is_layered(p)]
+    if not layered:
+        return sphere_ab(spheres, n_m, wavelength, cap, deriv)
+    ab = torch.zeros((n, cap + 1, 2, 2), dtype=torch.float64, device=dev)
+    dab = (torch.zeros((n, cap + 1, 4, 2), dtype=torch.float64, device=dev)
+           if deriv else None)
+    nmax = torch.zeros(n, dtype=torch.int32, device=dev)
+    plain = [i for i in range(n) if i not in set(layered)]
+    if plain:
+        idx = torch.tensor(plain, device=dev)
+        a, d, m = sphere_ab(spheres[idx].contiguous(), n_m, wavelength, cap,
+                            deriv)
+        ab[idx], nmax[idx] = a, m
+        if deriv:
+            dab[idx] = d
+    groups = {}
+    for i in layered:
+        groups.setdefault(particles[i].nlayers, []).append(i)
+    for L, members in groups.items():
+        r = np.array([particles[i].radii for i in members], dtype=float)
+        ind = np.zeros((len(members), L, 2))
+        for j, i in enumerate(members):
+            ind[j, :, 0] = particles[i].indices.real
+            ind[j, :, 1] = particles[i].indices.imag
+        a, d, m = layered_ab(torch.from_numpy(r).to(dev),
+                             torch.from_numpy(ind).to(dev), n_m, wavelength,
+                             cap, deriv)
+        idx = torch.tensor(members, device=dev)
+        ab[idx], nmax[idx] = a, m
+        if deriv:
+            dab[idx] = d
+    return ab, dab, nmax
+
+
+def layered_ab_host(particles, n_m, wavelength, deriv=False):
+    '''Coefficients of LayeredSphere particles as numpy complex arrays.'''
+    dev = get_device()
+    cap = max(particle_nmax(p, n_m, wavelength) for p in particles) + 2
+    rec = np.zeros(len(particles), dtype=SPHERE_DTYPE)
+    for i, p in enumerate(particles):
+        rec[i] = (0., 0., 0., p.a_p, p.n_p, p.k_p)
+    ab, dab, nmax = particle_ab(particles, spheres_tensor(rec, dev), n_m,
+                                wavelength, cap, deriv)
+    a = ab.cpu().numpy()
+    a = a[..., 0] + 1j * a[..., 1]
+    d = None
+    if deriv:
+        d = dab.cpu().numpy()
+        d = d[..., 0] + 1j * d[..., 1]
+    return a, d, nmax.cpu().numpy()

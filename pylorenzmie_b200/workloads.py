@@ -18,6 +18,8 @@ of sigma = 0.05 (the instrument's noise).
   5 % in a_p, +0.03 in n_p and +15 px in z_p.
 * large       -- crops of 401x401 with a_p ~ U(3, 6) um, n_p ~ U(1.4, 2.0),
   z_p ~ U(200, 600) px.
+* layered     -- three-layer core-shell spheres in crops of 101..201 px
+  (the video-stream workload; see ``layered``).
 '''
 import numpy as np
 
@@ -84,6 +86,43 @@ def large(B, seed=0, side=401):
     p[:, 3] = rng.uniform(3., 6., B)
     p[:, 4] = rng.uniform(1.4, 2.0, B)
     return p
+
+
+def layered(B, seed=0, magnification=0.048):
+    '''Three-layer core-shell features of the video-stream workload:
+    crop sides U{101, 103, .., 201}, radius fractions ~U(0.3, 0.9) nested
+    (sorted), layer indices ~U(1.33, 1.80), outer a_p ~U(0.5, 2.5) um,
+    z_p ~U(150, 400) px (at least a_p/magnification + 10 px), centred
+    +-2 px.  Returns sides (B,), params (B, 6), fractions (B, 2) and inner
+    indices (B, 2).  Starts: a_p +5 %, n_p +0.02, z_p +10 px.'''
+    rng = np.random.default_rng(seed)
+    sides = 2 * rng.integers(50, 101, B) + 1
+    frac = np.sort(rng.uniform(0.3, 0.9, (B, 2)), axis=1)
+    idx = rng.uniform(1.33, 1.80, (B, 3))
+    p = np.zeros((B, 6))
+    c = (sides - 1) / 2.
+    p[:, 0] = c + rng.uniform(-2., 2., B)
+    p[:, 1] = c + rng.uniform(-2., 2., B)
+    p[:, 3] = rng.uniform(0.5, 2.5, B)
+    p[:, 2] = np.maximum(rng.uniform(150., 400., B),
+                         p[:, 3] / magnification + 10.)
+    p[:, 4] = idx[:, 2]
+    start = p.copy()
+    start[:, 3] *= 1.05
+    start[:, 4] += 0.02
+    start[:, 2] += 10.
+    return sides, p, start, frac, idx[:, :2].astype(complex)
+
+
+def layered_spheres(params, fractions, core_indices):
+    from .theory import LayeredSphere
+    out = []
+    for row, f, c in zip(np.atleast_2d(params), fractions, core_indices):
+        s = LayeredSphere(a_p=row[3], n_p=row[4], k_p=row[5],
+                          fractions=tuple(f), core_indices=tuple(c))
+        s.r_p = row[:3]
+        out.append(s)
+    return out
 
 
 def spheres(params):

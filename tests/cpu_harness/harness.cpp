@@ -10,6 +10,7 @@
 
 #include <vector>
 
+#include "lmb_layered.cuh"
 #include "lmb_lm.cuh"
 #include "lmb_mie.cuh"
 #include "lmb_pixel.cuh"
@@ -38,6 +39,58 @@ API int h_sphere_ab(double a_p, double n_p, double k_p, double n_m, double lam,
     zd out[2], dout[4];
     mie_coefficient(s, n, d1in.data(), d1inz.data(), psi.data(), psix.data(),
                     zeta.data(), zetax.data(), out, dab ? dout : 0);
+    ab[4 * n + 0] = out[0].re;
+    ab[4 * n + 1] = out[0].im;
+    ab[4 * n + 2] = out[1].re;
+    ab[4 * n + 3] = out[1].im;
+    if (dab)
+      for (int j = 0; j < 4; ++j) {
+        dab[8 * n + 2 * j] = dout[j].re;
+        dab[8 * n + 2 * j + 1] = dout[j].im;
+      }
+  }
+  return 0;
+}
+
+// Multilayer coefficients: radii [L], idx [L][2]; outputs as h_sphere_ab.
+API int h_layered_ab(const double* radii, const double* idx, int L, double n_m,
+                     double lam, int cap, double* ab, double* dab, int* nmax) {
+  LayeredScalars s = layered_setup(radii, idx, L, n_m, lam);
+  *nmax = s.nmax;
+  if (s.nmax > cap) return 3;
+  const int nm = s.nmax;
+  std::vector<dz> d1a(nm + 2), d1b(nm + 2), ha(nm + 2), hb(nm + 2);
+  layered_core(s, d1a.data(), ha.data(), hb.data());
+  for (int ii = 1; ii < L; ++ii) {
+    const bool outer = ii == L - 1;
+    dz z1, z2;
+    z1.v = s.x[ii] * s.m[ii];
+    z1.s = z1.v;
+    z1.m = outer ? mk(s.x[ii], 0.) : mk(0., 0.);
+    z2.v = s.x[ii - 1] * s.m[ii];
+    z2.s = z2.v;
+    z2.m = outer ? mk(s.x[ii - 1], 0.) : mk(0., 0.);
+    layered_d1_down(z1, nm, d1a.data());
+    layered_d1_down(z2, nm, d1b.data());
+    layered_shell_up(s, ii, d1a.data(), d1b.data(), ha.data(), hb.data());
+  }
+  MieScalars med;
+  med.k = s.k;
+  med.x = s.x[L - 1];
+  med.n_m = n_m;
+  med.m = s.m[L - 1];
+  med.nmax = nm;
+  std::vector<double> d1m(nm + 1), d1mx(nm + 1), psi(nm + 1), psix(nm + 1);
+  std::vector<zd> zeta(nm + 1), zetax(nm + 1);
+  mie_d1_medium(med, d1m.data(), d1mx.data());
+  mie_upward(med, d1m.data(), d1mx.data(), psi.data(), psix.data(), zeta.data(),
+             zetax.data());
+  memset(ab, 0, sizeof(double) * 4 * (cap + 1));
+  if (dab) memset(dab, 0, sizeof(double) * 8 * (cap + 1));
+  for (int n = 1; n <= nm; ++n) {
+    zd out[2], dout[4];
+    layered_coefficient(s, n, ha[n], hb[n], psi.data(), psix.data(), zeta.data(),
+                        zetax.data(), out, dab ? dout : 0);
     ab[4 * n + 0] = out[0].re;
     ab[4 * n + 1] = out[0].im;
     ab[4 * n + 2] = out[1].re;

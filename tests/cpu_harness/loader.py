@@ -37,6 +37,8 @@ def load():
         tmp.replace(LIB)
     lib = ctypes.CDLL(str(LIB))
     lib.h_sphere_ab.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, _dp, _dp, _ip]
+    lib.h_layered_ab.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_int, _dp, _dp, _ip]
     lib.h_field.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, ctypes.c_int,
                             ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
     lib.h_jacobian.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
@@ -68,6 +70,27 @@ class Harness:
         st = self.lib.h_sphere_ab(a_p, n_p, k_p, n_m, wavelength, cap, ptr(ab),
                                   ptr(dab) if deriv else None,
                                   ctypes.byref(nmax))
+        if st != 0:
+            raise ValueError(f'nmax {nmax.value} above cap')
+        n = nmax.value
+        ab = ab[:n + 1, :, 0] + 1j * ab[:n + 1, :, 1]
+        if deriv:
+            dab = dab[:n + 1, :, 0] + 1j * dab[:n + 1, :, 1]
+            return ab, dab
+        return ab
+
+    def layered_ab(self, radii, indices, n_m, wavelength, cap=1024,
+                   deriv=False):
+        r = np.ascontiguousarray(radii, dtype=float)
+        idx = np.zeros((r.size, 2))
+        idx[:, 0] = np.real(indices)
+        idx[:, 1] = np.imag(indices)
+        ab = np.zeros((cap + 1, 2, 2))
+        dab = np.zeros((cap + 1, 4, 2)) if deriv else None
+        nmax = ctypes.c_int()
+        st = self.lib.h_layered_ab(ptr(r), ptr(idx), r.size, n_m, wavelength,
+                                   cap, ptr(ab), ptr(dab) if deriv else None,
+                                   ctypes.byref(nmax))
         if st != 0:
             raise ValueError(f'nmax {nmax.value} above cap')
         n = nmax.value

@@ -150,3 +150,34 @@ def test_lm_state_machine_matches_scipy(h, golden_fit, variables):
     assert {1: 2, 2: 3, 3: 4, 4: 1}[info] == res.status
     assert abs(redchi - rc) < 1e-9 * rc
     np.testing.assert_allclose(dp, sdp, rtol=1e-6)
+
+
+@pytest.mark.parametrize('radii,idx', [
+    ([0.3, 0.75], [1.6, 1.45 + 0.002j]),
+    ([0.4, 0.8, 1.2], [1.8 + 0.01j, 1.33, 1.5]),
+    ([0.5, 1.2, 2.0], [1.4, 1.7, 1.55 + 0.001j]),
+])
+def test_layered_ab_and_tangents(h, radii, idx):
+    ab, dab = h.layered_ab(radii, idx, 1.34, 0.447, deriv=True)
+    ref = mie.layered_coefficients(radii, idx, 1.34, 0.447)
+    assert ab.shape == ref.shape
+    assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()
+    ap = radii[-1]
+    frac = np.asarray(radii) / ap
+    da = 1e-6 * ap
+    fa = (mie.layered_coefficients(frac * (ap + da), idx, 1.34, 0.447) -
+          mie.layered_coefficients(frac * (ap - da), idx, 1.34, 0.447)) / (2 * da)
+    ip, im = list(idx), list(idx)
+    ip[-1] += 1e-6
+    im[-1] -= 1e-6
+    fn = (mie.layered_coefficients(radii, ip, 1.34, 0.447) -
+          mie.layered_coefficients(radii, im, 1.34, 0.447)) / 2e-6
+    assert np.abs(dab[:, :2] - fa).max() < 1e-6 * np.abs(fa).max()
+    assert np.abs(dab[:, 2:] - fn).max() < 1e-6 * np.abs(fn).max()
+
+
+def test_layered_one_layer_matches_reference(h, golden_layered):
+    for i, (a, n, nm, lam) in enumerate(golden_layered['cases']):
+        ab = h.layered_ab([a.real], [n], nm.real, lam.real)
+        ref = golden_layered[f'ab_{i}']
+        assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()

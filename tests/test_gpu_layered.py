@@ -1,0 +1,114 @@
+'''GPU: multilayer (core-shell) spheres -- Yang coefficients, holograms,
+Jacobians and batched fits -- against the FP64 oracle (a restatement of
+lib/obsolete/sphere_coefficients.py with its input handling repaired; the
+one-layer case is pinned to the reference's own output, the multilayer
+values are parity unpinned beyond the oracle).'''
+import numpy as np
+import pytest
+
+from oracle import field as ofield, fit as ofit, mie
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+
+
+def _oracle_particle(p, frac, core):
+    d = dict(zip(KEYS, p))
+    d['fractions'] = list(frac)
+    d['core_indices'] = list(core)
+    d['layers'] = (np.append(np.asarray(frac) * p[3], p[3]),
+                   np.append(np.asarray(core, complex), p[4] + 1j * p[5]))
+    return d
+
+
+def test_layered_ab_matches_oracle(golden_layered):
+    from pylorenzmie_b200 import LayeredSphere
+    cases = [((0.3,), (1.6,), 0.75, 1.45 + 0.002j),
+             ((0.33, 0.67), (1.8 + 0.01j, 1.33), 1.2, 1.5),
+             ((0.25, 0.6), (1.4, 1.7), 2.0, 1.55 + 0.001j)]
+    for frac, core, a, n in cases:
+        s = LayeredSphere(a_p=a, n_p=n.real, k_p=n.imag, fractions=frac,
+                          core_indices=core)
+        ab = s.ab(1.34, 0.447)
+        ref = mie.layered_coefficients(s.radii, s.indices, 1.34, 0.447)
+        assert ab.shape == ref.shape
+        assert np.abs(ab - ref).max() <= 1e-11 * np.abs(ref).max()
+
+
+def test_layered_hologram_and_jacobian():
+    from pylorenzmie_b200 import LorenzMie, LayeredSphere
+    p = [30.4, 29.7, 180., 1.2, 1.55, 0.0]
+    frac, core = (0.35, 0.7), (1.75 + 0.005j, 1.38)
+    s = LayeredSphere(a_p=p[3], n_p=p[4], k_p=p[5], fractions=frac,
+                      core_indices=core)
+    s.r_p = p[:3]
+    c = ofield.meshgrid((61, 61))
+    inst = ofield.DEFAULT_INSTRUMENT
+    ref = ofield.hologram(c, [_oracle_particle(p, frac, core)], inst)
+    for fp64, tol in ((False, 2e-5), (True, 1e-11)):
+        m = LorenzMie(coordinates=c, particle=s, double_precision=fp64)
+        assert np.abs(m.hologram() - ref).max() <= tol
+    J = LorenzMie(coordinates=c, particle=s).jac()
+    for j, key in enumerate(KEYS):
+        step = 1e-5 * max(abs(p[j]), 1e-2) if j < 5 else 1e-7
+        pp, pm = list(p), list(p)
+        pp[j] += step
+        pm[j] -= step
+        fd = (ofield.hologram(c, [_oracle_particle(pp, frac, core)], inst) -
+              ofield.hologram(c, [_oracle_particle(pm, frac, core)], inst)
+              ) / (2 * step)
+        err = np.abs(J[key] - fd).max() / np.abs(fd).max()
+        assert err < 3e-4, (key, err)
+
+
+TIGHT = {'method': 'lm', 'ftol': 1e-10, 'xtol': 1e-10, 'gtol': 1e-10,
+         'loss': 'linear', 'max_nfev': 2000, 'diff_step': 1e-5,
+         'x_scale': 'jac'}
+
+
+@pytest.mark.parametrize('tight', [True, False])
+def test_layered_batch_fit_vs_oracle(tight):
+    """Fits of 3-layer spheres in one device call against the oracle fit of
+    each.  Converged tightly (ftol 1e-10), both must reach the same minimum
+    within a_p 1 nm, n_p 1e-4, x/y/z_p 0.02 px.  With the default settings
+    both stop on ftol = 1e-4, where the stopping point depends on the path
+    (forward-difference vs analytic Jacobian): there each parameter must be
+    within the target or half its uncertainty, and our chi^2 no worse."""
+    from pylorenzmie_b200 import (LorenzMie, Optimizer, Hologram, workloads)
+    settings = dict(TIGHT) if tight else None
+    sides, truth, start, frac, core = workloads.layered(4, seed=2)
+    sides[:] = [101, 111, 121, 131]
+    c = (sides - 1) / 2.
+    truth[:, 0] = c + 0.4
+    truth[:, 1] = c - 0.7
+    start[:, :2] = truth[:, :2]
+    holos, oracle = [], []
+    for i, s in enumerate(sides):
+        g = ofield.meshgrid((s, s))
+        h = ofield.hologram(g, [_oracle_particle(truth[i], frac[i], core[i])],
+                            ofield.DEFAULT_INSTRUMENT)
+        d = h + np.random.default_rng(60 + i).normal(0., 0.05, h.shape)
+        holos.append(Hologram(d.reshape(s, s)))
+        po = _oracle_particle(start[i], frac[i], core[i])
+        del po['layers']
+        oracle.append(ofit.fit(d, g, po, ofield.DEFAULT_INSTRUMENT,
+                               settings=settings))
+    particles = workloads.layered_spheres(start, frac, core)
+    opt = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1))),
+                    settings=dict(TIGHT) if tight else None)
+    df = opt.optimize_batch(holos, particles=particles)
+    tol = {'x_p': 0.02, 'y_p': 0.02, 'z_p': 0.02, 'a_p': 1e-3, 'n_p': 1e-4}
+    for i in range(4):
+        o = oracle[i]
+        assert o['success'] and df['success'][i]
+        for k, t in tol.items():
+            bound = t if tight else max(t, 0.5 * o['d' + k])
+            assert abs(df[k][i] - o[k]) <= bound, (i, k, df[k][i], o[k])
+        if not tight:
+            assert df['redchi'][i] <= o['redchi'] * (1 + 1e-4)
+    # a single layered fit through optimize()
+    m = LorenzMie(coordinates=np.zeros((2, 1)), particle=particles[0])
+    r = Optimizer(model=m, settings=dict(TIGHT) if tight else None
+                  ).optimize(holos[0])
+    assert abs(r['a_p'] - oracle[0]['a_p']) <= 1e-3
