@@ -240,7 +240,12 @@ def b200_arm(args):
         b['d_params'].copy_(b['d_params0'])
         return _fit.fit_device(b['d_feat'], b['d_data'], None, b['d_params'],
                                B, npix * B, inst, variables, None, b['cap'],
-                               b['start'], stats)
+                               b['start'], stats, tile_config=tile_config)
+
+    from pylorenzmie_b200 import autotune
+    b0 = batches[0]
+    tile_config = autotune.tune(b0['packed'], b0['start'], inst, variables,
+                                b0['cap'], None, dev)
 
     peak = ctypes.c_double()
     _native.check(lib.lmb_measure_fp32_peak(ctypes.byref(peak),
@@ -356,7 +361,8 @@ def b200_arm(args):
                    'crop': '201x201', 'parallelism': f'features sharded '
                    f'over {world} GPU(s), no collective',
                    'l2': f'{ROTATE} rotating input batches '
-                         f'({ROTATE * B * npix * 4 / 1e6:.0f} MB) > 126 MB L2'},
+                         f'({ROTATE * B * npix * 4 / 1e6:.0f} MB) > 126 MB L2',
+                   'tile_config': tile_config},
         'fit_quality': {'success_fraction': success, 'mean_nfev': nfev},
         'roofline': roofline,
         'cpu_baseline': cpu_base,
@@ -412,11 +418,12 @@ def run_extras(dev, inst, chosen_value):
     p = workloads.frame(seed=5)
     while p.shape[0] < 16:
         p = np.vstack([p, workloads.frame(seed=5 + p.shape[0])])[:16]
+    frames = {}
     for fp64 in (False, True):
         m = LorenzMie(coordinates=LorenzMie.meshgrid((1024, 1280)),
                       particle=workloads.spheres(p), instrument=inst,
                       double_precision=fp64, device=dev)
-        m.hologram(device=True)
+        frames[fp64] = m.hologram(device=True).double()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -431,6 +438,64 @@ def run_extras(dev, inst, chosen_value):
             'value': 1280 * 1024 * p.shape[0] / sec / 1e6,
             'unit': 'Mpx/s (pixel-particles)', 'spheres': int(p.shape[0]),
             'ms_per_frame': sec * 1e3}
+    diff = (frames[False] - frames[True]).abs()
+    out['frame_fp32']['max_abs_error_vs_fp64'] = float(diff.max())
+    out['frame_fp32']['max_rel_error_vs_fp64'] = float(
+        (diff / frames[True].abs().clamp_min(1.)).max())
+    out['frame_fp32']['max_hologram'] = float(frames[True].max())
+
+    # differentiation workload: 64 crops of 401x401, a_p 3-6 um
+    from pylorenzmie_b200.theory import autograd as ag
+    from pylorenzmie_b200.theory import _kernels as K
+    P = torch.tensor(workloads.large(64, seed=11), dtype=torch.float64,
+                     device=dev)
+    coords = LorenzMie.meshgrid((401, 401))
+    ag.jacobian(P, coords)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    H, J = ag.jacobian(P, coords)
+    torch.cuda.synchronize()
+    tj = time.perf_counter() - t0
+    Pg = P.clone().requires_grad_(True)
+    d = (H.float() + 0.05 * torch.randn(H.shape, device=dev)).detach()
+    ((ag.hologram(Pg, coords) - d) ** 2).sum().backward()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Pg.grad = None
+    ((ag.hologram(Pg, coords) - d) ** 2).sum().backward()
+    torch.cuda.synchronize()
+    tg = time.perf_counter() - t0
+    out['jacobian_401'] = {
+        'value': 64 / tj, 'unit': 'Jacobian evaluations/s (401x401 crop, '
+                                  '6 columns)',
+        'grad_chi2_per_s': 64 / tg,
+        'mean_nmax': float(K.wiscombe_yang(
+            P[:, 3].cpu().numpy(), P[:, 4].cpu().numpy(), 0., inst.n_m,
+            inst.wavelength).mean())}
+    del H, J
+
+    # layered spheres in a stream: 8 frames x 32 features per call
+    sides, truth, start, frac, core = workloads.layered(256, seed=13)
+    parts = workloads.layered_spheres(truth, frac, core)
+    imgs = workloads.render_particles(parts, [(s, s) for s in sides],
+                                      seed=13, device=dev)
+    holos = [Hologram(im.astype(np.float64)) for im in imgs]
+    starts = workloads.layered_spheres(start, frac, core)
+    opt = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1)),
+                                    instrument=inst, device=dev))
+    opt.optimize_batch(holos, particles=starts)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 4
+    for _ in range(reps):
+        df = opt.optimize_batch(holos, particles=starts)
+    torch.cuda.synchronize()
+    err = np.abs(df['a_p'].to_numpy() - truth[:, 3])
+    out['layered_stream_e2e'] = {
+        'value': 256 * reps / (time.perf_counter() - t0), 'unit': UNIT,
+        'features_per_call': 256, 'layers': 3,
+        'success_fraction': float(df['success'].mean()),
+        'median_abs_a_p_error_vs_truth_um': float(np.median(err))}
 
     # mixed crop sizes 51..301, 256 features per launch
     sides, truth, start = workloads.mixed_crops(256, seed=9)

@@ -263,7 +263,8 @@ class Optimizer(LMObject):
         return '\n'.join(lines)
 
     # ------------------------------------------------------------------
-    def optimize_batch(self, holograms, particles=None, starts=None):
+    def optimize_batch(self, holograms, particles=None, starts=None,
+                       autotune=None):
         '''Fit one sphere per hologram, all on the device in one call.
 
         holograms : list of Hologram (crops; any sizes)
@@ -272,6 +273,9 @@ class Optimizer(LMObject):
                     is kept, their outer radius and index are fitted
         starts    : array (B, 6) of x_p, y_p, z_p, a_p, n_p, k_p (overrides
                     the particles' start values)
+        autotune  : time the evaluation kernel's launch shapes once per
+                    problem class and use the fastest (default: batches of
+                    64 features or more)
         Returns a DataFrame, one row per feature, with the columns of
         ``result`` plus ``status`` and ``nfev``.
         '''
@@ -289,9 +293,12 @@ class Optimizer(LMObject):
                 getattr(p, 'k_p', 0.)] for p in particles], dtype=float)
         items = [self._pixels(h) for h in holograms]
         packed = _fit.PackedFeatures(items)
+        if autotune is None:
+            autotune = len(holograms) >= 64
         params, res = _fit.fit_packed(packed, starts, self.model.instrument,
                                       self.variables, self.settings,
-                                      device=self.model.device, layers=layers)
+                                      device=self.model.device, layers=layers,
+                                      autotune=autotune)
         return batch_frame(params, res, packed, self.variables)
 
 

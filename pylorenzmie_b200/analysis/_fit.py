@@ -258,7 +258,8 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
 
 
 def fit_packed(packed, starts, instrument, variables, settings=None,
-               device=None, nmax_cap=None, stats=False, layers=None):
+               device=None, nmax_cap=None, stats=False, layers=None,
+               autotune=False):
     '''Fit every packed feature; returns (params (B, 6), results record
     array with dparams, redchi, cost, status, success, nfev, njev) and,
     when stats, the FitStats of the call.'''
@@ -271,9 +272,15 @@ def fit_packed(packed, starts, instrument, variables, settings=None,
     if nmax_cap is None:
         nmax_cap = fit_capacity(starts, float(instrument.n_m),
                                 float(instrument.wavelength), layers)
+    tile_config = 0
+    if autotune:
+        from .. import autotune as _tuner
+        tile_config = _tuner.tune(packed, starts, instrument, variables,
+                                  nmax_cap, layers, d_data.device)
     d_res, fs = fit_device(d_feat, d_data, d_coords, d_params, B,
                            packed.total, instrument, variables, settings,
-                           nmax_cap, starts, stats, layers=layers)
+                           nmax_cap, starts, stats, tile_config=tile_config,
+                           layers=layers)
     params = d_params.view(torch.float64).reshape(B, 6).cpu().numpy()
     res = d_res[:B * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
         _native.RESULT_DTYPE).copy()

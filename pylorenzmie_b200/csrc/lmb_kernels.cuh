@@ -225,9 +225,9 @@ __device__ inline zd rot_i(zd z, int k) {  // z * i^k
 template <typename R, bool kJac>
 __device__ void stage_coef(const zd* ab, const zd* dab, int nmax,
                            Quad<R>* sm) {
-  constexpr int W = kJac ? 4 : 2;
+  constexpr int W = kJac ? int(JAC_QUADS) : 2;
   for (int n = threadIdx.x; n <= nmax; n += blockDim.x) {
-    Quad<R> q[4];
+    Quad<R> q[JAC_QUADS];
     if (n == 0) {
       for (int j = 0; j < W; ++j) q[j].x = q[j].y = q[j].z = q[j].w = R(0);
     } else {
@@ -247,6 +247,8 @@ __device__ void stage_coef(const zd* ab, const zd* dab, int nmax,
         const zd ben = en * rot_i(dab[4 * n + 3], n);
         q[2].x = R(ala.re); q[2].y = R(ala.im); q[2].z = R(bea.re); q[2].w = R(bea.im);
         q[3].x = R(aln.re); q[3].y = R(aln.im); q[3].z = R(ben.re); q[3].w = R(ben.im);
+        q[4].x = R(nn1 * ala.re); q[4].y = R(nn1 * ala.im);
+        q[4].z = R(nn1 * aln.re); q[4].w = R(nn1 * aln.im);
       }
     }
     for (int j = 0; j < W; ++j) sm[W * n + j] = q[j];
@@ -452,7 +454,7 @@ struct FitCtx {
   double* base;        // [nf][6] start values (fixed parameters keep them)
   zd* ab;              // [nf][nmaxp][2]
   zd* dab;             // [nf][nmaxp][4]
-  Quad<float>* coef32; // [nf][nmaxp][4] FP32 per-order records of the eval point
+  Quad<float>* coef32; // [nf][nmaxp][JAC_QUADS] FP32 records of the eval point
   int* nmax;           // [nf]
   int* tile_begin;     // [nf+1]
   int2* tiles;         // [max_tiles]
@@ -572,9 +574,10 @@ k_fit_eval(FitCtx c) {
     }
     const int nm = min(max(c.nmax[f], 0), nmaxp - 1);
     {
-      const float4* src = reinterpret_cast<const float4*>(c.coef32 + size_t(f) * nmaxp * 4);
+      const float4* src =
+          reinterpret_cast<const float4*>(c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
       float4* dst = reinterpret_cast<float4*>(coef);
-      for (int i = threadIdx.x; i < 4 * (nm + 1); i += TPB) dst[i] = src[i];
+      for (int i = threadIdx.x; i < JAC_QUADS * (nm + 1); i += TPB) dst[i] = src[i];
     }
     const lmb_feature ft = c.features[f];
     const EvalPoint ep = c.ev[f];
@@ -623,6 +626,98 @@ k_fit_eval(FitCtx c) {
       atomicAdd(c.work + 1, (unsigned long long)np * (unsigned long long)nm);
     }
     __syncthreads();
+  }
+}
+
+// Warp-granular evaluation: every warp pulls whole 512-pixel tiles from the
+// queue (16 pixels per lane), keeps its own copy of the coefficients of the
+// feature it is on, and reduces its 28 sums with shuffles -- no block-wide
+// barrier anywhere.  WPB warps per CTA, MINB CTAs per SM at least.
+template <int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * 32, MINB)
+k_fit_eval_warp(FitCtx c) {
+  extern __shared__ __align__(16) char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nmaxp = c.nmax_cap + 1;
+  Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem) +
+                      size_t(warp) * JAC_QUADS * nmaxp;
+  const int ntiles = c.counters[2];
+  const bool bohren = c.flags & LMB_BOHREN;
+  const float kf = float(c.k);
+  const float inv_noise = float(c.inv_noise);
+  constexpr int PPL = 16;  // pixels per lane: 32 x 16 = 512 = one tile
+  int cur = -1, nm = 0;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(c.counters, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= ntiles) break;
+    const int2 tile = c.tiles[t];
+    const int f = tile.x;
+    if (!c.ev[f].active) continue;
+    if (f != cur) {
+      __syncwarp();
+      nm = min(max(c.nmax[f], 0), nmaxp - 1);
+      const float4* src =
+          reinterpret_cast<const float4*>(c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
+      float4* dst = reinterpret_cast<float4*>(coef);
+      for (int i = lane; i < JAC_QUADS * (nm + 1); i += 32) dst[i] = src[i];
+      __syncwarp();
+      cur = f;
+    }
+    const lmb_feature ft = c.features[f];
+    const EvalPoint ep = c.ev[f];
+    float acc[FIT_NSUM];
+#pragma unroll
+    for (int j = 0; j < FIT_NSUM; ++j) acc[j] = 0.f;
+    for (int q = 0; q < PPL; ++q) {
+      const long long i = (long long)tile.y + q * 32 + lane;
+      if (i >= ft.npix || i >= (long long)tile.y + c.tile_pixels) break;
+      double x, y;
+      if (ft.nx > 0) {
+        const long long row = i / ft.nx;
+        x = ft.x0 + double(i - row * ft.nx);
+        y = ft.y0 + double(row);
+      } else {
+        const float2 xy = reinterpret_cast<const float2*>(c.coords)[ft.data_offset + i];
+        x = xy.x;
+        y = xy.y;
+      }
+      const float d = c.data[ft.data_offset + i];
+      const Geometry<float> g = geometry<float>(c.k, x - ep.p[0], y - ep.p[1],
+                                                -ep.p[2], 0., ep.p[2], bohren);
+      float H, dH[6];
+      holo_jac_pixel(g, coef, nm, kf, &H, dH);
+      const float r = (H - d) * inv_noise;
+      float J[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) J[j] = dH[j] * inv_noise;
+      acc[0] += r * r;
+      int o = 1;
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = a; b < 6; ++b) acc[o++] += J[a] * J[b];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) acc[22 + a] += J[a] * r;
+    }
+#pragma unroll
+    for (int j = 0; j < FIT_NSUM; ++j) {
+      float v = acc[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      acc[j] = v;
+    }
+    // lane j writes sum j (a fixed-order, deterministic reduction)
+#pragma unroll
+    for (int j = 0; j < FIT_NSUM; ++j)
+      if (lane == j) c.partial[(size_t)t * FIT_NSUM + j] = acc[j];
+    if (lane == 0) {
+      long long np = ft.npix - tile.y;
+      if (np > c.tile_pixels) np = c.tile_pixels;
+      atomicAdd(c.work, (unsigned long long)np);
+      atomicAdd(c.work + 1, (unsigned long long)np * (unsigned long long)nm);
+    }
   }
 }
 
@@ -704,7 +799,7 @@ k_fit_step(FitCtx c) {
     stage_coef<float, true>(c.ab + size_t(f) * nmaxp * 2,
                             c.dab + size_t(f) * nmaxp * 4,
                             min(c.nmax[f], nmaxp - 1),
-                            c.coef32 + size_t(f) * nmaxp * 4);
+                            c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
   if (lane == 0) {
     if (st != LMB_OK) {
       gs->phase = LM_PHASE_DONE;

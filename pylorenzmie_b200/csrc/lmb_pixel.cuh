@@ -56,11 +56,15 @@ namespace lmb {
 //   c0 = (alpha.re, alpha.im, beta.re, beta.im)
 //   c1 = (n(n+1) alpha.re, n(n+1) alpha.im, 1 + 1/n, n)
 // and, for the Jacobian, the a_p and n_p derivatives of alpha and beta:
-//   c2 = d/da_p (alpha, beta), c3 = d/dn_p (alpha, beta).
+//   c2 = d/da_p (alpha, beta), c3 = d/dn_p (alpha, beta),
+//   c4 = n(n+1) d/da_p alpha, n(n+1) d/dn_p alpha.
+// JAC_QUADS records per order for the Jacobian, 2 for the value.
 template <typename R>
 struct Quad {
   R x, y, z, w;
 };
+
+enum { JAC_QUADS = 5 };
 
 template <typename R>
 struct Geometry {
@@ -216,7 +220,7 @@ struct JacSums {
   cplx<R> p[3];   // d/dn_p
 };
 
-// coef: 4 Quads per order (index n*4 + {0..3}), see Quad above.
+// coef: JAC_QUADS Quads per order (index n*JAC_QUADS + j), see Quad above.
 template <typename R>
 LMB_HD JacSums<R> order_sum_jac(const Geometry<R>& g, const Quad<R>* coef,
                                 int nmax) {
@@ -235,27 +239,30 @@ LMB_HD JacSums<R> order_sum_jac(const Geometry<R>& g, const Quad<R>* coef,
   cplx<R> h2 = g.hm1, h1 = g.h0;
   cplx<R> hp2 = mk(R(0), R(0)), hp1 = hp2;  // d h~/dkr
   const R sv = g.s1mu, ikr = g.ikrs, ikr2 = g.ikrs * g.ikr;
+#pragma unroll 2
   for (int n = 1; n <= nmax; ++n) {
-    const Quad<R> c0 = coef[4 * n];
-    const Quad<R> c1 = coef[4 * n + 1];
-    const Quad<R> c2 = coef[4 * n + 2];
-    const Quad<R> c3 = coef[4 * n + 3];
+    const Quad<R> c0 = coef[JAC_QUADS * n];
+    const Quad<R> c1 = coef[JAC_QUADS * n + 1];
+    const Quad<R> c2 = coef[JAC_QUADS * n + 2];
+    const Quad<R> c3 = coef[JAC_QUADS * n + 3];
+    const Quad<R> c4 = coef[JAC_QUADS * n + 4];
     const R fn = c1.w;
     const R cn = c1.z;
     const R spi = sv * pi;
     const R tau = pim1 - fn * del + fn * spi;
     const R dspi = pi + sv * dpi;
     const R dtau = dpim1 - fn * ddel + fn * dspi;
-    const R a2 = (fn + fn - R(1)) * ikr;
+    const R tn1 = fn + fn - R(1);
+    const R a2 = tn1 * ikr;
     const cplx<R> h = mk(a2 * h1.re - h2.re, a2 * h1.im - h2.im);
     const R a1 = fn * ikr;
     const cplx<R> dh = mk(a1 * h.re - h1.re, a1 * h.im - h1.im);
-    const R nn1 = fn * (fn + R(1));
     // d/dkr of h~_n = (2n-1) ikr h~_{n-1} - h~_{n-2} and of dh
-    const cplx<R> hp = mk(a2 * hp1.re - (fn + fn - R(1)) * ikr2 * h1.re - hp2.re,
-                          a2 * hp1.im - (fn + fn - R(1)) * ikr2 * h1.im - hp2.im);
-    const cplx<R> dhp = mk(a1 * hp.re - fn * ikr2 * h.re - hp1.re,
-                           a1 * hp.im - fn * ikr2 * h.im - hp1.im);
+    const R b2 = tn1 * ikr2, b1 = fn * ikr2;
+    const cplx<R> hp = mk(a2 * hp1.re - b2 * h1.re - hp2.re,
+                          a2 * hp1.im - b2 * h1.im - hp2.im);
+    const cplx<R> dhp = mk(a1 * hp.re - b1 * h.re - hp1.re,
+                           a1 * hp.im - b1 * h.im - hp1.im);
     const cplx<R> al = mk(c0.x, c0.y), be = mk(c0.z, c0.w);
     const cplx<R> al1 = mk(c1.x, c1.y);
     const cplx<R> ala = mk(c2.x, c2.y), bea = mk(c2.z, c2.w);
@@ -274,12 +281,13 @@ LMB_HD JacSums<R> order_sum_jac(const Geometry<R>& g, const Quad<R>* coef,
     A.t[0] = A.t[0] + pi * Zk;
     A.t[1] = A.t[1] + tau * Xk - pi * Yk;
     A.t[2] = A.t[2] + pi * Xk - tau * Yk;
-    // a_p: n(n+1) d alpha is formed from d alpha
-    const cplx<R> Xa = ala * dh, Ya = bea * h, Za = nn1 * (ala * h);
+    // a_p (c4 holds n(n+1) d alpha)
+    const cplx<R> ala1 = mk(c4.x, c4.y), aln1 = mk(c4.z, c4.w);
+    const cplx<R> Xa = ala * dh, Ya = bea * h, Za = ala1 * h;
     A.a[0] = A.a[0] + pi * Za;
     A.a[1] = A.a[1] + tau * Xa - pi * Ya;
     A.a[2] = A.a[2] + pi * Xa - tau * Ya;
-    const cplx<R> Xn = aln * dh, Yn = ben * h, Zn = nn1 * (aln * h);
+    const cplx<R> Xn = aln * dh, Yn = ben * h, Zn = aln1 * h;
     A.p[0] = A.p[0] + pi * Zn;
     A.p[1] = A.p[1] + tau * Xn - pi * Yn;
     A.p[2] = A.p[2] + pi * Xn - tau * Yn;

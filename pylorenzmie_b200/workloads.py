@@ -152,3 +152,23 @@ def render(params, shape, seed=0, instrument=None, device=None,
     h = h + noise * torch.randn(h.shape, generator=g, device=h.device,
                                 dtype=h.dtype)
     return h.float().reshape(len(lists), *shape)
+
+
+def render_particles(particles, shapes, seed=0, instrument=None, device=None,
+                     noise=NOISE):
+    '''Noisy holograms (list of (ny, nx) float32 numpy arrays), one particle
+    (Sphere or LayeredSphere) per crop, crops of differing shapes.'''
+    import torch
+    from .theory import LorenzMie, Instrument
+    inst = instrument or Instrument()
+    g = torch.Generator(device='cuda' if device is None else device)
+    g.manual_seed(int(seed))
+    out = []
+    for p, shape in zip(particles, shapes):
+        m = LorenzMie(coordinates=LorenzMie.meshgrid(shape), particle=p,
+                      instrument=inst, double_precision=True, device=device)
+        h = m.hologram(device=True)
+        h = h + noise * torch.randn(h.shape, generator=g, device=h.device,
+                                    dtype=h.dtype)
+        out.append(h.float().reshape(shape).cpu().numpy())
+    return out

@@ -117,7 +117,7 @@ template <typename R>
 static void stage(const double* ab, const double* dab, int nmax, Quad<R>* q,
                   int w) {
   for (int n = 0; n <= nmax; ++n) {
-    Quad<R> r[4];
+    Quad<R> r[JAC_QUADS];
     memset(r, 0, sizeof(r));
     if (n > 0) {
       const double fn = n, nn1 = fn * (fn + 1.), en = (2. * fn + 1.) / nn1;
@@ -125,13 +125,15 @@ static void stage(const double* ab, const double* dab, int nmax, Quad<R>* q,
       const zd al = en * rot_i(a, n + 1), be = en * rot_i(b, n);
       r[0] = Quad<R>{R(al.re), R(al.im), R(be.re), R(be.im)};
       r[1] = Quad<R>{R(nn1 * al.re), R(nn1 * al.im), R(1. + 1. / fn), R(fn)};
-      if (w == 4) {
+      if (w == JAC_QUADS) {
         zd d[4];
         for (int j = 0; j < 4; ++j) d[j] = mk(dab[8 * n + 2 * j], dab[8 * n + 2 * j + 1]);
         const zd ala = en * rot_i(d[0], n + 1), bea = en * rot_i(d[1], n);
         const zd aln = en * rot_i(d[2], n + 1), ben = en * rot_i(d[3], n);
         r[2] = Quad<R>{R(ala.re), R(ala.im), R(bea.re), R(bea.im)};
         r[3] = Quad<R>{R(aln.re), R(aln.im), R(ben.re), R(ben.im)};
+        r[4] = Quad<R>{R(nn1 * ala.re), R(nn1 * ala.im), R(nn1 * aln.re),
+                       R(nn1 * aln.im)};
       }
     }
     for (int j = 0; j < w; ++j) q[w * n + j] = r[j];
@@ -172,8 +174,8 @@ template <typename R>
 static void jac_one(const double* coords, long long npts, const double* p,
                     const double* ab, const double* dab, int nmax, double k,
                     int flags, double* holo, double* jac) {
-  std::vector<Quad<R>> q(4 * (nmax + 1));
-  stage<R>(ab, dab, nmax, q.data(), 4);
+  std::vector<Quad<R>> q(JAC_QUADS * (nmax + 1));
+  stage<R>(ab, dab, nmax, q.data(), JAC_QUADS);
   for (long long i = 0; i < npts; ++i) {
     const double x = coords[i], y = coords[npts + i], z = coords[2 * npts + i];
     Geometry<R> g = geometry<R>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);

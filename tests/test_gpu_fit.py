@@ -117,3 +117,20 @@ def test_fit_edge_cases():
     assert not df['success'][0] and not df['success'][1]
     assert df['success'][2]
     assert abs(df['a_p'][2] - 0.75) < 0.02
+
+
+def test_autotuned_batch_matches_default(tmp_path, monkeypatch):
+    from pylorenzmie_b200 import Hologram, workloads, autotune
+    monkeypatch.setenv('LMB200_AUTOTUNE_CACHE', str(tmp_path / 'tune.json'))
+    autotune._memory.clear()
+    truth, start = workloads.batch_201(8, seed=4)
+    truth[:, :2] -= 60.  # centre the spheres on 81x81 crops
+    start[:, :2] -= 60.
+    data = workloads.render(truth, (81, 81), seed=4).cpu().numpy()
+    holos = [Hologram(d.astype(float)) for d in data]
+    opt = make_optimizer(start[0], (8, 8))
+    d0 = opt.optimize_batch(holos, starts=start, autotune=False)
+    d1 = opt.optimize_batch(holos, starts=start, autotune=True)
+    assert (tmp_path / 'tune.json').exists()
+    for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p'):
+        assert np.all(np.abs(d0[k] - d1[k]) <= TOL[k] * 0.1)

@@ -213,3 +213,21 @@ def test_workloads():
     assert 1 <= p.shape[0] <= 16
     assert np.all(p[:, 2] >= p[:, 3] / 0.048 + 10 - 1e-9)
     assert len(workloads.spheres(p)) == p.shape[0]
+
+
+def test_autotune_keys_and_cache(tmp_path, monkeypatch):
+    from pylorenzmie_b200 import autotune
+    monkeypatch.setenv('LMB200_AUTOTUNE_CACHE', str(tmp_path / 'tune.json'))
+    k1 = autotune.problem_key('B200', 30, 201 * 201)
+    k2 = autotune.problem_key('B200', 32, 150 * 150)
+    k3 = autotune.problem_key('B200', 33, 201 * 201)
+    assert k1 == k2 and k1 != k3
+    assert 'layered' in autotune.problem_key('B200', 30, 100, layered=True)
+    assert autotune.cache_path() == tmp_path / 'tune.json'
+    autotune._store('x', {'config': 3})
+    autotune._memory.clear()
+    assert autotune.lookup('x') == {'config': 3}
+    assert autotune.lookup('missing') is None
+    shapes = autotune.shapes()
+    assert len(shapes) >= 2 and shapes[0][0] == 0
+    assert all(t % 32 == 0 and 512 % p == 0 for _, t, p, _ in shapes)
