@@ -45,6 +45,8 @@ def parse():
     ap.add_argument('--batch', type=int, default=BATCH)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-extras', action='store_true')
+    ap.add_argument('--tile-config', type=int, default=None,
+                    help='fixed evaluation launch shape (default: autotune)')
     return ap.parse_args()
 
 
@@ -244,8 +246,11 @@ def b200_arm(args):
 
     from pylorenzmie_b200 import autotune
     b0 = batches[0]
-    tile_config = autotune.tune(b0['packed'], b0['start'], inst, variables,
-                                b0['cap'], None, dev)
+    if args.tile_config is None:
+        tile_config = autotune.tune(b0['packed'], b0['start'], inst,
+                                    variables, b0['cap'], None, dev)
+    else:
+        tile_config = int(args.tile_config)
 
     peak = ctypes.c_double()
     _native.check(lib.lmb_measure_fp32_peak(ctypes.byref(peak),

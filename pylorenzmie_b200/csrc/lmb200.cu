@@ -43,22 +43,29 @@ struct EvalShape {
   int tpb, ppt, minb;
   void (*fn)(FitCtx);
   int warp_tiles;  // 1: each warp owns a tile and a copy of the coefficients
+  int pair;        // 1: packed two-pixel loop, pair-layout records
 };
 const EvalShape kEvalShapes[] = {
-    {64, 8, 8, k_fit_eval<64, 8, 8>},
+    // packed two-pixel loop (default); the geometry is recomputed after the
+    // order loop, which frees registers for occupancy
+    {64, 8, 6, k_fit_eval_pair<64, 8, 6, true>, 0, 1},
+    // scalar loop: also the fallback when pair records do not fit in
+    // shared memory (kScalarShape)
     {128, 4, 4, k_fit_eval<128, 4, 4>},
-    {128, 4, 5, k_fit_eval<128, 4, 5>},
-    {128, 4, 6, k_fit_eval<128, 4, 6>},
-    {256, 2, 2, k_fit_eval<256, 2, 2>},
-    {256, 2, 3, k_fit_eval<256, 2, 3>},
+    {128, 4, 3, k_fit_eval_pair<128, 4, 3, true>, 0, 1},
+    {64, 8, 5, k_fit_eval_pair<64, 8, 5, true>, 0, 1},
+    {32, 16, 12, k_fit_eval_pair<32, 16, 12, true>, 0, 1},
+    {64, 8, 4, k_fit_eval_pair<64, 8, 4, false>, 0, 1},
+    {128, 4, 2, k_fit_eval_pair<128, 4, 2, false>, 0, 1},
+    {256, 2, 2, k_fit_eval_pair<256, 2, 2, false>, 0, 1},
+    {64, 8, 8, k_fit_eval<64, 8, 8>},
     {64, 8, 10, k_fit_eval<64, 8, 10>},
-    {512, 1, 1, k_fit_eval<512, 1, 1>},
+    {256, 2, 2, k_fit_eval<256, 2, 2>},
     {128, 16, 4, k_fit_eval_warp<4, 4>, 1},
-    {64, 16, 8, k_fit_eval_warp<2, 8>, 1},
     {256, 16, 2, k_fit_eval_warp<8, 2>, 1},
-    {32, 16, 16, k_fit_eval_warp<1, 16>, 1},
 };
 constexpr int kNumEvalShapes = int(sizeof(kEvalShapes) / sizeof(kEvalShapes[0]));
+constexpr int kScalarShape = 1;  // scalar loop, used when pair records do not fit
 
 struct FitLayout {
   size_t state, ev, base, ab, dab, coef32, nmax, tile_begin, tiles, partial,
@@ -84,7 +91,8 @@ FitLayout fit_layout(int nf, long long total_pixels, int nmax_cap) {
   L.base = take(sizeof(double) * 6 * nf);
   L.ab = take(sizeof(zd) * 2 * nmaxp * nf);
   L.dab = take(sizeof(zd) * 4 * nmaxp * nf);
-  L.coef32 = take(sizeof(Quad<float>) * JAC_QUADS * nmaxp * nf);
+  // room for either record layout (scalar JAC_QUADS or pair PAIR_QUADS)
+  L.coef32 = take(sizeof(float4) * PAIR_QUADS * nmaxp * nf);
   L.nmax = take(sizeof(int) * nf);
   L.tile_begin = take(sizeof(int) * (nf + 1));
   L.tiles = take(sizeof(int2) * size_t(L.max_tiles));
@@ -354,10 +362,19 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
 
   const size_t ab_smem = nlayers > 1 ? layered_scratch_bytes(nmax_cap + 1)
                                      : ab_scratch_bytes(nmax_cap + 1);
-  const size_t coef_smem = sizeof(Quad<float>) * JAC_QUADS * (size_t(nmax_cap) + 1);
   const int shape_index = settings->tile_config;
   if (shape_index < 0 || shape_index >= kNumEvalShapes) return LMB_ERR_ARG;
-  const EvalShape shape = kEvalShapes[shape_index];
+  EvalShape shape = kEvalShapes[shape_index];
+  // pair records take 256 B per order: above ~800 orders they no longer fit
+  // in shared memory next to the reduction buffer, so such batches use the
+  // scalar loop
+  if (shape.pair && sizeof(float4) * PAIR_QUADS * (size_t(nmax_cap) + 1) >
+                        size_t(200) * 1024)
+    shape = kEvalShapes[kScalarShape];
+  c.pair_records = shape.pair;
+  const size_t coef_smem = (shape.pair ? sizeof(float4) * PAIR_QUADS
+                                       : sizeof(Quad<float>) * JAC_QUADS) *
+                           (size_t(nmax_cap) + 1);
   auto eval = shape.fn;
   const size_t eval_smem = shape.warp_tiles ? coef_smem * (shape.tpb / 32) : coef_smem;
   LMB_CK(smem_attr((const void*)k_fit_step, ab_smem));

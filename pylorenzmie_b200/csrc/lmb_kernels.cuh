@@ -21,6 +21,7 @@
 #include "lmb_lm.cuh"
 #include "lmb_mie.cuh"
 #include "lmb_pixel.cuh"
+#include "lmb_records.cuh"
 
 namespace lmb {
 
@@ -213,45 +214,26 @@ __global__ void k_layered_ab(const double* radii, const double* indices, int L,
 // ---------------------------------------------------------------------------
 // Staging of per-order records (see lmb_pixel.cuh, struct Quad).
 
-__device__ inline zd rot_i(zd z, int k) {  // z * i^k
-  switch (k & 3) {
-    case 0: return z;
-    case 1: return mk(-z.im, z.re);
-    case 2: return mk(-z.re, -z.im);
-    default: return mk(z.im, -z.re);
-  }
-}
-
 template <typename R, bool kJac>
 __device__ void stage_coef(const zd* ab, const zd* dab, int nmax,
                            Quad<R>* sm) {
   constexpr int W = kJac ? int(JAC_QUADS) : 2;
   for (int n = threadIdx.x; n <= nmax; n += blockDim.x) {
     Quad<R> q[JAC_QUADS];
-    if (n == 0) {
-      for (int j = 0; j < W; ++j) q[j].x = q[j].y = q[j].z = q[j].w = R(0);
-    } else {
-      const double fn = double(n);
-      const double nn1 = fn * (fn + 1.);
-      const double en = (2. * fn + 1.) / nn1;
-      // alpha = i E_n a_n = en i^{n+1} a_n, beta = E_n b_n = en i^n b_n
-      const zd al = en * rot_i(ab[2 * n], n + 1);
-      const zd be = en * rot_i(ab[2 * n + 1], n);
-      q[0].x = R(al.re); q[0].y = R(al.im); q[0].z = R(be.re); q[0].w = R(be.im);
-      q[1].x = R(nn1 * al.re); q[1].y = R(nn1 * al.im);
-      q[1].z = R(1. + 1. / fn); q[1].w = R(fn);
-      if (kJac) {
-        const zd ala = en * rot_i(dab[4 * n + 0], n + 1);
-        const zd bea = en * rot_i(dab[4 * n + 1], n);
-        const zd aln = en * rot_i(dab[4 * n + 2], n + 1);
-        const zd ben = en * rot_i(dab[4 * n + 3], n);
-        q[2].x = R(ala.re); q[2].y = R(ala.im); q[2].z = R(bea.re); q[2].w = R(bea.im);
-        q[3].x = R(aln.re); q[3].y = R(aln.im); q[3].z = R(ben.re); q[3].w = R(ben.im);
-        q[4].x = R(nn1 * ala.re); q[4].y = R(nn1 * ala.im);
-        q[4].z = R(nn1 * aln.re); q[4].w = R(nn1 * aln.im);
-      }
-    }
+    order_record<R>(ab + 2 * n, kJac ? dab + 4 * n : dab, n, W, q);
     for (int j = 0; j < W; ++j) sm[W * n + j] = q[j];
+  }
+}
+
+// Records of order_sum_jac_pair: PAIR_QUADS float4 per order, every value
+// duplicated into both lanes of a float2.
+__device__ void stage_pair(const zd* ab, const zd* dab, int nmax, float4* sm) {
+  for (int n = threadIdx.x; n <= nmax; n += blockDim.x) {
+    float v[PAIR_VALUES];
+    pair_record(ab + 2 * n, dab + 4 * n, n, v);
+    for (int j = 0; j < PAIR_QUADS; ++j)
+      sm[PAIR_QUADS * n + j] =
+          make_float4(v[2 * j], v[2 * j], v[2 * j + 1], v[2 * j + 1]);
   }
 }
 
@@ -454,7 +436,8 @@ struct FitCtx {
   double* base;        // [nf][6] start values (fixed parameters keep them)
   zd* ab;              // [nf][nmaxp][2]
   zd* dab;             // [nf][nmaxp][4]
-  Quad<float>* coef32; // [nf][nmaxp][JAC_QUADS] FP32 records of the eval point
+  Quad<float>* coef32; // [nf][nmaxp][JAC_QUADS or PAIR_QUADS] FP32 records
+                       // of the evaluation point (pair layout if pair_records)
   int* nmax;           // [nf]
   int* tile_begin;     // [nf+1]
   int2* tiles;         // [max_tiles]
@@ -469,6 +452,7 @@ struct FitCtx {
   double n_m, wavelength, k, inv_noise;
   LMSettings set;
   int variables, flags, max_iterations;
+  int pair_records;    // the evaluation kernel reads stage_pair records
 };
 
 __device__ inline bool feature_valid(const lmb_feature& ft, long long total) {
@@ -622,6 +606,142 @@ k_fit_eval(FitCtx c) {
     if (threadIdx.x == 0) {
       long long np = ft.npix - tile.y;
       if (np > c.tile_pixels) np = c.tile_pixels;
+      atomicAdd(c.work, (unsigned long long)np);
+      atomicAdd(c.work + 1, (unsigned long long)np * (unsigned long long)nm);
+    }
+    __syncthreads();
+  }
+}
+
+// Two pixels of one sphere through one packed order loop; hologram and
+// 6-column Jacobian of each.  (dx, dy, dz): pixel minus particle position.
+// With kRecompute the pixel geometry is formed again after the order loop
+// instead of being held in registers across it (the empty asm statements
+// keep the compiler from merging the two computations).
+template <bool kRecompute>
+__device__ inline void holo_jac_pair(double k, const double* dx,
+                                     const double* dy, double dz, double zp,
+                                     bool bohren, const float4* rec, int nm,
+                                     float kf, float* H, float (*dH)[6]) {
+  Geometry<float> g[2];
+  for (int l = 0; l < 2; ++l)
+    g[l] = geometry<float>(k, dx[l], dy[l], dz, 0., zp, bohren);
+  PairSums P;
+  order_sum_jac_pair(pair_in(g[0], g[1]), rec, nm, P);
+  if (kRecompute) {
+    for (int l = 0; l < 2; ++l) {
+      double x = dx[l], y = dy[l];
+      asm volatile("" : "+d"(x), "+d"(y));
+      g[l] = geometry<float>(k, x, y, dz, 0., zp, bohren);
+    }
+  }
+#pragma unroll
+  for (int lane = 0; lane < 2; ++lane) {
+    const Geometry<float>& gl = g[lane];
+    const JacSums<float> A = pair_lane(P, lane, gl.smu);
+    cplx<float> e[3], de[6][3];
+    epilogue_jac<float>(gl, A, kf, e, de);
+    H[lane] = intensity<float>(e);
+    const cplx<float> et0 = mk(e[0].re + 1.f, e[0].im);
+    for (int j = 0; j < 6; ++j)
+      dH[lane][j] = 2.f * (et0.re * de[j][0].re + et0.im * de[j][0].im +
+                           e[1].re * de[j][1].re + e[1].im * de[j][1].im +
+                           e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+  }
+}
+
+__device__ inline void fit_pixel_xy(const lmb_feature& ft, const float* coords,
+                                    long long i, double* x, double* y) {
+  if (ft.nx > 0) {
+    const long long row = i / ft.nx;
+    *x = ft.x0 + double(i - row * ft.nx);
+    *y = ft.y0 + double(row);
+  } else {
+    const float2 xy = reinterpret_cast<const float2*>(coords)[ft.data_offset + i];
+    *x = xy.x;
+    *y = xy.y;
+  }
+}
+
+// Evaluation with the packed two-pixel loop: as k_fit_eval, each thread
+// takes pixel pairs (i, i + TPB) of its tile; PPT is even.  The records in
+// coef32 are in the pair layout (stage_pair).
+template <int TPB, int PPT, int MINB, bool kRecompute>
+__global__ void __launch_bounds__(TPB, MINB)
+k_fit_eval_pair(FitCtx c) {
+  static_assert(PPT % 2 == 0, "pixel pairs");
+  extern __shared__ __align__(16) char smem[];
+  float4* rec = reinterpret_cast<float4*>(smem);
+  __shared__ float red[(TPB / 32) * FIT_NSUM];
+  __shared__ int s_tile;
+  const int ntiles = c.counters[2];
+  const int nmaxp = c.nmax_cap + 1;
+  const bool bohren = c.flags & LMB_BOHREN;
+  const float kf = float(c.k);
+  const float inv_noise = float(c.inv_noise);
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(c.counters, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= ntiles) break;
+    const int2 tile = c.tiles[t];
+    const int f = tile.x;
+    if (!c.ev[f].active) {
+      __syncthreads();
+      continue;
+    }
+    const int nm = min(max(c.nmax[f], 0), nmaxp - 1);
+    {
+      const float4* src =
+          reinterpret_cast<const float4*>(c.coef32) + size_t(f) * nmaxp * PAIR_QUADS;
+      for (int i = threadIdx.x; i < PAIR_QUADS * (nm + 1); i += TPB) rec[i] = src[i];
+    }
+    const lmb_feature ft = c.features[f];
+    const EvalPoint ep = c.ev[f];
+    __syncthreads();
+    float acc[FIT_NSUM];
+#pragma unroll
+    for (int j = 0; j < FIT_NSUM; ++j) acc[j] = 0.f;
+    long long lim = (long long)tile.y + c.tile_pixels;
+    if (lim > ft.npix) lim = ft.npix;
+    for (int q = 0; q < PPT; q += 2) {
+      const long long i0 = (long long)tile.y + q * TPB + threadIdx.x;
+      if (i0 >= lim) break;
+      const long long i1r = i0 + TPB;
+      const bool v1 = i1r < lim;
+      const long long i1 = v1 ? i1r : i0;
+      double x0, y0, x1, y1;
+      fit_pixel_xy(ft, c.coords, i0, &x0, &y0);
+      fit_pixel_xy(ft, c.coords, i1, &x1, &y1);
+      const float d0 = c.data[ft.data_offset + i0];
+      const float d1 = c.data[ft.data_offset + i1];
+      const double dx[2] = {x0 - ep.p[0], x1 - ep.p[0]};
+      const double dy[2] = {y0 - ep.p[1], y1 - ep.p[1]};
+      float H[2], dH[2][6];
+      holo_jac_pair<kRecompute>(c.k, dx, dy, -ep.p[2], ep.p[2], bohren, rec, nm,
+                                kf, H, dH);
+#pragma unroll
+      for (int lane = 0; lane < 2; ++lane) {
+        if (lane == 1 && !v1) break;
+        const float r = (H[lane] - (lane ? d1 : d0)) * inv_noise;
+        float J[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) J[j] = dH[lane][j] * inv_noise;
+        acc[0] += r * r;
+        int o = 1;
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+          for (int b = a; b < 6; ++b) acc[o++] += J[a] * J[b];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) acc[22 + a] += J[a] * r;
+      }
+    }
+    block_reduce<FIT_NSUM, TPB>(acc, red);
+    if (threadIdx.x < FIT_NSUM)
+      c.partial[(size_t)t * FIT_NSUM + threadIdx.x] = red[threadIdx.x];
+    if (threadIdx.x == 0) {
+      const long long np = lim - tile.y;
       atomicAdd(c.work, (unsigned long long)np);
       atomicAdd(c.work + 1, (unsigned long long)np * (unsigned long long)nm);
     }
@@ -795,11 +915,16 @@ k_fit_step(FitCtx c) {
                         w, c.ab + size_t(f) * nmaxp * 2, c.dab + size_t(f) * nmaxp * 4,
                         c.nmax + f);
   }
-  if (st == LMB_OK)
-    stage_coef<float, true>(c.ab + size_t(f) * nmaxp * 2,
-                            c.dab + size_t(f) * nmaxp * 4,
-                            min(c.nmax[f], nmaxp - 1),
-                            c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
+  if (st == LMB_OK) {
+    const zd* abf = c.ab + size_t(f) * nmaxp * 2;
+    const zd* dabf = c.dab + size_t(f) * nmaxp * 4;
+    const int nm = min(c.nmax[f], nmaxp - 1);
+    if (c.pair_records)
+      stage_pair(abf, dabf, nm,
+                 reinterpret_cast<float4*>(c.coef32) + size_t(f) * nmaxp * PAIR_QUADS);
+    else
+      stage_coef<float, true>(abf, dabf, nm, c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
+  }
   if (lane == 0) {
     if (st != LMB_OK) {
       gs->phase = LM_PHASE_DONE;

@@ -100,6 +100,44 @@ LMB_HD cplx<float> cis(float t) {
   return mk(c, s);
 }
 
+// Two FP32 lanes in one register pair, operated on by the packed sm_100
+// instructions (fma/mul/add .rn.f32x2: each lane rounds exactly like its
+// scalar counterpart, so the host emulation below is bit-identical).
+#if defined(__CUDACC__)
+typedef float2 f2;
+#else
+struct f2 {
+  float x, y;
+};
+#endif
+LMB_HD f2 pk(float x, float y) {
+  f2 r;
+  r.x = x;
+  r.y = y;
+  return r;
+}
+LMB_HD f2 pfma(f2 a, f2 b, f2 c) {
+#if defined(__CUDA_ARCH__)
+  return __ffma2_rn(a, b, c);
+#else
+  return pk(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+LMB_HD f2 pmul(f2 a, f2 b) {
+#if defined(__CUDA_ARCH__)
+  return __fmul2_rn(a, b);
+#else
+  return pk(a.x * b.x, a.y * b.y);
+#endif
+}
+LMB_HD f2 padd(f2 a, f2 b) {
+#if defined(__CUDA_ARCH__)
+  return __fadd2_rn(a, b);
+#else
+  return pk(a.x + b.x, a.y + b.y);
+#endif
+}
+
 LMB_HD float lsqrt(float x) { return sqrtf(x); }
 LMB_HD double lsqrt(double x) { return sqrt(x); }
 LMB_HD float labs_(float x) { return fabsf(x); }

@@ -317,6 +317,182 @@ LMB_HD JacSums<R> order_sum_jac(const Geometry<R>& g, const Quad<R>* coef,
   return A;
 }
 
+// ---------------------------------------------------------------------------
+// The Jacobian order loop for two pixels of one particle at once, in packed
+// two-lane FP32 (one pfma does the work of two scalar FMAs in one issue
+// slot).  Same recurrences and sums as order_sum_jac; the differences are
+// signs chosen so that every update is a plain fused multiply-add:
+//  * h'_n = s_n h~_n with s_n = +1, -1, -1, +1 for n = 0, 1, 2, 3 (mod 4):
+//      h'_n = [(-1)^n (2n-1) ikr] h'_{n-1} + h'_{n-2}
+//    and the same sign on the kr tangent hp'_n;
+//  * dh''_n = sig_n dh_n with sig_n = (-1)^{n+1} s_n:
+//      dh''_n = [(-1)^{n+1} n ikr] h'_n + h'_{n-1}
+//    (and the same for the tangent, with -ikr2 terms from the chain rule);
+//  * the Wiscombe state keeps -Delta_n, so that tau_n = pi_{n-1} +
+//    n (s pi_n - Delta_n) and Delta_{n+1} follow from one shared sum;
+//  * the signs s_n, sig_n and the minus of the beta terms are folded into
+//    the per-order coefficients, which also carry -Im of every complex
+//    coefficient (a complex product is then two multiplies and two fmas).
+// Per order: PAIR_VALUES values, each duplicated into both lanes (float2):
+//   0 n, 1 c_n = 1 + 1/n, 2 (-1)^n (2n-1), 3 (-1)^{n+1} n,
+//   then nine complex coefficients as (re, im, -im):
+//   4 sig alpha, 7 -s beta, 10 s n(n+1) alpha, 13..21 the same for
+//   d/da_p, 22..30 for d/dn_p; 31 unused.
+enum { PAIR_VALUES = 32, PAIR_QUADS = PAIR_VALUES / 2 };
+
+struct PairIn {
+  f2 sv;              // s = 1 - |cos(theta)|
+  f2 ikr;             // sign(mu) / kr
+  f2 nikr2;           // -sign(mu) / kr^2
+  cplx<f2> hm1, h0;   // h_{-1}, h~_0
+};
+
+struct PairSums {
+  cplx<f2> s[3], t[3], u[3], a[3], p[3];
+};
+
+// c * v for a coefficient stored as (re, im, -im)
+LMB_HD cplx<f2> pcmul(f2 re, f2 im, f2 nim, cplx<f2> v) {
+  return mk(pfma(re, v.re, pmul(nim, v.im)), pfma(re, v.im, pmul(im, v.re)));
+}
+// acc + w v
+LMB_HD cplx<f2> pacc(cplx<f2> acc, f2 w, cplx<f2> v) {
+  return mk(pfma(w, v.re, acc.re), pfma(w, v.im, acc.im));
+}
+
+// rec: PAIR_QUADS float4 per order (index n * PAIR_QUADS + j); the two
+// values of a float4 are (x, y) and (z, w).
+template <typename Q4>
+LMB_HD void order_sum_jac_pair(const PairIn& in, const Q4* rec, int nmax,
+                               PairSums& A) {
+  const f2 z2 = pk(0.f, 0.f), m1 = pk(-1.f, -1.f);
+  const cplx<f2> zero = mk(z2, z2);
+  for (int c = 0; c < 3; ++c) {
+    A.s[c] = zero;
+    A.t[c] = zero;
+    A.u[c] = zero;
+    A.a[c] = zero;
+    A.p[c] = zero;
+  }
+  f2 pim1 = z2, pi = pk(1.f, 1.f), nd = m1;  // nd = -Delta
+  f2 dpim1 = z2, dpi = z2, ndd = z2;         // d/ds
+  cplx<f2> h2 = in.hm1, h1 = in.h0, hp2 = zero, hp1 = zero;
+  const f2 sv = in.sv, ikr = in.ikr, nikr2 = in.nikr2;
+#pragma unroll 2
+  for (int n = 1; n <= nmax; ++n) {
+    const Q4* r = rec + PAIR_QUADS * n;
+    f2 v[PAIR_VALUES];
+#pragma unroll
+    for (int j = 0; j < PAIR_QUADS; ++j) {
+      const Q4 q = r[j];
+      v[2 * j] = pk(q.x, q.y);
+      v[2 * j + 1] = pk(q.z, q.w);
+    }
+    const f2 fn = v[0], cn = v[1], tns = v[2], fns = v[3];
+    // Wiscombe pi, tau and their s tangents
+    const f2 spi = pmul(sv, pi);
+    const f2 w = padd(nd, spi);
+    const f2 tau = pfma(fn, w, pim1);
+    const f2 ndn = pfma(cn, w, spi);
+    const f2 dspi = pfma(sv, dpi, pi);
+    const f2 wd = padd(ndd, dspi);
+    const f2 dtau = pfma(fn, wd, dpim1);
+    const f2 nddn = pfma(cn, wd, dspi);
+    // Riccati-Bessel recurrences (signed as described above)
+    const f2 a2 = pmul(tns, ikr), a1 = pmul(fns, ikr);
+    const f2 b2 = pmul(tns, nikr2), b1 = pmul(fns, nikr2);
+    const cplx<f2> h = mk(pfma(a2, h1.re, h2.re), pfma(a2, h1.im, h2.im));
+    const cplx<f2> dh = mk(pfma(a1, h.re, h1.re), pfma(a1, h.im, h1.im));
+    const cplx<f2> hp = mk(pfma(a2, hp1.re, pfma(b2, h1.re, hp2.re)),
+                           pfma(a2, hp1.im, pfma(b2, h1.im, hp2.im)));
+    const cplx<f2> dhp = mk(pfma(a1, hp.re, pfma(b1, h.re, hp1.re)),
+                            pfma(a1, hp.im, pfma(b1, h.im, hp1.im)));
+    // value and the s tangent
+    {
+      const cplx<f2> X = pcmul(v[4], v[5], v[6], dh);
+      const cplx<f2> Y = pcmul(v[7], v[8], v[9], h);
+      const cplx<f2> Z = pcmul(v[10], v[11], v[12], h);
+      A.s[0] = pacc(A.s[0], pi, Z);
+      A.s[1] = pacc(pacc(A.s[1], tau, X), pi, Y);
+      A.s[2] = pacc(pacc(A.s[2], pi, X), tau, Y);
+      A.u[0] = pacc(A.u[0], dpi, Z);
+      A.u[1] = pacc(pacc(A.u[1], dtau, X), dpi, Y);
+      A.u[2] = pacc(pacc(A.u[2], dpi, X), dtau, Y);
+    }
+    // kr tangent
+    {
+      const cplx<f2> X = pcmul(v[4], v[5], v[6], dhp);
+      const cplx<f2> Y = pcmul(v[7], v[8], v[9], hp);
+      const cplx<f2> Z = pcmul(v[10], v[11], v[12], hp);
+      A.t[0] = pacc(A.t[0], pi, Z);
+      A.t[1] = pacc(pacc(A.t[1], tau, X), pi, Y);
+      A.t[2] = pacc(pacc(A.t[2], pi, X), tau, Y);
+    }
+    // a_p
+    {
+      const cplx<f2> X = pcmul(v[13], v[14], v[15], dh);
+      const cplx<f2> Y = pcmul(v[16], v[17], v[18], h);
+      const cplx<f2> Z = pcmul(v[19], v[20], v[21], h);
+      A.a[0] = pacc(A.a[0], pi, Z);
+      A.a[1] = pacc(pacc(A.a[1], tau, X), pi, Y);
+      A.a[2] = pacc(pacc(A.a[2], pi, X), tau, Y);
+    }
+    // n_p
+    {
+      const cplx<f2> X = pcmul(v[22], v[23], v[24], dh);
+      const cplx<f2> Y = pcmul(v[25], v[26], v[27], h);
+      const cplx<f2> Z = pcmul(v[28], v[29], v[30], h);
+      A.p[0] = pacc(A.p[0], pi, Z);
+      A.p[1] = pacc(pacc(A.p[1], tau, X), pi, Y);
+      A.p[2] = pacc(pacc(A.p[2], pi, X), tau, Y);
+    }
+    pim1 = pi;
+    pi = pfma(m1, ndn, pi);
+    nd = ndn;
+    dpim1 = dpi;
+    dpi = pfma(m1, nddn, dpi);
+    ndd = nddn;
+    h2 = h1;
+    h1 = h;
+    hp2 = hp1;
+    hp1 = hp;
+  }
+}
+
+// One lane of the packed sums as the scalar loop's JacSums, with the same
+// parity unfolding and s -> mu conversion at the end of order_sum_jac.
+LMB_HD JacSums<float> pair_lane(const PairSums& P, int lane, float sg) {
+  JacSums<float> A;
+  for (int c = 0; c < 3; ++c) {
+#define LMB_LANE(dst, src)                                   \
+  dst[c] = lane ? mk(src[c].re.y, src[c].im.y) : mk(src[c].re.x, src[c].im.x)
+    LMB_LANE(A.s, P.s);
+    LMB_LANE(A.t, P.t);
+    LMB_LANE(A.u, P.u);
+    LMB_LANE(A.a, P.a);
+    LMB_LANE(A.p, P.p);
+#undef LMB_LANE
+  }
+  A.s[2] = sg * A.s[2];
+  A.a[2] = sg * A.a[2];
+  A.p[2] = sg * A.p[2];
+  A.t[2] = sg * A.t[2];
+  A.u[0] = (-sg) * A.u[0];
+  A.u[1] = (-sg) * A.u[1];
+  A.u[2] = -A.u[2];
+  return A;
+}
+
+LMB_HD PairIn pair_in(const Geometry<float>& g0, const Geometry<float>& g1) {
+  PairIn in;
+  in.sv = pk(g0.s1mu, g1.s1mu);
+  in.ikr = pk(g0.ikrs, g1.ikrs);
+  in.nikr2 = pk(-(g0.ikrs * g0.ikr), -(g1.ikrs * g1.ikr));
+  in.hm1 = mk(pk(g0.hm1.re, g1.hm1.re), pk(g0.hm1.im, g1.hm1.im));
+  in.h0 = mk(pk(g0.h0.re, g1.h0.re), pk(g0.h0.im, g1.h0.im));
+  return in;
+}
+
 // Dual numbers over the three displacement coordinates (kx, ky, kz).
 template <typename R>
 struct dr3 {

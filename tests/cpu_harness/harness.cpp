@@ -14,6 +14,7 @@
 #include "lmb_lm.cuh"
 #include "lmb_mie.cuh"
 #include "lmb_pixel.cuh"
+#include "lmb_records.cuh"
 
 using namespace lmb;
 
@@ -104,39 +105,29 @@ API int h_layered_ab(const double* radii, const double* idx, int L, double n_m,
   return 0;
 }
 
-static zd rot_i(zd z, int k) {
-  switch (k & 3) {
-    case 0: return z;
-    case 1: return mk(-z.im, z.re);
-    case 2: return mk(-z.re, -z.im);
-    default: return mk(z.im, -z.re);
-  }
-}
-
+// Records staged exactly as the kernels stage them (lmb_records.cuh).
 template <typename R>
 static void stage(const double* ab, const double* dab, int nmax, Quad<R>* q,
                   int w) {
   for (int n = 0; n <= nmax; ++n) {
-    Quad<R> r[JAC_QUADS];
-    memset(r, 0, sizeof(r));
-    if (n > 0) {
-      const double fn = n, nn1 = fn * (fn + 1.), en = (2. * fn + 1.) / nn1;
-      const zd a = mk(ab[4 * n], ab[4 * n + 1]), b = mk(ab[4 * n + 2], ab[4 * n + 3]);
-      const zd al = en * rot_i(a, n + 1), be = en * rot_i(b, n);
-      r[0] = Quad<R>{R(al.re), R(al.im), R(be.re), R(be.im)};
-      r[1] = Quad<R>{R(nn1 * al.re), R(nn1 * al.im), R(1. + 1. / fn), R(fn)};
-      if (w == JAC_QUADS) {
-        zd d[4];
-        for (int j = 0; j < 4; ++j) d[j] = mk(dab[8 * n + 2 * j], dab[8 * n + 2 * j + 1]);
-        const zd ala = en * rot_i(d[0], n + 1), bea = en * rot_i(d[1], n);
-        const zd aln = en * rot_i(d[2], n + 1), ben = en * rot_i(d[3], n);
-        r[2] = Quad<R>{R(ala.re), R(ala.im), R(bea.re), R(bea.im)};
-        r[3] = Quad<R>{R(aln.re), R(aln.im), R(ben.re), R(ben.im)};
-        r[4] = Quad<R>{R(nn1 * ala.re), R(nn1 * ala.im), R(nn1 * aln.re),
-                       R(nn1 * aln.im)};
-      }
-    }
-    for (int j = 0; j < w; ++j) q[w * n + j] = r[j];
+    zd a[2], d[4];
+    for (int j = 0; j < 2; ++j) a[j] = mk(ab[4 * n + 2 * j], ab[4 * n + 2 * j + 1]);
+    if (w == JAC_QUADS)
+      for (int j = 0; j < 4; ++j) d[j] = mk(dab[8 * n + 2 * j], dab[8 * n + 2 * j + 1]);
+    order_record<R>(a, d, n, w, q + w * n);
+  }
+}
+
+static void stage_pair_host(const double* ab, const double* dab, int nmax,
+                            Quad<float>* q) {
+  for (int n = 0; n <= nmax; ++n) {
+    zd a[2], d[4];
+    for (int j = 0; j < 2; ++j) a[j] = mk(ab[4 * n + 2 * j], ab[4 * n + 2 * j + 1]);
+    for (int j = 0; j < 4; ++j) d[j] = mk(dab[8 * n + 2 * j], dab[8 * n + 2 * j + 1]);
+    float v[PAIR_VALUES];
+    pair_record(a, d, n, v);
+    for (int j = 0; j < PAIR_QUADS; ++j)
+      q[PAIR_QUADS * n + j] = Quad<float>{v[2 * j], v[2 * j], v[2 * j + 1], v[2 * j + 1]};
   }
 }
 
@@ -198,6 +189,39 @@ API void h_jacobian(const double* coords, long long npts, const double* p,
     jac_one<double>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac);
   else
     jac_one<float>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac);
+}
+
+// Hologram and Jacobian of one sphere through the packed two-pixel loop
+// (pixels i and i + 1 share one pass; an odd last pixel is paired with
+// itself), FP32 only.
+API void h_jacobian_pair(const double* coords, long long npts, const double* p,
+                     const double* ab, const double* dab, int nmax, double k,
+                     int flags, double* holo, double* jac) {
+  std::vector<Quad<float>> q(PAIR_QUADS * (nmax + 1));
+  stage_pair_host(ab, dab, nmax, q.data());
+  for (long long i = 0; i < npts; i += 2) {
+    const long long i1 = i + 1 < npts ? i + 1 : i;
+    Geometry<float> g[2];
+    for (int l = 0; l < 2; ++l) {
+      const long long ii = l ? i1 : i;
+      const double x = coords[ii], y = coords[npts + ii], z = coords[2 * npts + ii];
+      g[l] = geometry<float>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
+    }
+    PairSums P;
+    order_sum_jac_pair(pair_in(g[0], g[1]), q.data(), nmax, P);
+    for (int l = 0; l < 2; ++l) {
+      const long long ii = l ? i1 : i;
+      const JacSums<float> A = pair_lane(P, l, g[l].smu);
+      cplx<float> e[3], de[6][3];
+      epilogue_jac<float>(g[l], A, float(k), e, de);
+      holo[ii] = intensity<float>(e);
+      const cplx<float> et0 = mk(e[0].re + 1.f, e[0].im);
+      for (int j = 0; j < 6; ++j)
+        jac[j * npts + ii] = 2.f * (et0.re * de[j][0].re + et0.im * de[j][0].im +
+                                    e[1].re * de[j][1].re + e[1].im * de[j][1].im +
+                                    e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+    }
+  }
 }
 
 // Levenberg-Marquardt state machine driven from Python.

@@ -44,6 +44,9 @@ def load():
     lib.h_jacobian.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
                                ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                ctypes.c_int, _dp, _dp]
+    lib.h_jacobian_pair.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
+                                    ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_int, _dp, _dp]
     lib.h_lm_new.restype = ctypes.c_void_p
     lib.h_lm_new.argtypes = [ctypes.c_int, _ip, _dp] + [ctypes.c_double] * 4 + [ctypes.c_int]
     lib.h_lm_free.argtypes = [ctypes.c_void_p]
@@ -134,4 +137,17 @@ class Harness:
         self.lib.h_jacobian(ptr(c), npts, ptr(pv), ptr(a), ptr(d), n, k,
                             1 | (2 if bohren else 0), int(fp64), ptr(holo),
                             ptr(jac))
+        return holo, jac
+
+    def jacobian_pair(self, coords, p, ab, dab, k, bohren=True):
+        '''As jacobian (FP32), through the packed two-pixel order loop.'''
+        c = np.ascontiguousarray(coords, dtype=float)
+        npts = c.shape[1]
+        n, a, d = self._pack_ab(ab, dab)
+        holo = np.zeros(npts)
+        jac = np.zeros((6, npts))
+        pv = np.asarray(p, dtype=float)
+        self.lib.h_jacobian_pair(ptr(c), npts, ptr(pv), ptr(a), ptr(d), n, k,
+                                 1 | (2 if bohren else 0), ptr(holo),
+                                 ptr(jac))
         return holo, jac

@@ -181,3 +181,36 @@ def test_layered_one_layer_matches_reference(h, golden_layered):
         ab = h.layered_ab([a.real], [n], nm.real, lam.real)
         ref = golden_layered[f'ab_{i}']
         assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize('shape,p', [
+    ((48, 48), [20.3, 25.7, 120., 0.9, 1.6, 0.01]),
+    ((40, 40), [20., 20., -130., 0.6, 1.5, 0.]),
+    ((33, 33), [16., 16., 80., 1.0, 1.4, 0.]),
+    ((21, 31), [15.2, 10.1, 60., 2.5, 1.7, 0.002]),
+])
+def test_jacobian_pair_loop(h, shape, p):
+    '''The packed two-pixel loop (signed recurrences, pair records) gives the
+    scalar loop's hologram and Jacobian to FP32 rounding, and the FD
+    Jacobian of the oracle to the scalar loop's tolerance.'''
+    c = field.coordinates3(field.meshgrid(shape))
+    ab, dab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447, deriv=True)
+    H1, J1 = h.jacobian(c, p[:3], ab, dab, K, True, 0)
+    H2, J2 = h.jacobian_pair(c, p[:3], ab, dab, K, True)
+    # FP32 rounding differs in order only: relative to the hologram's size
+    assert np.all(np.abs(H2 - H1) < 1e-5 + 4e-6 * np.abs(H1))
+    for j in range(6):
+        scale = np.abs(J1[j]).max()
+        assert np.abs(J2[j] - J1[j]).max() < 1e-4 * scale, KEYS[j]
+    inst = field.DEFAULT_INSTRUMENT
+    h0 = field.hologram(c, [dict(zip(KEYS, p))], inst)
+    assert np.all(np.abs(H2 - h0) < 2e-5 + 2e-6 * np.abs(h0))
+    for j in range(6):
+        step = 1e-5 * max(abs(p[j]), 1e-2) if j < 5 else 1e-7
+        pp, pm = list(p), list(p)
+        pp[j] += step
+        pm[j] -= step
+        fd = (field.hologram(c, [dict(zip(KEYS, pp))], inst) -
+              field.hologram(c, [dict(zip(KEYS, pm))], inst)) / (2 * step)
+        err = np.abs(J2[j] - fd).max() / np.abs(fd).max()
+        assert err < 3e-4, (KEYS[j], err)

@@ -134,3 +134,58 @@ def test_autotuned_batch_matches_default(tmp_path, monkeypatch):
     assert (tmp_path / 'tune.json').exists()
     for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p'):
         assert np.all(np.abs(d0[k] - d1[k]) <= TOL[k] * 0.1)
+
+
+def test_every_launch_shape_gives_the_same_fit():
+    '''All evaluation kernels (CTA tiles, warp tiles, packed two-pixel loop)
+    on one batch of mixed crops, odd tile ends and explicit-coordinate
+    features included: the same fit as shape 0.  The shapes sum the normal
+    equations in different orders, so on small crops, where the chi^2
+    surface is flat within FP32 rounding, the stopping point may move: each
+    parameter must agree within the target or a third of its uncertainty,
+    and chi^2 to 1e-3.'''
+    import torch
+    from pylorenzmie_b200 import autotune, Instrument, _native
+    from pylorenzmie_b200.analysis import _fit
+    rng = np.random.default_rng(11)
+    items, starts = [], []
+    for i in range(12):
+        s = int(rng.choice([61, 71, 81, 101]))
+        c = (s - 1) / 2.
+        truth = [c + rng.uniform(-2, 2), c + rng.uniform(-2, 2),
+                 rng.uniform(120., 200.), rng.uniform(0.8, 1.2),
+                 rng.uniform(1.38, 1.6), 0.]
+        data = _render(500 + i, (s, s), truth)
+        start = list(truth)
+        start[2] += 12.
+        start[3] *= 1.04
+        start[4] += 0.02
+        if i % 3 == 2:  # a random 60 % of the pixels, explicit coordinates
+            keep = rng.random(s * s) < 0.6
+            coords = ofield.meshgrid((s, s))[:, keep]
+            items.append((data[keep], None, coords))
+        else:
+            items.append((data, (0., 0., s, s), None))
+        starts.append(start)
+    starts = np.array(starts)
+    inst = Instrument()
+    variables = ['x_p', 'y_p', 'z_p', 'a_p', 'n_p']
+    packed = _fit.PackedFeatures(items)
+    ref = None
+    for idx, tpb, ppt, minb in autotune.shapes():
+        d_feat, d_data, d_coords, d_params = _fit.upload(packed, starts)
+        d_res, _ = _fit.fit_device(d_feat, d_data, d_coords, d_params, 12,
+                                   packed.total, inst, variables, None,
+                                   None, starts, tile_config=idx)
+        p = d_params.view(torch.float64).reshape(12, 6).cpu().numpy()
+        r = d_res[:12 * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
+            _native.RESULT_DTYPE)
+        assert r['success'].all(), idx
+        if ref is None:
+            ref, rref = p, r.copy()
+            continue
+        for j, k in enumerate(KEYS[:5]):
+            bound = np.maximum(TOL[k], rref['dparams'][:, j] / 3.)
+            assert np.all(np.abs(p[:, j] - ref[:, j]) <= bound), \
+                (idx, tpb, ppt, minb, k, p[:, j] - ref[:, j], bound)
+        assert np.all(np.abs(r['redchi'] / rref['redchi'] - 1) < 1e-3), idx
