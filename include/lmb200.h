@@ -27,6 +27,7 @@ extern "C" {
 #define LMB_ERR_NMAX 3         /* a sphere needs more orders than nmax_cap */
 #define LMB_ERR_WORKSPACE 4    /* workspace too small */
 #define LMB_ERR_UNSUPPORTED 5  /* flag combination not supported */
+#define LMB_ERR_TIMEOUT 6      /* streamed fit: data did not arrive in time */
 
 /* flags */
 #define LMB_CARTESIAN 1   /* project the field on x, y, z (else r, theta, phi) */
@@ -184,7 +185,8 @@ typedef struct lmb_fit_result {
   double cost;        /* 0.5 * sum of squared residuals */
   int status;         /* scipy least_squares status: 1..4 success, 0 max_nfev,
                          <0 failure (-1 improper input, -2 non-finite
-                         residuals, -3 nmax above cap) */
+                         residuals, -3 nmax above cap, -4 withdrawn before
+                         its data arrived: lmb_fit_batch_streamed) */
   int success;
   int nfev, njev;
 } lmb_fit_result;
@@ -258,6 +260,52 @@ int lmb_fit_batch_layered(const lmb_feature *features, int nfeatures,
                           lmb_fit_result *results, void *workspace,
                           size_t workspace_bytes, lmb_fit_stats *stats,
                           void *stream);
+
+/*
+ * Host-side packing: concatenate nsources crops (sources[i]: counts[i]
+ * contiguous values, LMB_PACK_F64 doubles or LMB_PACK_F32 floats) as
+ * float32 into dst, on up to nthreads native threads (a persistent pool;
+ * the calling thread takes a share).  For the pinned staging buffer of a
+ * batched or streamed fit.  No counterpart in the reference, whose fits
+ * subtract float64 data on the host (analysis/Optimizer.py:257-260).
+ */
+#define LMB_PACK_F64 0
+#define LMB_PACK_F32 1
+int lmb_pack_crops(const void *const *sources, const long long *counts,
+                   int nsources, int src_type, float *dst, int nthreads);
+
+/*
+ * lmb_fit_batch (any layer count) that starts before all of its pixel data
+ * is on the device.  No counterpart in the reference, whose fits run one
+ * feature at a time on the host.
+ *
+ * The feature records, params (start values) and, for layered spheres,
+ * the layer arrays must be on the device when the call is made (they are
+ * read by its first kernel).  The pixel data (and explicit coordinates)
+ * may still be arriving: features are admitted in order as the caller
+ * advances the device int *ready -- features [0, *ready) have their data
+ * in place -- which the caller writes on another stream (or from another
+ * thread) after each portion of the data has been copied, for example with
+ * cudaMemcpyAsync of the new count on the copy's stream.  Admitted features
+ * start their Levenberg-Marquardt iterations at the next round while the
+ * others wait, so the host's conversion and transfer of later features
+ * overlaps the fitting of earlier ones.  A negative *ready withdraws the
+ * batch: features not yet admitted end with status -4.  The call returns
+ * LMB_ERR_TIMEOUT if no feature is running and no new feature has been
+ * admitted for wait_seconds.  nlayers = 1 with null layer arrays fits
+ * homogeneous spheres.
+ */
+int lmb_fit_batch_streamed(const lmb_feature *features, int nfeatures,
+                           long long total_pixels, const float *data,
+                           const float *coords, lmb_sphere *params,
+                           int nlayers, const double *layer_fractions,
+                           const double *layer_indices, double n_m,
+                           double wavelength, double magnification,
+                           double noise, int nmax_cap,
+                           const lmb_fit_settings *settings, const int *ready,
+                           double wait_seconds, lmb_fit_result *results,
+                           void *workspace, size_t workspace_bytes,
+                           lmb_fit_stats *stats, void *stream);
 
 /*
  * lmb_fit_batch for callers that cannot allocate device memory.  No

@@ -17,6 +17,9 @@ LMB_ERR_CUDA = 2
 LMB_ERR_NMAX = 3
 LMB_ERR_WORKSPACE = 4
 LMB_ERR_UNSUPPORTED = 5
+LMB_ERR_TIMEOUT = 6
+LMB_PACK_F64 = 0
+LMB_PACK_F32 = 1
 
 LMB_CARTESIAN = 1
 LMB_BOHREN = 2
@@ -85,12 +88,18 @@ _SIGNATURES = {
                                    _d, _d, _d, _d, _i,
                                    ctypes.POINTER(FitSettings), _vp, _vp, _sz,
                                    ctypes.POINTER(FitStats), _vp]),
+    'lmb_fit_batch_streamed': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _i, _vp,
+                                    _vp, _d, _d, _d, _d, _i,
+                                    ctypes.POINTER(FitSettings), _vp, _d,
+                                    _vp, _vp, _sz, ctypes.POINTER(FitStats),
+                                    _vp]),
     'lmb_fit_tile_config': (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i),
                                  ctypes.POINTER(_i)]),
     'lmb_fit_batch': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _d, _d, _d, _d, _i,
                            ctypes.POINTER(FitSettings), _vp, _vp, _sz,
                            ctypes.POINTER(FitStats), _vp]),
     'lmb_measure_fp32_peak': (_i, [ctypes.POINTER(_d), _vp]),
+    'lmb_pack_crops': (_i, [_vp, _vp, _i, _i, _vp, _i]),
 }
 
 _lock = threading.Lock()

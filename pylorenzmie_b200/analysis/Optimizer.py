@@ -264,7 +264,7 @@ class Optimizer(LMObject):
 
     # ------------------------------------------------------------------
     def optimize_batch(self, holograms, particles=None, starts=None,
-                       autotune=None):
+                       autotune=None, chunks=None):
         '''Fit one sphere per hologram, all on the device in one call.
 
         holograms : list of Hologram (crops; any sizes)
@@ -276,6 +276,10 @@ class Optimizer(LMObject):
         autotune  : time the evaluation kernel's launch shapes once per
                     problem class and use the fastest (default: batches of
                     64 features or more)
+        chunks    : pipeline depth: the batch is fitted in this many parts,
+                    each on its own stream, so that converting and copying
+                    one part overlaps the fit of the previous one (default:
+                    1 below ~2 Mpx, up to 4 above)
         Returns a DataFrame, one row per feature, with the columns of
         ``result`` plus ``status`` and ``nfev``.
         '''
@@ -292,17 +296,16 @@ class Optimizer(LMObject):
                 getattr(p, 'r_0', (0., 0., 0.)), float)), p.a_p, p.n_p,
                 getattr(p, 'k_p', 0.)] for p in particles], dtype=float)
         items = [self._pixels(h) for h in holograms]
-        packed = _fit.PackedFeatures(items)
         if autotune is None:
             autotune = len(holograms) >= 64
-        params, res = _fit.fit_packed(packed, starts, self.model.instrument,
-                                      self.variables, self.settings,
-                                      device=self.model.device, layers=layers,
-                                      autotune=autotune)
-        return batch_frame(params, res, packed, self.variables)
+        params, res, npix = _fit.fit_items(
+            items, starts, self.model.instrument, self.variables,
+            self.settings, device=self.model.device, layers=layers,
+            autotune=autotune, chunks=chunks)
+        return batch_frame(params, res, npix, self.variables)
 
 
-def batch_frame(params, res, packed, variables):
+def batch_frame(params, res, npix, variables):
     '''DataFrame of batched fit results in the Optimizer.result layout.'''
     idx = [PARAM_KEYS.index(v) for v in variables]
     cols = {}
@@ -310,7 +313,7 @@ def batch_frame(params, res, packed, variables):
         cols[v] = params[:, j]
         cols['d' + v] = res['dparams'][:, j]
     cols['success'] = res['success'].astype(bool)
-    cols['npix'] = packed.features['npix']
+    cols['npix'] = np.asarray(npix)
     cols['redchi'] = res['redchi']
     cols['status'] = res['status']
     cols['nfev'] = res['nfev']

@@ -105,23 +105,51 @@ class PackedFeatures:
 
     def write_data(self, out):
         '''Convert every crop into the float32 array ``out`` (total,).'''
-        offs = self.features['data_offset']
+        return self.write_range(out, 0, len(self._sources))
 
-        def work(lo, hi):
-            for i in range(lo, hi):
-                src = self._sources[i]
-                n = src.size
-                np.copyto(out[offs[i]:offs[i] + n], src.reshape(-1),
-                          casting='unsafe')
-        nf = len(self._sources)
+    def write_range(self, out, lo, hi):
+        '''Convert crops lo..hi-1 into their places in ``out`` (total,).
+        The crops are contiguous in ``out``; the range is cut into equal
+        runs of pixels, one per thread, whatever the crop sizes.  Float64
+        or float32 crops are converted by the library's native threads
+        (lmb_pack_crops), others by numpy.'''
+        if hi <= lo:
+            return out
+        offs = self.features['data_offset']
+        npix = self.features['npix']
+        begin = int(offs[lo])
+        end = int(offs[hi - 1] + npix[hi - 1])
+        srcs = self._sources[lo:hi]
+        kind = _pack_kind(srcs)
+        if kind is not None and out.dtype == np.float32 and \
+                out.flags.c_contiguous:
+            ptrs = np.array([s.ctypes.data for s in srcs], dtype=np.uintp)
+            counts = np.ascontiguousarray(npix[lo:hi], dtype=np.int64)
+            _native.check(_native.load().lmb_pack_crops(
+                ptrs.ctypes.data, counts.ctypes.data, hi - lo, kind,
+                out[begin:].ctypes.data, _pack_threads()), 'lmb_pack_crops')
+            return out
+
+        def work(a, b):  # pixels [a, b) of the packed buffer
+            i = int(np.searchsorted(offs, a, side='right')) - 1
+            while a < b:
+                n0 = int(offs[i])
+                n = int(npix[i])
+                s0, s1 = a - n0, min(b, n0 + n) - n0
+                if s1 > s0:
+                    np.copyto(out[n0 + s0:n0 + s1],
+                              self._sources[i].reshape(-1)[s0:s1],
+                              casting='unsafe')
+                a = n0 + s1 if s1 > s0 else a
+                i += 1
         pool = _pool()
-        if pool is None or self.total < (1 << 20) or nf < 4:
-            work(0, nf)
+        if pool is None or end - begin < (1 << 19):
+            work(begin, end)
             return out
         nthreads = pool._max_workers
-        step = (nf + nthreads - 1) // nthreads
-        futs = [pool.submit(work, lo, min(lo + step, nf))
-                for lo in range(0, nf, step)]
+        cuts = np.linspace(begin, end, nthreads + 1).astype(np.int64)
+        futs = [pool.submit(work, int(a), int(b))
+                for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
         for f in futs:
             f.result()
         return out
@@ -143,13 +171,39 @@ class PackedFeatures:
 _POOL = None
 
 
+def _pack_kind(sources):
+    '''LMB_PACK_F64/F32 if every source is a C-contiguous array of that
+    type, else None.'''
+    if not sources:
+        return None
+    dt = sources[0].dtype
+    kinds = {np.dtype(np.float64): _native.LMB_PACK_F64,
+             np.dtype(np.float32): _native.LMB_PACK_F32}
+    if dt not in kinds:
+        return None
+    if any(s.dtype != dt or not s.flags.c_contiguous for s in sources):
+        return None
+    return kinds[dt]
+
+
+def _pack_threads():
+    import os
+    # leave a core for the thread that drives a streamed fit (its waits on
+    # the GPU spin)
+    return max(1, min(32, (os.cpu_count() or 1) - 1))
+
+
+
+
 def _pool():
     '''Thread pool for packing (numpy releases the GIL while copying).'''
     global _POOL
     if _POOL is None:
         import os
         from concurrent.futures import ThreadPoolExecutor
-        n = min(16, os.cpu_count() or 1)
+        # leave a core each for the caller and the thread that drives a
+        # streamed fit (its waits on the GPU spin)
+        n = min(16, (os.cpu_count() or 1) - 2)
         _POOL = ThreadPoolExecutor(max_workers=n) if n > 1 else False
     return _POOL or None
 
@@ -171,11 +225,11 @@ class _Staging:
 _staging = _Staging()
 
 
-def upload(packed, starts, device=None):
-    '''Device copies of a packed batch: (features, data, coords, params).
-    The crops are converted to float32 directly into the pinned staging
-    buffer and everything crosses to the device in one copy.'''
-    dev = get_device(device)
+def stage(packed, starts, staging=None):
+    '''Write a packed batch into a pinned staging buffer: the crops as
+    float32, the feature records, the starts and any explicit coordinates,
+    each at a 256-byte aligned offset.  Returns (pinned uint8 tensor, offsets,
+    sizes).'''
     starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
     pieces = [packed.features.view(np.uint8), None, starts]
     if packed.coords is not None:
@@ -185,31 +239,52 @@ def upload(packed, starts, device=None):
         nbytes.append(packed.coords.nbytes)
     sizes = [(n + 255) // 256 * 256 for n in nbytes]
     total = sum(sizes)
-    stage = _staging.take(total)
-    host = stage.numpy()
-    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    buf = (staging or _staging).take(total)
+    host = buf.numpy()
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(int)
     for k, a in enumerate(pieces):
         if a is None:
             packed.write_data(host[offs[k]:offs[k] + nbytes[k]].view(np.float32))
         else:
             host[offs[k]:offs[k] + nbytes[k]] = a.view(np.uint8).reshape(-1)
+    return buf, offs, nbytes
+
+
+def to_device(buf, offs, nbytes, dev):
+    '''One asynchronous copy of a staged batch on the current stream;
+    device views (features, data, coords or None, params).  The pinned
+    buffer must not be rewritten before the copy has completed.'''
+    total = int(offs[-1] + (nbytes[-1] + 255) // 256 * 256)
     dbuf = torch.empty(max(total, 1), dtype=torch.uint8, device=dev)
-    dbuf[:total].copy_(stage[:total], non_blocking=True)
+    dbuf[:total].copy_(buf[:total], non_blocking=True)
     dtypes = [torch.uint8, torch.float32, torch.float64, torch.float32]
     out = [dbuf[offs[k]:offs[k] + nbytes[k]].view(dtypes[k])
-           for k in range(len(pieces))]
+           for k in range(len(nbytes))]
+    d_coords = out[3] if len(nbytes) > 3 else None
+    return out[0], out[1], d_coords, out[2]
+
+
+def upload(packed, starts, device=None):
+    '''Device copies of a packed batch: (features, data, coords, params).
+    The crops are converted to float32 directly into the pinned staging
+    buffer and everything crosses to the device in one copy.'''
+    dev = get_device(device)
+    buf, offs, nbytes = stage(packed, starts)
+    out = to_device(buf, offs, nbytes, dev)
     # the staging buffer is reused by the next call: wait for this copy
     torch.cuda.current_stream(dev).synchronize()
-    d_coords = out[3] if packed.coords is not None else None
-    return out[0], out[1], d_coords, out[2]
+    return out
 
 
 def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
                instrument, variables, settings=None, nmax_cap=None,
-               starts_host=None, stats=False, tile_config=0, layers=None):
+               starts_host=None, stats=False, tile_config=0, layers=None,
+               ready=None, wait_seconds=60.):
     '''Run lmb_fit_batch on device-resident inputs.  d_params is updated in
     place with the fitted values; returns (results tensor (B*80 uint8),
-    FitStats or None).'''
+    FitStats or None).  With ``ready`` (a device int32 tensor) the fit is
+    streamed (lmb_fit_batch_streamed): features are admitted as the caller
+    advances it.'''
     dev = d_data.device
     lib = _native.load()
     settings = dict(DEFAULT_SETTINGS if settings is None else settings)
@@ -234,6 +309,18 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
     st.max_iterations = st.max_nfev
     st.tile_config = int(tile_config)
     fs = _native.FitStats() if stats else None
+    if ready is not None:
+        if layers is None:
+            L, d_frac, d_ind = 1, None, None
+        else:
+            L, d_frac, d_ind = _layer_arrays(layers, nfeatures, dev)
+        _native.check(lib.lmb_fit_batch_streamed(
+            ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
+            ptr(d_params), L, ptr(d_frac), ptr(d_ind), n_m, lam,
+            float(instrument.magnification), float(instrument.noise),
+            nmax_cap, st, ptr(ready), float(wait_seconds), ptr(d_res),
+            ptr(ws), nbytes, fs, stream_handle(dev)), 'lmb_fit_batch_streamed')
+        return d_res, fs
     if layers is None:
         _native.check(lib.lmb_fit_batch(
             ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
@@ -241,13 +328,7 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
             float(instrument.noise), nmax_cap, st, ptr(d_res), ptr(ws),
             nbytes, fs, stream_handle(dev)), 'lmb_fit_batch')
         return d_res, fs
-    L, frac, idx = layers
-    d_frac = torch.from_numpy(np.ascontiguousarray(frac, dtype=np.float64)
-                              ).to(dev)
-    ind = np.zeros((nfeatures, L - 1, 2))
-    ind[..., 0] = np.real(idx)
-    ind[..., 1] = np.imag(idx)
-    d_ind = torch.from_numpy(ind).to(dev)
+    L, d_frac, d_ind = _layer_arrays(layers, nfeatures, dev)
     _native.check(lib.lmb_fit_batch_layered(
         ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
         ptr(d_params), L, ptr(d_frac), ptr(d_ind), n_m, lam,
@@ -255,6 +336,18 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
         st, ptr(d_res), ptr(ws), nbytes, fs, stream_handle(dev)),
         'lmb_fit_batch_layered')
     return d_res, fs
+
+
+def _layer_arrays(layers, nfeatures, dev):
+    '''(nlayers, device fractions, device inner indices (re, im)).'''
+    L, frac, idx = layers
+    d_frac = torch.from_numpy(np.ascontiguousarray(frac, dtype=np.float64)
+                              ).to(dev)
+    ind = np.zeros((nfeatures, L - 1, 2))
+    ind[..., 0] = np.real(idx)
+    ind[..., 1] = np.imag(idx)
+    d_ind = torch.from_numpy(ind).to(dev)
+    return L, d_frac, d_ind
 
 
 def fit_packed(packed, starts, instrument, variables, settings=None,
@@ -285,3 +378,162 @@ def fit_packed(packed, starts, instrument, variables, settings=None,
     res = d_res[:B * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
         _native.RESULT_DTYPE).copy()
     return (params, res, fs) if stats else (params, res)
+
+
+_streams = {}
+
+
+def _fit_streams(dev):
+    '''(fit stream, copy stream) of a device, created once.'''
+    if dev not in _streams:
+        _streams[dev] = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+    return _streams[dev]
+
+
+_flags = None
+_WORKER = None
+
+
+def _worker():
+    global _WORKER
+    if _WORKER is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _WORKER = ThreadPoolExecutor(max_workers=1)
+    return _WORKER
+
+
+def default_chunks(npix):
+    '''Portions in which a batch's pixel data is streamed to the device:
+    one below ~2 Mpx (the host work is short), else up to 8 of at least
+    ~1 Mpx each.'''
+    total = int(np.sum(npix))
+    if len(npix) < 8 or total < (2 << 20):
+        return 1
+    return int(min(8, len(npix) // 4, total // (1 << 20)))
+
+
+def split_by_pixels(npix, chunks):
+    '''Contiguous index ranges with about equal pixel totals.'''
+    cum = np.cumsum(npix)
+    edges = [0]
+    for c in range(1, chunks):
+        edges.append(int(np.searchsorted(cum, cum[-1] * c / chunks)) + 1)
+    edges.append(len(npix))
+    edges = sorted(set(min(max(e, 0), len(npix)) for e in edges))
+    return [(a, b) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+
+
+def fit_items(items, starts, instrument, variables, settings=None,
+              device=None, layers=None, autotune=False, chunks=None,
+              wait_seconds=60.):
+    '''Fit crops given as (data, grid, coords) items.  Large batches are
+    streamed: the feature records and starts go to the device first and the
+    fit starts (lmb_fit_batch_streamed, driven by a worker thread); the host
+    then converts the pixel data portion by portion into pinned memory and
+    copies each on a second stream, advancing the device's admission count
+    after each copy, so that conversion and transfer overlap the fitting of
+    the features already admitted.  Returns (params (B, 6), results record
+    array, npix (B,)).'''
+    global _flags
+    starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
+    B = starts.shape[0]
+    if len(items) != B:
+        raise ValueError('one start per feature')
+    packed = PackedFeatures(items)
+    npix = packed.features['npix'].astype(np.int64)
+    if chunks is None:
+        chunks = default_chunks(npix)
+    if B == 0 or chunks <= 1:
+        params, res = fit_packed(packed, starts, instrument, variables,
+                                 settings, device, layers=layers,
+                                 autotune=autotune)
+        return params, res, npix
+    dev = get_device(device)
+    nmax_cap = fit_capacity(starts, float(instrument.n_m),
+                            float(instrument.wavelength), layers)
+    tile_config = 0
+    if autotune:
+        from .. import autotune as _tuner
+        tile_config = _tuner.tune(packed, starts, instrument, variables,
+                                  nmax_cap, layers, dev)
+    ranges = split_by_pixels(npix, chunks)
+    # pinned layout: [features | starts | coords | data], 256-byte aligned
+    pieces = [packed.features.view(np.uint8), starts.view(np.uint8)]
+    if packed.coords is not None:
+        pieces.append(packed.coords.view(np.uint8))
+    sizes = [(p.nbytes + 255) // 256 * 256 for p in pieces]
+    head = sum(sizes)
+    total = head + packed.total * 4
+    buf = _staging.take(total)
+    host = buf.numpy()
+    off = 0
+    for p, sz in zip(pieces, sizes):
+        host[off:off + p.nbytes] = p.reshape(-1)
+        off += sz
+    hdata = host[head:head + packed.total * 4].view(np.float32)
+    if _flags is None or _flags.numel() < len(ranges) + 1:
+        _flags = torch.zeros(max(len(ranges) + 1, 64), dtype=torch.int32,
+                             pin_memory=True)
+    s_fit, s_copy = _fit_streams(dev)
+    s_fit.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s_fit):
+        dbuf = torch.empty(total, dtype=torch.uint8, device=dev)
+        dbuf[:head].copy_(buf[:head], non_blocking=True)
+        d_ready = torch.zeros(1, dtype=torch.int32, device=dev)
+    s_copy.wait_stream(s_fit)
+    dbuf.record_stream(s_copy)
+    d_ready.record_stream(s_copy)
+    d_feat = dbuf[:pieces[0].nbytes]
+    d_params = dbuf[sizes[0]:sizes[0] + pieces[1].nbytes].view(torch.float64)
+    d_coords = None
+    if packed.coords is not None:
+        o = sizes[0] + sizes[1]
+        d_coords = dbuf[o:o + pieces[2].nbytes].view(torch.float32)
+    d_data = dbuf[head:total].view(torch.float32)
+    future = _worker().submit(_fit_streamed, s_fit, d_feat, d_data, d_coords,
+                              d_params, B, packed.total, instrument,
+                              variables, settings, nmax_cap, starts,
+                              tile_config, layers, d_ready, wait_seconds)
+    offs = packed.features['data_offset']
+    try:
+        for k, (a, b) in enumerate(ranges):
+            packed.write_range(hdata, a, b)
+            lo = int(offs[a]) * 4
+            hi = int(offs[b - 1] + npix[b - 1]) * 4
+            with torch.cuda.stream(s_copy):
+                dbuf[head + lo:head + hi].copy_(buf[head + lo:head + hi],
+                                                non_blocking=True)
+                _flags[k] = b
+                d_ready.copy_(_flags[k:k + 1], non_blocking=True)
+    except BaseException:
+        _flags[len(ranges)] = -1
+        with torch.cuda.stream(s_copy):
+            d_ready.copy_(_flags[len(ranges):len(ranges) + 1],
+                          non_blocking=True)
+        try:
+            future.result()
+        finally:
+            s_copy.synchronize()
+        raise
+    try:
+        params, res = future.result()
+    finally:
+        # the pinned buffers are reused by the next call
+        s_copy.synchronize()
+    torch.cuda.current_stream(dev).wait_stream(s_fit)
+    return params, res, npix
+
+
+def _fit_streamed(stream, d_feat, d_data, d_coords, d_params, n, total,
+                  instrument, variables, settings, nmax_cap, starts,
+                  tile_config, layers, d_ready, wait_seconds):
+    with torch.cuda.stream(stream):
+        d_res, _ = fit_device(d_feat, d_data, d_coords, d_params, n, total,
+                              instrument, variables, settings, nmax_cap,
+                              starts, False, tile_config=tile_config,
+                              layers=layers, ready=d_ready,
+                              wait_seconds=wait_seconds)
+        params = d_params.view(torch.float64).reshape(n, 6).cpu().numpy()
+        res = d_res[:n * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
+            _native.RESULT_DTYPE).copy()
+    return params, res

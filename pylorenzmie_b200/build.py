@@ -20,7 +20,7 @@ CSRC = PKG / 'csrc'
 INCLUDE = ROOT / 'include'
 LIBDIR = PKG / '_lib'
 LIBRARY = LIBDIR / 'liblmb200.so'
-SOURCES = ['lmb200.cu']
+SOURCES = ['lmb200.cu', 'lmb_host.cpp']
 GENCODE = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

@@ -4,7 +4,9 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "lmb200.h"
@@ -162,6 +164,7 @@ const char* lmb_status_string(int status) {
     case LMB_ERR_NMAX: return "sphere needs more partial-wave orders than nmax_cap";
     case LMB_ERR_WORKSPACE: return "workspace too small";
     case LMB_ERR_UNSUPPORTED: return "unsupported flag combination";
+    case LMB_ERR_TIMEOUT: return "streamed fit: no data arrived in time";
     default: return "unknown status";
   }
 }
@@ -301,7 +304,8 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
                    lmb_fit_result* results, void* workspace,
                    size_t workspace_bytes, lmb_fit_stats* stats, void* stream,
                    int nlayers, const double* layer_frac,
-                   const double* layer_index) {
+                   const double* layer_index, const int* ready = nullptr,
+                   double wait_seconds = 0.) {
   if (nlayers < 1 || nlayers > LMB_MAX_LAYERS) return LMB_ERR_ARG;
   if (nlayers > 1 && nfeatures > 0 && (!layer_frac || !layer_index))
     return LMB_ERR_ARG;
@@ -335,6 +339,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   c.counters = reinterpret_cast<int*>(ws + L.counters);
   c.work = reinterpret_cast<unsigned long long*>(ws + L.counters + 8 * sizeof(int));
   c.total_pixels = total_pixels;
+  c.ready = ready;
   c.nlayers = nlayers;
   c.layer_frac = layer_frac;
   c.layer_index = layer_index;
@@ -396,34 +401,61 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   };
   int launches = 0, evals = 0, iterations = 0;
   int status = LMB_OK;
+  // counters[1] (features with an evaluation pending) and counters[4]
+  // (features still waiting for their data) after each step
+  int cnt[5] = {0, 0, 0, 0, 0};
+  auto read_counts = [&]() -> bool {
+    return cudaMemcpyAsync(cnt, c.counters, sizeof(cnt), cudaMemcpyDeviceToHost,
+                           st) == cudaSuccess &&
+           cudaStreamSynchronize(st) == cudaSuccess;
+  };
   do {
     if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
     k_fit_setup<<<1, 1024, 0, st>>>(c);
     k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
     launches += 2;
-    if (cudaGetLastError() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-    for (int it = 0; it < c.max_iterations; ++it) {
-      if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) {
-        status = LMB_ERR_CUDA;
-        break;
+    if (cudaGetLastError() != cudaSuccess || !read_counts()) {
+      status = LMB_ERR_CUDA;
+      break;
+    }
+    // Every evaluation advances each running feature's nfev, which the
+    // step kernel caps at max_iterations, so the rounds after the last
+    // admission are bounded by max_iterations; waiting for data is bounded
+    // by wait_seconds without progress.
+    int since_admission = 0, pending = cnt[4];
+    auto wait_start = std::chrono::steady_clock::now();
+    while (cnt[1] > 0 || cnt[4] > 0) {
+      if (cnt[1] > 0) {
+        if (++since_admission > c.max_iterations + 1) break;
+        if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) {
+          status = LMB_ERR_CUDA;
+          break;
+        }
+        if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+        eval<<<egrid, shape.tpb, eval_smem, st>>>(c);
+        if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+        launches += 1;
+        ++evals;
+      } else {
+        const double waited = std::chrono::duration<double>(
+            std::chrono::steady_clock::now() - wait_start).count();
+        if (waited > wait_seconds) { status = LMB_ERR_TIMEOUT; break; }
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
       }
-      if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-      eval<<<egrid, shape.tpb, eval_smem, st>>>(c);
-      if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
       cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
+      cudaMemsetAsync(c.counters + 4, 0, sizeof(int), st);
       k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
-      launches += 2;
-      ++evals;
+      launches += 1;
       ++iterations;
-      if (cudaGetLastError() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-      int running = 0;
-      if (cudaMemcpyAsync(&running, c.counters + 1, sizeof(int),
-                          cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-          cudaStreamSynchronize(st) != cudaSuccess) {
+      if (cudaGetLastError() != cudaSuccess || !read_counts()) {
         status = LMB_ERR_CUDA;
         break;
       }
-      if (running == 0) break;
+      if (cnt[4] < pending) {  // new features admitted
+        pending = cnt[4];
+        since_admission = 0;
+        wait_start = std::chrono::steady_clock::now();
+      }
     }
     if (status != LMB_OK) break;
     k_fit_finalize<<<(nfeatures + 127) / 128, 128, 0, st>>>(c);
@@ -482,6 +514,24 @@ int lmb_fit_batch(const lmb_feature* features, int nfeatures,
                         stream, 1, nullptr, nullptr);
 }
 
+int lmb_fit_batch_streamed(const lmb_feature* features, int nfeatures,
+                           long long total_pixels, const float* data,
+                           const float* coords, lmb_sphere* params,
+                           int nlayers, const double* layer_fractions,
+                           const double* layer_indices, double n_m,
+                           double wavelength, double magnification,
+                           double noise, int nmax_cap,
+                           const lmb_fit_settings* settings, const int* ready,
+                           double wait_seconds, lmb_fit_result* results,
+                           void* workspace, size_t workspace_bytes,
+                           lmb_fit_stats* stats, void* stream) {
+  if (!ready || !(wait_seconds >= 0.)) return LMB_ERR_ARG;
+  return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
+                        n_m, wavelength, magnification, noise, nmax_cap,
+                        settings, results, workspace, workspace_bytes, stats,
+                        stream, nlayers, layer_fractions, layer_indices, ready,
+                        wait_seconds);
+}
 int lmb_fit_batch_layered(const lmb_feature* features, int nfeatures,
                           long long total_pixels, const float* data,
                           const float* coords, lmb_sphere* params, int nlayers,

@@ -1,0 +1,172 @@
+// Host-side packing of hologram crops for the batched fit: conversion of
+// many crops to float32 into one (pinned) staging buffer, on a persistent
+// pool of native threads so that the caller's interpreter lock is not
+// involved and small portions of a streamed batch convert at full speed.
+#include <stddef.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "lmb200.h"
+
+namespace {
+
+template <typename T>
+__attribute__((target("avx2"))) void convert_avx2(const T* s, float* d,
+                                                  size_t n) {
+  for (size_t i = 0; i < n; ++i) d[i] = static_cast<float>(s[i]);
+}
+
+template <typename T>
+void convert_base(const T* s, float* d, size_t n) {
+  for (size_t i = 0; i < n; ++i) d[i] = static_cast<float>(s[i]);
+}
+
+bool have_avx2() {
+  static const bool v = __builtin_cpu_supports("avx2");
+  return v;
+}
+
+struct PackJob {
+  const void* const* sources;
+  const long long* first;  // [n + 1] prefix sums of the counts
+  int nsources;
+  int src_type;
+  float* dst;
+  long long total;
+  int parts;
+};
+
+// Convert elements [a, b) of the concatenated sources.
+void run_part(const PackJob& j, long long a, long long b) {
+  if (a >= b) return;
+  int i = int(std::upper_bound(j.first, j.first + j.nsources + 1, a) - j.first) - 1;
+  const bool avx2 = have_avx2();
+  while (a < b && i < j.nsources) {
+    const long long lo = a - j.first[i];
+    const long long hi = std::min(b, j.first[i + 1]) - j.first[i];
+    if (hi > lo) {
+      float* d = j.dst + j.first[i] + lo;
+      const size_t n = size_t(hi - lo);
+      if (j.src_type == LMB_PACK_F64) {
+        const double* s = static_cast<const double*>(j.sources[i]) + lo;
+        avx2 ? convert_avx2(s, d, n) : convert_base(s, d, n);
+      } else {
+        const float* s = static_cast<const float*>(j.sources[i]) + lo;
+        avx2 ? convert_avx2(s, d, n) : convert_base(s, d, n);
+      }
+      a = j.first[i] + hi;
+    }
+    ++i;
+  }
+}
+
+// Persistent workers; part 0 of every job runs on the calling thread.
+class Pool {
+ public:
+  void run(const PackJob& job) {
+    std::unique_lock<std::mutex> call(call_mutex_);  // one job at a time
+    grow(job.parts - 1);
+    {
+      std::lock_guard<std::mutex> g(m_);
+      job_ = &job;
+      pending_ = job.parts - 1;
+      ++generation_;
+    }
+    cv_work_.notify_all();
+    do_part(job, 0);
+    std::unique_lock<std::mutex> g(m_);
+    cv_done_.wait(g, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_work_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+
+ private:
+  static void do_part(const PackJob& j, int p) {
+    const long long a = j.total * p / j.parts;
+    const long long b = j.total * (p + 1) / j.parts;
+    run_part(j, a, b);
+  }
+
+  // Called by run() before it publishes a job: a new worker starts from
+  // the current generation, so it takes part in the job about to come.
+  void grow(int workers) {
+    while (int(threads_.size()) < workers) {
+      const int id = int(threads_.size()) + 1;  // its part index
+      const uint64_t g0 = generation_;
+      threads_.emplace_back([this, id, g0] { loop(id, g0); });
+    }
+  }
+
+  void loop(int id, uint64_t seen) {
+    for (;;) {
+      const PackJob* job;
+      {
+        std::unique_lock<std::mutex> g(m_);
+        cv_work_.wait(g, [&] { return stop_ || generation_ != seen; });
+        if (stop_) return;
+        seen = generation_;
+        job = job_;
+        if (!job || id >= job->parts) continue;
+      }
+      do_part(*job, id);
+      {
+        std::lock_guard<std::mutex> g(m_);
+        --pending_;
+      }
+      cv_done_.notify_one();
+    }
+  }
+
+  std::mutex call_mutex_, m_;
+  std::condition_variable cv_work_, cv_done_;
+  std::vector<std::thread> threads_;
+  const PackJob* job_ = nullptr;
+  int pending_ = 0;
+  uint64_t generation_ = 0;
+  bool stop_ = false;
+};
+
+Pool& pool() {
+  static Pool* p = new Pool();  // never destroyed: workers live with the process
+  return *p;
+}
+
+}  // namespace
+
+extern "C" int lmb_pack_crops(const void* const* sources,
+                              const long long* counts, int nsources,
+                              int src_type, float* dst, int nthreads) {
+  if (nsources < 0 || nthreads < 1 || nthreads > 256) return LMB_ERR_ARG;
+  if (src_type != LMB_PACK_F64 && src_type != LMB_PACK_F32) return LMB_ERR_ARG;
+  if (nsources == 0) return LMB_OK;
+  if (!sources || !counts || !dst) return LMB_ERR_ARG;
+  std::vector<long long> first(size_t(nsources) + 1, 0);
+  for (int i = 0; i < nsources; ++i) {
+    if (counts[i] < 0 || (counts[i] > 0 && !sources[i])) return LMB_ERR_ARG;
+    first[i + 1] = first[i] + counts[i];
+  }
+  PackJob job{sources, first.data(), nsources, src_type, dst, first.back(), 1};
+  // at least ~256 k elements per part: below that, waking threads costs
+  // more than it saves
+  const long long want = std::max(1LL, job.total / (256LL << 10));
+  job.parts = int(std::min<long long>(nthreads, want));
+  if (job.parts == 1) {
+    run_part(job, 0, job.total);
+    return LMB_OK;
+  }
+  pool().run(job);
+  return LMB_OK;
+}

@@ -442,7 +442,8 @@ struct FitCtx {
   int* tile_begin;     // [nf+1]
   int2* tiles;         // [max_tiles]
   double* partial;     // [max_tiles][FIT_NSUM]
-  int* counters;       // [0] tile queue, [1] running, [2] ntiles, [3] overflow
+  int* counters;       // [0] tile queue, [1] running, [2] ntiles, [3] overflow,
+                       // [4] waiting for data
   unsigned long long* work;  // [0] pixels, [1] pixel-orders evaluated
   long long total_pixels;
   int nf, nmax_cap, max_tiles, tile_pixels;
@@ -453,6 +454,10 @@ struct FitCtx {
   LMSettings set;
   int variables, flags, max_iterations;
   int pair_records;    // the evaluation kernel reads stage_pair records
+  // Streamed admission: features [0, *ready) have their data on the
+  // device; the rest wait in LM_PHASE_INIT (counted in counters[4]).  A
+  // negative value withdraws the batch.  Null: every feature is ready.
+  const int* ready;
 };
 
 __device__ inline bool feature_valid(const lmb_feature& ft, long long total) {
@@ -494,6 +499,7 @@ __global__ void k_fit_setup(FitCtx c) {
     c.counters[3] = carry > c.max_tiles ? 1 : 0;
     c.counters[0] = 0;
     c.counters[1] = 0;
+    c.counters[4] = 0;
     c.work[0] = 0ull;
     c.work[1] = 0ull;
   }
@@ -855,6 +861,24 @@ k_fit_step(FitCtx c) {
   LMState* gs = c.state + f;
   const int phase = gs->phase;
   if (phase == LM_PHASE_DONE) return;
+  if (phase == LM_PHASE_INIT && c.ready) {
+    // one read for the whole warp: the flag may change while we look
+    int r = 0;
+    if (lane == 0) r = *reinterpret_cast<const volatile int*>(c.ready);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r < 0) {  // withdrawn by the producer: this feature is not fitted
+      if (lane == 0) {
+        gs->phase = LM_PHASE_DONE;
+        gs->info = -4;
+        c.ev[f].active = 0;
+      }
+      return;
+    }
+    if (f >= r) {
+      if (lane == 0) atomicAdd(c.counters + 4, 1);
+      return;
+    }
+  }
   const int nmaxp = c.nmax_cap + 1;
   if (lane == 0) {
     s_need = 0;

@@ -189,3 +189,59 @@ def test_every_launch_shape_gives_the_same_fit():
             assert np.all(np.abs(p[:, j] - ref[:, j]) <= bound), \
                 (idx, tpb, ppt, minb, k, p[:, j] - ref[:, j], bound)
         assert np.all(np.abs(r['redchi'] / rref['redchi'] - 1) < 1e-3), idx
+
+
+def test_streamed_batch_is_bit_identical():
+    '''optimize_batch streamed in portions (the fit starts on the first
+    features while the rest are converted and copied) gives exactly the
+    per-feature results of the one-shot call: a feature's sums do not
+    depend on the other features in its batch or on when it was admitted.'''
+    from pylorenzmie_b200 import Hologram, workloads
+    truth, start = workloads.batch_201(24, seed=9)
+    truth[:, :2] -= 60.
+    start[:, :2] -= 60.
+    data = workloads.render(truth, (81, 81), seed=9).cpu().numpy()
+    holos = [Hologram(d.astype(float)) for d in data]
+    opt = make_optimizer(start[0], (8, 8))
+    d1 = opt.optimize_batch(holos, starts=start, autotune=False, chunks=1)
+    for chunks in (3, 24):
+        d3 = opt.optimize_batch(holos, starts=start, autotune=False,
+                                chunks=chunks)
+        assert len(d3) == 24 and list(d3.columns) == list(d1.columns)
+        for col in d1.columns:
+            np.testing.assert_array_equal(d1[col].to_numpy(),
+                                          d3[col].to_numpy())
+
+
+def test_streamed_fit_withdraw_and_timeout():
+    '''lmb_fit_batch_streamed: features admitted before a withdrawal are
+    fitted, the rest end with status -4; with nothing admitted the call
+    gives up after wait_seconds with LMB_ERR_TIMEOUT (host-side limit, no
+    kernel waits).'''
+    import torch
+    from pylorenzmie_b200 import Instrument, _native
+    from pylorenzmie_b200.analysis import _fit
+    truth = np.array([[20.3, 19.6, 150., 0.75, 1.45, 0.]] * 6)
+    items = [(_render(40 + i, (41, 41), truth[i]), (0., 0., 41, 41), None)
+             for i in range(6)]
+    starts = truth.copy()
+    starts[:, 2] += 8.
+    packed = _fit.PackedFeatures(items)
+    inst = Instrument()
+    variables = ['x_p', 'y_p', 'z_p', 'a_p', 'n_p']
+    d_feat, d_data, d_coords, d_params = _fit.upload(packed, starts)
+    ready = torch.tensor([-1], dtype=torch.int32, device=d_data.device)
+    # withdrawn before anything was admitted
+    d_res, _ = _fit.fit_device(d_feat, d_data, d_coords, d_params, 6,
+                               packed.total, inst, variables, None, None,
+                               starts, ready=ready, wait_seconds=5.)
+    r = d_res.cpu().numpy().view(_native.RESULT_DTYPE)
+    assert list(r['status']) == [-4] * 6 and not r['success'].any()
+    # three admitted, then the producer stops without withdrawing
+    d_feat, d_data, d_coords, d_params = _fit.upload(packed, starts)
+    ready.fill_(3)
+    with pytest.raises(_native.LMBError) as e:
+        _fit.fit_device(d_feat, d_data, d_coords, d_params, 6, packed.total,
+                        inst, variables, None, None, starts, ready=ready,
+                        wait_seconds=0.5)
+    assert e.value.status == _native.LMB_ERR_TIMEOUT

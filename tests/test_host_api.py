@@ -231,3 +231,42 @@ def test_autotune_keys_and_cache(tmp_path, monkeypatch):
     shapes = autotune.shapes()
     assert len(shapes) >= 2 and shapes[0][0] == 0
     assert all(t % 32 == 0 and 512 % p == 0 for _, t, p, _ in shapes)
+
+
+def test_pipeline_chunking():
+    from pylorenzmie_b200.analysis import _fit
+    npix = np.array([201 * 201] * 256)
+    assert _fit.default_chunks(npix) == 8
+    assert _fit.default_chunks(npix[:4]) == 1
+    assert _fit.default_chunks(np.array([2500] * 64)) == 1
+    rng = np.random.default_rng(0)
+    for n, c in [(10, 3), (256, 4), (5, 4), (1, 2)]:
+        px = rng.integers(100, 90000, n)
+        r = _fit.split_by_pixels(px, c)
+        assert r[0][0] == 0 and r[-1][1] == n
+        assert all(a < b for a, b in r)
+        assert all(r[i][1] == r[i + 1][0] for i in range(len(r) - 1))
+        assert len(r) <= c
+    r = _fit.split_by_pixels(np.full(100, 7), 4)
+    assert [b - a for a, b in r] == [25, 25, 25, 25]
+
+
+def test_packed_write_range_any_cut():
+    '''write_range converts exactly the crops asked for, whatever the crop
+    sizes and the thread cuts (cuts fall inside crops).'''
+    from pylorenzmie_b200.analysis import _fit
+    rng = np.random.default_rng(3)
+    items = []
+    for i in range(37):
+        n = int(rng.integers(1, 90000))
+        items.append((rng.random(n), None, np.zeros((2, n))))
+    pk = _fit.PackedFeatures(items)
+    ref = np.concatenate([it[0] for it in items]).astype(np.float32)
+    out = np.full(pk.total, -1., np.float32)
+    pk.write_range(out, 5, 23)
+    a = pk.features['data_offset'][5]
+    b = pk.features['data_offset'][22] + pk.features['npix'][22]
+    np.testing.assert_array_equal(out[a:b], ref[a:b])
+    assert np.all(out[:a] == -1.) and np.all(out[b:] == -1.)
+    np.testing.assert_array_equal(pk.write_data(np.empty(pk.total, np.float32)),
+                                  ref)

@@ -92,3 +92,37 @@ def test_workspace_sizes(lib):
     assert lib.lmb_fit_workspace_bytes(0, 0, 40) == 0
     assert lib.lmb_vjp_workspace_bytes(1000, 2) == 8 * 2 * 6 * 8
     assert lib.lmb_vjp_workspace_bytes(0, 2) == 0
+
+
+
+def test_pack_crops_host_conversion():
+    '''lmb_pack_crops (host code, no GPU): many crops of float64 or float32,
+    any lengths, on several native threads: numpy's float32 rounding, in
+    order, nothing written outside the destination run.'''
+    lib = _native.load()
+    rng = np.random.default_rng(5)
+    for dtype, kind in ((np.float64, _native.LMB_PACK_F64),
+                        (np.float32, _native.LMB_PACK_F32)):
+        for sizes in ([0, 1, 7], [300000, 5, 0, 700001, 3],
+                      list(rng.integers(0, 40000, 200))):
+            srcs = [rng.normal(0., 3., n).astype(dtype) for n in sizes]
+            ptrs = np.array([s.ctypes.data for s in srcs], dtype=np.uintp)
+            counts = np.array(sizes, dtype=np.int64)
+            total = int(counts.sum())
+            out = np.full(total + 5, -7., np.float32)
+            for threads in (1, 6):
+                out[:] = -7.
+                assert lib.lmb_pack_crops(ptrs.ctypes.data,
+                                          counts.ctypes.data, len(srcs), kind,
+                                          out[2:].ctypes.data, threads) == 0
+                ref = np.concatenate(srcs).astype(np.float32) if srcs else []
+                np.testing.assert_array_equal(out[2:2 + total], ref)
+                assert np.all(out[:2] == -7.) and np.all(out[2 + total:] == -7.)
+    ptrs = np.zeros(1, dtype=np.uintp)
+    counts = np.array([4], dtype=np.int64)
+    out = np.zeros(4, np.float32)
+    assert lib.lmb_pack_crops(ptrs.ctypes.data, counts.ctypes.data, 1,
+                              _native.LMB_PACK_F64, out.ctypes.data, 2) == \
+        _native.LMB_ERR_ARG          # null source with a positive count
+    assert lib.lmb_pack_crops(ptrs.ctypes.data, counts.ctypes.data, 1, 7,
+                              out.ctypes.data, 2) == _native.LMB_ERR_ARG
