@@ -245,3 +245,20 @@ def test_streamed_fit_withdraw_and_timeout():
                         inst, variables, None, None, starts, ready=ready,
                         wait_seconds=0.5)
     assert e.value.status == _native.LMB_ERR_TIMEOUT
+
+
+def test_distributed_fit_single_rank_is_optimize_batch():
+    '''optimize_batch_distributed without a process group (one rank) is
+    optimize_batch, rows in input order.'''
+    from pylorenzmie_b200 import Hologram, workloads
+    from pylorenzmie_b200.distributed import optimize_batch_distributed
+    truth, start = workloads.batch_201(6, seed=21)
+    truth[:, :2] -= 70.
+    start[:, :2] -= 70.
+    data = workloads.render(truth, (61, 61), seed=21).cpu().numpy()
+    holos = [Hologram(d.astype(float)) for d in data]
+    opt = make_optimizer(start[0], (8, 8))
+    d0 = opt.optimize_batch(holos, starts=start, autotune=False)
+    d1 = optimize_batch_distributed(opt, holos, starts=start, autotune=False)
+    for col in d0.columns:
+        np.testing.assert_array_equal(d0[col].to_numpy(), d1[col].to_numpy())
