@@ -115,6 +115,33 @@ int lmb_hologram(const double *coords, long long npts,
                  int flags, void *out, void *stream);
 
 /*
+ * chi^2 = sum over pixels of ((hologram - data) / noise)^2 for each of
+ * nitems particle lists at shared coordinates: the objective of one
+ * differential-evolution generation in one launch.  Replaces the
+ * per-candidate _DEObjective calls of DEEstimator
+ * (analysis/DEEstimator.py:32-37, driven by scipy's differential_evolution
+ * at :158-166) and of RadialEstimator (analysis/RadialEstimator.py:32-37).
+ * NaN residuals are skipped (numpy.nansum).  Inputs as lmb_hologram, plus
+ *   data       [npts] FP64 normalized intensities
+ *   chi2       [nitems] FP64 out
+ *   nonfinite  [nitems] int out, or NULL: pixels whose hologram came out
+ *              NaN or infinite.  With FP32 sums these mark candidates whose
+ *              focal plane cuts the sphere, where the partial waves outgrow
+ *              FP32's range; the caller re-evaluates them with LMB_FP64 so
+ *              that NaN pixels are skipped only where the FP64 model (the
+ *              reference's) gives NaN.
+ *   workspace  of lmb_chi2_workspace_bytes(npts, nitems) bytes
+ * FP32 field sums unless LMB_FP64; the residuals and sums are FP64.
+ */
+size_t lmb_chi2_workspace_bytes(long long npts, int nitems);
+int lmb_chi2_batch(const double *coords, long long npts, const double *data,
+                   double noise, const lmb_sphere *spheres,
+                   const int *item_start, int nitems, const double *ab,
+                   const int *nmax, int nmax_cap, double k, int flags,
+                   double *chi2, int *nonfinite, void *workspace,
+                   size_t workspace_bytes, void *stream);
+
+/*
  * Hologram and its Jacobian for nitems single-sphere items, FP32 sums,
  * Cartesian field (LMB_BOHREN honoured).  Fills the analytic-Jacobian
  * slot of the reference: jaxLorenzMie.jac / jac_params

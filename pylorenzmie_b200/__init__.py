@@ -10,4 +10,5 @@ __version__ = '0.1.0'
 from .lib import meshgrid, LMObject  # noqa: F401
 from .theory import (Particle, Sphere, LayeredSphere, Instrument,  # noqa: F401
                      LorenzMie)
-from .analysis import Hologram, Mask, Optimizer  # noqa: F401
+from .analysis import (Hologram, Mask, Optimizer, DEEstimator,  # noqa: F401
+                       RadialEstimator, Feature, Frame)

@@ -1,0 +1,118 @@
+'''Global estimate of a sphere's parameters by differential evolution, with
+each generation's population evaluated on the GPU in one launch.
+
+Same fields, defaults and behaviour as analysis/DEEstimator.py: x_p, y_p
+are pinned to the crop's coordinate means (:140-141), a fresh random
+subset of ``fraction`` of the pixels (minus ``exclude``) is drawn once per
+call (:143-146), and scipy's differential_evolution minimizes
+sum(((H - data)/noise)^2) with NaN residuals skipped (:32-37) over
+``bounds`` (:153-166).  The reference evaluates each candidate with one
+model.hologram() call, spread over worker processes; here the search runs
+scipy's same algorithm with ``vectorized=True`` and ``updating='deferred'``
+(the reference's setting), so a generation is one lmb_chi2_batch launch.
+With the same seed and an FP64 model the search follows the reference's
+trajectory; with FP32 sums the energies differ by rounding only.
+'''
+from dataclasses import dataclass, field
+
+import numpy as np
+import pandas as pd
+from scipy.optimize import differential_evolution
+
+from .BaseEstimator import BaseEstimator
+from .Mask import Mask
+from ._population import PopulationChi2, batchable
+
+DEFAULT_BOUNDS = {
+    'z_p': (10., 600.),
+    'a_p': (0.25, 10.0),
+    'n_p': (1.0, 3.0),
+}
+
+
+class _HostObjective:
+    '''One model.hologram() per candidate: for searches over variables the
+    population kernel does not cover (instrument properties, layered or
+    multi-particle models).'''
+
+    def __init__(self, model, data, variables, noise):
+        self.model, self.data = model, data
+        self.variables, self.noise = variables, noise
+
+    def __call__(self, x):
+        x = np.asarray(x, dtype=float)
+        X = x.reshape(len(self.variables), -1)
+        out = np.empty(X.shape[1])
+        for s in range(X.shape[1]):
+            self.model.properties = dict(zip(self.variables, X[:, s]))
+            with np.errstate(over='ignore', invalid='ignore'):
+                diff = (self.model.hologram() - self.data) / self.noise
+                out[s] = float(np.nansum(diff ** 2))
+        return float(out[0]) if x.ndim == 1 else out
+
+
+def run_search(model, data, coords, variables, bounds, noise, popsize, seed,
+               settings):
+    '''scipy differential_evolution over ``variables`` with the population
+    objective; returns the OptimizeResult.  The model's coordinates are
+    restored on exit.'''
+    settings = dict(settings)
+    settings.pop('workers', None)
+    settings['updating'] = 'deferred'
+    settings['vectorized'] = True
+    saved = model.coordinates
+    try:
+        if batchable(model, variables):
+            objective = PopulationChi2(model, data, coords, variables, noise)
+        else:
+            model.coordinates = coords
+            objective = _HostObjective(model, data, variables, noise)
+        with np.errstate(over='ignore', invalid='ignore'):
+            return differential_evolution(objective, bounds, popsize=popsize,
+                                          seed=seed, **settings)
+    finally:
+        model.coordinates = saved
+
+
+@dataclass
+class DEEstimator(BaseEstimator):
+    '''Estimate initial particle parameters by global search.'''
+
+    model: object
+    bounds: dict = field(default_factory=lambda: DEFAULT_BOUNDS.copy())
+    fraction: float = 0.02
+    exclude: np.ndarray | None = None
+    popsize: int = 10
+    seed: int | None = None
+    settings: dict = field(default_factory=lambda: {'tol': 0.01,
+                                                     'polish': False,
+                                                     'updating': 'deferred',
+                                                     'workers': -1})
+
+    @property
+    def properties(self):
+        return dict(fraction=self.fraction, popsize=self.popsize,
+                    bounds=self.bounds, settings=self.settings)
+
+    @properties.setter
+    def properties(self, properties):
+        for name, value in properties.items():
+            if hasattr(self, name):
+                setattr(self, name, value)
+
+    def estimate(self, hologram):
+        '''Estimate particle parameters; returns the particle's properties
+        as a pandas Series and leaves the model at the estimate.'''
+        self.model.particle.x_p = float(hologram.coordinates[0].mean())
+        self.model.particle.y_p = float(hologram.coordinates[1].mean())
+        mask = Mask(fraction=self.fraction)
+        if self.exclude is not None:
+            mask.exclude = self.exclude
+        data, coords = mask.apply(hologram)
+        variables = list(self.bounds.keys())
+        result = run_search(self.model, data, coords, variables,
+                            list(self.bounds.values()),
+                            self.model.instrument.noise, self.popsize,
+                            self.seed, self.settings)
+        self.model.properties = dict(zip(variables, result.x))
+        return pd.Series(self.model.particle.properties)

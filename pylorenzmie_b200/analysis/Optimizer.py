@@ -184,14 +184,19 @@ class Optimizer(LMObject):
             self._optimize_host()
         return self.result
 
-    def _optimize_device(self, data, grid, coords):
-        packed = _fit.PackedFeatures([(data, grid, coords)])
+    def _start(self):
+        '''(1, 6) start vector of the model's single sphere.'''
         part = self.model.particle[0] if len(self.model.particle) else None
         r = np.asarray(part.r_p, float) + np.asarray(
             getattr(part, 'r_0', (0., 0., 0.)), float)
-        start = np.array([[r[0], r[1], r[2], part.a_p, part.n_p,
-                           getattr(part, 'k_p', 0.)]])
-        params, res = _fit.fit_packed(packed, start, self.model.instrument,
+        return np.array([[r[0], r[1], r[2], part.a_p, part.n_p,
+                          getattr(part, 'k_p', 0.)]])
+
+    def _optimize_device(self, data, grid, coords):
+        packed = _fit.PackedFeatures([(data, grid, coords)])
+        part = self.model.particle[0] if len(self.model.particle) else None
+        params, res = _fit.fit_packed(packed, self._start(),
+                                      self.model.instrument,
                                       self.variables, self.settings,
                                       device=self.model.device,
                                       layers=_fit.layers_of([part]))
@@ -201,17 +206,22 @@ class Optimizer(LMObject):
                              'residuals is less than the number of variables.')
         if status == -2:
             raise ValueError('Residuals are not finite in the initial point.')
+        self._accept(params[0], res[0])
+
+    def _accept(self, fitted, res):
+        '''Take a device fit's result: the model is left at the fitted
+        values (as scipy leaves it at its last evaluation) and ``result``
+        reports them.'''
+        part = self.model.particle[0] if len(self.model.particle) else None
         idx = [PARAM_KEYS.index(v) for v in self.variables]
-        fitted = params[0]
-        # write back like scipy leaves the model at its last evaluation
         r0 = np.asarray(getattr(part, 'r_0', (0., 0., 0.)), float)
         self.model.properties = {v: float(fitted[PARAM_KEYS.index(v)] -
                                           (r0[PARAM_KEYS.index(v)] if
                                            PARAM_KEYS.index(v) < 3 else 0.))
                                  for v in self.variables}
-        self._result = _Result(fitted[idx], res['success'][0],
-                               res['redchi'][0], res['dparams'][0][idx],
-                               status, res['nfev'][0], res['cost'][0])
+        self._result = _Result(fitted[idx], res['success'], res['redchi'],
+                               res['dparams'][idx], int(res['status']),
+                               res['nfev'], res['cost'])
 
     def _optimize_host(self):
         p0 = np.array([self.model.properties[p] for p in self.variables])

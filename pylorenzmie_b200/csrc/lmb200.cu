@@ -219,6 +219,58 @@ int lmb_hologram(const double* coords, long long npts,
                       nmax_cap, k, flags, out, stream);
 }
 
+size_t lmb_chi2_workspace_bytes(long long npts, int nitems) {
+  if (npts <= 0 || nitems <= 0) return 0;
+  const size_t n = size_t((npts + 255) / 256) * size_t(nitems);
+  return align_up(n * sizeof(double), 256) + n * sizeof(int);
+}
+
+int lmb_chi2_batch(const double* coords, long long npts, const double* data,
+                   double noise, const lmb_sphere* spheres,
+                   const int* item_start, int nitems, const double* ab,
+                   const int* nmax, int nmax_cap, double k, int flags,
+                   double* chi2, int* nonfinite, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  if (nitems < 0 || npts < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
+  if (nitems == 0) return LMB_OK;
+  if (!chi2 || !(noise > 0.)) return LMB_ERR_ARG;
+  cudaStream_t st = as_stream(stream);
+  if (npts == 0) {
+    LMB_CK(cudaMemsetAsync(chi2, 0, sizeof(double) * nitems, st));
+    if (nonfinite) LMB_CK(cudaMemsetAsync(nonfinite, 0, sizeof(int) * nitems, st));
+    return LMB_OK;
+  }
+  if (!coords || !data || !spheres || !item_start || !ab || !nmax) return LMB_ERR_ARG;
+  if (nitems > 65535 || (npts + 255) / 256 > 0x7fffffffLL) return LMB_ERR_ARG;
+  if (!workspace || workspace_bytes < lmb_chi2_workspace_bytes(npts, nitems))
+    return LMB_ERR_WORKSPACE;
+  const int tpb = 256;
+  const int nb = int((npts + tpb - 1) / tpb);
+  double* partial = reinterpret_cast<double*>(workspace);
+  int* partial_bad = reinterpret_cast<int*>(
+      reinterpret_cast<char*>(workspace) +
+      align_up(size_t(nb) * size_t(nitems) * sizeof(double), 256));
+  const dim3 grid{unsigned(nb), unsigned(nitems)};
+  if (flags & LMB_FP64) {
+    const size_t smem = sizeof(Quad<double>) * 2 * (size_t(nmax_cap) + 1);
+    LMB_CK(smem_attr((const void*)k_chi2<double>, smem));
+    k_chi2<double><<<grid, tpb, smem, st>>>(
+        coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
+        nmax_cap + 1, k, flags, data, 1. / noise, partial, partial_bad);
+  } else {
+    const size_t smem = sizeof(Quad<float>) * 2 * (size_t(nmax_cap) + 1);
+    LMB_CK(smem_attr((const void*)k_chi2<float>, smem));
+    k_chi2<float><<<grid, tpb, smem, st>>>(
+        coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
+        nmax_cap + 1, k, flags, data, 1. / noise, partial, partial_bad);
+  }
+  LMB_CK(cudaGetLastError());
+  k_chi2_reduce<<<(nitems + 127) / 128, 128, 0, st>>>(partial, partial_bad, nb,
+                                                       nitems, chi2, nonfinite);
+  LMB_CK(cudaGetLastError());
+  return LMB_OK;
+}
+
 int lmb_jacobian(const double* coords, long long npts,
                  const lmb_sphere* spheres, int nitems, const double* ab,
                  const double* dab, const int* nmax, int nmax_cap, double k,

@@ -305,6 +305,96 @@ k_field(const double* __restrict__ coords, long long npts,
 }
 
 // ---------------------------------------------------------------------------
+// Population chi^2: sum over the pixels of ((H - data) / noise)^2 for each
+// of nitems particle lists (the objective of a differential-evolution
+// generation), NaN residuals skipped as numpy.nansum does.  Per (item,
+// block) partial sums in FP64; k_chi2_reduce adds them in a fixed order.
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_chi2(const double* __restrict__ coords, long long npts,
+       const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
+       const zd* __restrict__ ab, const int* __restrict__ nmax, int nmaxp, double k,
+       int flags, const double* __restrict__ data, double inv_noise,
+       double* __restrict__ partial, int* __restrict__ partial_bad) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ double red[256 / 32];
+  __shared__ int redb[256 / 32];
+  Quad<R>* coef = reinterpret_cast<Quad<R>*>(smem);
+  const int item = blockIdx.y;
+  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = pix < npts;
+  const bool cart = flags & LMB_CARTESIAN;
+  const bool bohren = flags & LMB_BOHREN;
+  double x = 0., y = 0., z = 0.;
+  if (live) {
+    x = coords[pix];
+    y = coords[npts + pix];
+    z = coords[2 * npts + pix];
+  }
+  cplx<R> e[3];
+  for (int c = 0; c < 3; ++c) e[c] = mk(R(0), R(0));
+  const int pb = item_start[item], pe = item_start[item + 1];
+  for (int p = pb; p < pe; ++p) {
+    const int nm = min(max(nmax[p], 0), nmaxp - 1);
+    __syncthreads();
+    stage_coef<R, false>(ab + size_t(p) * nmaxp * 2, (const zd*)0, nm, coef);
+    __syncthreads();
+    if (live) {
+      const lmb_sphere sp = spheres[p];
+      const Geometry<R> g = geometry<R>(k, x - sp.x_p, y - sp.y_p, z - sp.z_p, z,
+                                        sp.z_p, bohren);
+      const Sums<R> sm = order_sum<R>(g, coef, nm);
+      cplx<R> ep[3];
+      epilogue<R>(g, sm, cart, ep);
+      for (int c = 0; c < 3; ++c) e[c] = e[c] + ep[c];
+    }
+  }
+  double v = 0.;
+  int bad = 0;
+  if (live) {
+    const R h = intensity<R>(e);
+    bad = isfinite(h) ? 0 : 1;
+    const double r = (double(h) - data[pix]) * inv_noise;
+    if (r == r) v = r * r;  // nansum
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    bad += __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[warp] = v;
+    redb[warp] = bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    int b = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+      t += red[w];
+      b += redb[w];
+    }
+    partial[(size_t)item * gridDim.x + blockIdx.x] = t;
+    partial_bad[(size_t)item * gridDim.x + blockIdx.x] = b;
+  }
+}
+
+__global__ void k_chi2_reduce(const double* partial, const int* partial_bad,
+                              int nblocks, int nitems, double* chi2,
+                              int* nonfinite) {
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= nitems) return;
+  double s = 0.;
+  int b = 0;
+  for (int k = 0; k < nblocks; ++k) {
+    s += partial[(size_t)item * nblocks + k];
+    b += partial_bad[(size_t)item * nblocks + k];
+  }
+  chi2[item] = s;
+  if (nonfinite) nonfinite[item] = b;
+}
+
+// ---------------------------------------------------------------------------
 // Hologram + 6-column Jacobian, single sphere per item.
 
 __device__ inline void holo_jac_pixel(const Geometry<float>& g,

@@ -77,6 +77,11 @@ def sphere_ab_host(records, n_m, wavelength, deriv=False):
     return a, d, nmax.cpu().numpy()
 
 
+def _contiguous(*tensors):
+    '''Row-major copies where needed: the library reads plain pointers.'''
+    return tuple(None if t is None else t.contiguous() for t in tensors)
+
+
 def _flags(cartesian, bohren, fp64):
     return ((_native.LMB_CARTESIAN if cartesian else 0) |
             (_native.LMB_BOHREN if bohren else 0) |
@@ -86,6 +91,8 @@ def _flags(cartesian, bohren, fp64):
 def hologram(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
              bohren=True, fp64=False):
     '''(nitems, npts) holograms; float32, or float64 when fp64.'''
+    coords, spheres, item_start, ab, nmax = _contiguous(
+        coords, spheres, item_start, ab, nmax)
     lib = _native.load()
     dev = coords.device
     npts = coords.shape[1]
@@ -101,9 +108,39 @@ def hologram(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
     return out
 
 
+def chi2(coords, data, noise, spheres, item_start, ab, nmax, cap, k,
+         cartesian=True, bohren=True, fp64=False, nonfinite=False):
+    '''(nitems,) float64 sums of ((hologram - data) / noise)^2, NaN
+    residuals skipped (lmb_chi2_batch); with ``nonfinite`` also the
+    (nitems,) int32 counts of NaN or infinite hologram pixels.'''
+    coords, data, spheres, item_start, ab, nmax = _contiguous(
+        coords, data, spheres, item_start, ab, nmax)
+    lib = _native.load()
+    dev = coords.device
+    npts = coords.shape[1]
+    nitems = item_start.shape[0] - 1
+    out = torch.empty(max(nitems, 1), dtype=torch.float64, device=dev)
+    bad = torch.empty(max(nitems, 1), dtype=torch.int32, device=dev) \
+        if nonfinite else None
+    nbytes = lib.lmb_chi2_workspace_bytes(npts, nitems)
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    _native.check(lib.lmb_chi2_batch(ptr(coords), npts, ptr(data),
+                                     float(noise), ptr(spheres),
+                                     ptr(item_start), nitems, ptr(ab),
+                                     ptr(nmax), cap, float(k),
+                                     _flags(cartesian, bohren, fp64),
+                                     ptr(out), ptr(bad), ptr(ws), nbytes,
+                                     stream_handle(dev)), 'lmb_chi2_batch')
+    if nonfinite:
+        return out[:nitems], bad[:nitems]
+    return out[:nitems]
+
+
 def field(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
           bohren=True, fp64=False):
     '''(nitems, 3, npts) scattered fields; complex64, or complex128.'''
+    coords, spheres, item_start, ab, nmax = _contiguous(
+        coords, spheres, item_start, ab, nmax)
     lib = _native.load()
     dev = coords.device
     npts = coords.shape[1]
@@ -120,6 +157,8 @@ def field(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
 
 def jacobian(coords, spheres, ab, dab, nmax, cap, k, bohren=True):
     '''Holograms (n, npts) and Jacobians (n, 6, npts), float64, FP32 sums.'''
+    coords, spheres, ab, dab, nmax = _contiguous(
+        coords, spheres, ab, dab, nmax)
     lib = _native.load()
     dev = coords.device
     npts = coords.shape[1]
@@ -136,6 +175,8 @@ def jacobian(coords, spheres, ab, dab, nmax, cap, k, bohren=True):
 
 def hologram_vjp(coords, spheres, ab, dab, nmax, cap, k, gout, bohren=True):
     '''sum_p gout[i, p] dH_i[p]/dparam_j -> (n, 6) float64.'''
+    coords, spheres, ab, dab, nmax, gout = _contiguous(
+        coords, spheres, ab, dab, nmax, gout)
     lib = _native.load()
     dev = coords.device
     npts = coords.shape[1]

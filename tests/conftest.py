@@ -52,3 +52,8 @@ def golden_fit():
 @pytest.fixture(scope='session')
 def golden_layered():
     return load_golden('layered')
+
+
+@pytest.fixture(scope='session')
+def golden_estimate():
+    return load_golden('estimate')

@@ -17,6 +17,7 @@ Outputs (small, committed):
   layered.npz   sphere_coefficients (one layer, scalar input) for a table
   holo.npz      LorenzMie.field/hologram for the reference tests' geometries
   fit.npz       a seeded 201x201 fit by the reference Optimizer
+  estimate.npz  seeded DEEstimator and RadialEstimator searches (81x81 crop)
 '''
 import os
 import sys
@@ -160,10 +161,48 @@ def make_fit(seed=20240521):
                         seed=np.array(seed))
 
 
+def make_estimate(seed=11):
+    from pylorenzmie.theory.LorenzMie import LorenzMie
+    from pylorenzmie.analysis.DEEstimator import DEEstimator
+    from pylorenzmie.analysis.RadialEstimator import RadialEstimator
+    from pylorenzmie.analysis.Hologram import Hologram
+    rng = np.random.default_rng(seed)
+    shape = (81, 81)
+    truth = dict(x_p=40.3, y_p=39.7, z_p=150., a_p=0.75, n_p=1.42, k_p=0.)
+
+    def model():
+        m = LorenzMie(coordinates=LorenzMie.meshgrid(shape))
+        m.instrument.wavelength = 0.447
+        m.instrument.magnification = 0.048
+        m.instrument.n_m = 1.340
+        return m
+    m = model()
+    m.properties = truth
+    data = (m.hologram() + rng.normal(0., 0.05, shape[0] * shape[1])
+            ).reshape(shape)
+    serial = {'tol': 0.01, 'polish': False, 'updating': 'deferred',
+              'workers': 1}
+    m = model()
+    np.random.seed(7)  # the DE pixel subset (Mask draws from numpy's global RNG)
+    de = DEEstimator(model=m, seed=3, settings=dict(serial)).estimate(
+        Hologram(data))
+    m = model()
+    radial = RadialEstimator(model=m, seed=3, settings=dict(serial)).estimate(
+        Hologram(data))
+    keys = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+    np.savez_compressed(HERE / 'estimate.npz', data=data,
+                        truth=np.array([truth[k] for k in keys]),
+                        de=np.array([float(de[k]) for k in keys]),
+                        radial=np.array([float(radial[k]) for k in keys]),
+                        mask_seed=np.array(7), de_seed=np.array(3),
+                        seed=np.array(seed))
+
+
 if __name__ == '__main__':
     import_reference()
     make_ab()
     make_layered()
     make_holo()
     make_fit()
+    make_estimate()
     print('golden fixtures written to', HERE)

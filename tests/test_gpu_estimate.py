@@ -1,0 +1,172 @@
+'''GPU: the population chi^2 kernel (lmb_chi2_batch) and the estimators
+that drive it (DEEstimator, RadialEstimator), and Frame / Feature with the
+batched Frame.optimize.  Parity anchors: the oracle's hologram for the
+kernel, the reference's own seeded searches (tests/golden/estimate.npz) for
+the estimators, and per-feature Optimizer.optimize for Frame.optimize.'''
+import numpy as np
+import pytest
+
+from oracle import field as ofield
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+
+
+def _model(shape=(81, 81), fp64=False):
+    from pylorenzmie_b200 import LorenzMie, Instrument
+    inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
+    return LorenzMie(coordinates=LorenzMie.meshgrid(shape), instrument=inst,
+                     double_precision=fp64)
+
+
+def test_population_chi2_matches_oracle():
+    import torch
+    from pylorenzmie_b200.theory import _kernels as K
+    rng = np.random.default_rng(2)
+    c = ofield.meshgrid((41, 53))
+    keep = rng.random(c.shape[1]) < 0.3
+    coords = c[:, keep]
+    truth = dict(zip(KEYS, [20.2, 25.9, 140., 0.8, 1.45, 0.]))
+    inst = ofield.DEFAULT_INSTRUMENT
+    data = ofield.hologram(coords, [truth], inst) + \
+        rng.normal(0., 0.05, coords.shape[1])
+    data[3] = np.nan                      # skipped, as numpy.nansum does
+    S = 37
+    P = np.tile([20.2, 25.9, 140., 0.8, 1.45, 0.], (S, 1))
+    P[:, 2] = rng.uniform(50., 300., S)
+    P[:, 3] = rng.uniform(0.3, 3.0, S)
+    P[:, 4] = rng.uniform(1.1, 2.5, S)
+    ref = np.array([np.nansum(((ofield.hologram(coords, [dict(zip(KEYS, p))],
+                                                inst) - data) / 0.05) ** 2)
+                    for p in P])
+    dev = torch.device('cuda')
+    c3 = torch.from_numpy(np.vstack([coords, np.zeros(coords.shape[1])])
+                          ).to(dev)
+    d = torch.from_numpy(data).to(dev)
+    rec = np.zeros(S, dtype=K.SPHERE_DTYPE)
+    for j, k in enumerate(KEYS):
+        rec[k] = P[:, j]
+    sp = K.spheres_tensor(rec, dev)
+    cap = K.nmax_cap_for(P[:, 3], P[:, 4], P[:, 5], 1.34, 0.447)
+    ab, _, nmax = K.sphere_ab(sp, 1.34, 0.447, cap)
+    item_start = torch.arange(S + 1, dtype=torch.int32, device=dev)
+    k = ofield.wavenumber(1.34, 0.447, 0.048)
+    got = K.chi2(c3, d, 0.05, sp, item_start, ab, nmax, cap, k,
+                 fp64=True).cpu().numpy()
+    np.testing.assert_allclose(got, ref, rtol=1e-10)
+    # FP32 sums: accurate where finite; candidates whose focal plane cuts
+    # the sphere overflow FP32 and are flagged ...
+    got, bad = K.chi2(c3, d, 0.05, sp, item_start, ab, nmax, cap, k,
+                      nonfinite=True)
+    got, bad = got.cpu().numpy(), bad.cpu().numpy()
+    ok = bad == 0
+    assert ok.sum() >= S // 2
+    np.testing.assert_allclose(got[ok], ref[ok], rtol=2e-5)
+    inside = P[:, 2] < P[:, 3] / 0.048      # z_p inside the sphere
+    assert np.all(inside[~ok])
+    # ... and the population objective re-evaluates those in FP64
+    from pylorenzmie_b200.analysis._population import PopulationChi2
+    m = _model(shape=(41, 53))
+    m.particle.x_p, m.particle.y_p = 20.2, 25.9
+    obj = PopulationChi2(m, data, coords, ['z_p', 'a_p', 'n_p'], 0.05)
+    np.testing.assert_allclose(obj(P[:, 2:5].T), ref, rtol=2e-5)
+
+
+@pytest.mark.parametrize('which', ['de', 'radial'])
+def test_estimators_follow_reference_search(golden_estimate, which):
+    '''FP64 model: the population search reproduces the reference's seeded
+    differential evolution (same pixel subset, same trajectory).  FP32:
+    the same basin.'''
+    from pylorenzmie_b200 import Hologram, DEEstimator, RadialEstimator
+    g = golden_estimate
+    ref = g[which]
+    for fp64 in (True, False):
+        m = _model(fp64=fp64)
+        m.particle.a_p, m.particle.n_p, m.particle.z_p = 1.0, 1.5, 100.
+        serial = {'tol': 0.01, 'polish': False, 'updating': 'deferred',
+                  'workers': 1}
+        if which == 'de':
+            est = DEEstimator(model=m, seed=int(g['de_seed']), settings=serial)
+            np.random.seed(int(g['mask_seed']))
+        else:
+            est = RadialEstimator(model=m, seed=int(g['de_seed']),
+                                  settings=serial)
+        out = est.estimate(Hologram(g['data']))
+        got = np.array([out[k] for k in KEYS[:5]])
+        if fp64:
+            np.testing.assert_allclose(got, ref[:5], rtol=1e-8)
+        elif which == 'de':
+            np.testing.assert_allclose(got, ref[:5], rtol=0.02)
+        else:
+            # the reference's radial search ends in a local minimum that
+            # FP32 rounding of the energies may or may not reproduce
+            lo = [b[0] for b in est.bounds.values()]
+            hi = [b[1] for b in est.bounds.values()]
+            assert np.all((got[2:5] >= lo) & (got[2:5] <= hi))
+        assert m.particle.a_p == out['a_p']
+
+
+def _frame_data(shape=(200, 400), seed=4):
+    rng = np.random.default_rng(seed)
+    truth = [[60.3, 70.6, 160., 0.8, 1.45, 0.],
+             [330.2, 90.4, 200., 1.1, 1.50, 0.],
+             [190.7, 140.1, 140., 0.6, 1.40, 0.]]
+    c = ofield.meshgrid(shape)
+    h = ofield.hologram(c, [dict(zip(KEYS, t)) for t in truth],
+                        ofield.DEFAULT_INSTRUMENT)
+    data = (h + rng.normal(0., 0.05, h.shape)).reshape(shape)
+    bboxes = [((int(t[0]) - 30, int(t[1]) - 30), 61, 61) for t in truth]
+    return data, np.array(truth), bboxes
+
+
+def test_frame_optimize_batches_features():
+    '''Frame.optimize (one batched device fit) gives each feature exactly
+    the result of its own Optimizer.optimize on the same pixels.'''
+    from pylorenzmie_b200 import Frame, Instrument
+    data, truth, bboxes = _frame_data()
+    inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
+
+    def frame():
+        f = Frame(data, instrument=inst)
+        f.bboxes = bboxes
+        for feat, t in zip(f.features, truth):
+            feat.mask.fraction = 1.0        # deterministic pixel sets
+            feat.particle.x_p, feat.particle.y_p = t[0] + 0.3, t[1] - 0.2
+            feat.particle.z_p = t[2] + 8.
+            feat.particle.a_p = t[3] * 1.04
+            feat.particle.n_p = t[4] + 0.02
+        return f
+    fa = frame()
+    batched = fa.optimize()
+    fb = frame()
+    single = [feat.optimize() for feat in fb.features]
+    assert len(batched) == 3
+    for i in range(3):
+        for k in batched.columns:
+            assert batched.iloc[i][k] == single[i][k], (i, k)
+        assert abs(batched.iloc[i]['a_p'] - truth[i][3]) < 0.03
+    # each feature keeps its own result, as after feature.optimize()
+    for feat, (_, row) in zip(fa.features, batched.iterrows()):
+        assert feat.optimizer.result['z_p'] == row['z_p']
+        assert feat.particle.z_p == row['z_p']
+
+
+def test_feature_mask_and_residuals():
+    from pylorenzmie_b200 import Frame, Instrument
+    data, truth, bboxes = _frame_data()
+    data = data.copy()
+    data[75, 65] = data.max() + 1.      # saturated pixel inside feature 0
+    f = Frame(data, instrument=Instrument(wavelength=0.447,
+                                          magnification=0.048, n_m=1.340))
+    f.bboxes = bboxes
+    feat = f.features[0]
+    assert feat.corner == (30.0, 40.0)
+    assert feat.mask.exclude.sum() == 1
+    feat.particle.x_p, feat.particle.y_p = truth[0][:2]
+    feat.particle.z_p, feat.particle.a_p, feat.particle.n_p = truth[0][2:5]
+    # the model alone (no neighbours): residuals are noise plus the
+    # neighbouring spheres' faint fringes
+    r = feat.residuals()
+    assert r.shape == feat.shape
+    assert np.nanstd(r) < 0.2

@@ -84,3 +84,25 @@ def test_coordinates_and_wavenumber():
         field.coordinates3(np.zeros((4, 2)))
     k = field.wavenumber(1.34, 0.447, 0.048)
     assert abs(k - 2 * np.pi / 0.447 * 1.34 * 0.048) < 1e-15
+
+
+def test_oracle_estimators_match_reference(golden_estimate):
+    '''The oracle's DEEstimator and RadialEstimator restatements reproduce
+    the reference's seeded searches (same pixel subset, same scipy DE
+    trajectory).'''
+    from oracle import estimate, field
+    g = golden_estimate
+    data = g['data']
+    coords = field.meshgrid(data.shape, flatten=False)
+    part = dict(zip(('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p'),
+                    [0., 0., 100., 1.0, 1.5, 0.]))
+    np.random.seed(int(g['mask_seed']))
+    p, _ = estimate.de_estimate(data, coords, part, field.DEFAULT_INSTRUMENT,
+                                seed=int(g['de_seed']))
+    got = np.array([p[k] for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')])
+    np.testing.assert_allclose(got, g['de'][:5], rtol=1e-9)
+    p, _ = estimate.radial_estimate(data, coords, (0., 0.), part,
+                                    field.DEFAULT_INSTRUMENT,
+                                    seed=int(g['de_seed']))
+    got = np.array([p[k] for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')])
+    np.testing.assert_allclose(got, g['radial'][:5], rtol=1e-9)
