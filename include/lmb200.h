@@ -115,6 +115,26 @@ int lmb_hologram(const double *coords, long long npts,
                  int flags, void *out, void *stream);
 
 /*
+ * lmb_field / lmb_hologram of an instrument with spherical aberration:
+ * each particle's scattered field is multiplied by exp(i Phi) with
+ *   Phi = aberration * r^4 / (r^2 + z_p^2)^2,
+ *   aberration = 4 n_m^3 spherical / k  (k in rad/pixel),
+ * r the in-plane distance from the particle and z_p its axial position
+ * (pixels).  Replaces AberratedLorenzMie._aberration / scattered_field
+ * (theory/Aberrated.py:62-85); aberration = 0 is lmb_field / lmb_hologram.
+ */
+int lmb_field_aberrated(const double *coords, long long npts,
+                        const lmb_sphere *spheres, const int *item_start,
+                        int nitems, const double *ab, const int *nmax,
+                        int nmax_cap, double k, int flags, double aberration,
+                        void *out, void *stream);
+int lmb_hologram_aberrated(const double *coords, long long npts,
+                           const lmb_sphere *spheres, const int *item_start,
+                           int nitems, const double *ab, const int *nmax,
+                           int nmax_cap, double k, int flags,
+                           double aberration, void *out, void *stream);
+
+/*
  * chi^2 = sum over pixels of ((hologram - data) / noise)^2 for each of
  * nitems particle lists at shared coordinates: the objective of one
  * differential-evolution generation in one launch.  Replaces the

@@ -147,3 +147,27 @@ def hologram(coordinates, particles, instrument, cartesian=True, bohren=True):
 
 DEFAULT_INSTRUMENT = dict(wavelength=0.447, magnification=0.048,
                           n_m=1.340, numerical_aperture=1.45, noise=0.05)
+
+
+def aberrated_hologram(coordinates, particles, instrument, spherical,
+                       cartesian=True, bohren=True):
+    '''Hologram of AberratedLorenzMie (theory/Aberrated.py:62-85): each
+    particle's scattered field times exp(i Phi), Phi = (4 n_m^3 / k) s
+    r^4 / (r^2 + z_p^2)^2 with r the in-plane distance from the particle
+    (pixels) and z_p its axial position.'''
+    c = coordinates3(coordinates)
+    k = wavenumber(instrument['n_m'], instrument['wavelength'],
+                   instrument['magnification'])
+    out = np.zeros(c.shape, complex)
+    for p in particles:
+        f = scattered_field(c, p, instrument, cartesian, bohren)
+        if spherical != 0.:
+            x = c[0] - p['x_p']
+            y = c[1] - p['y_p']
+            rsq = x * x + y * y
+            phase = (4. * instrument['n_m'] ** 3 / k) * spherical * \
+                rsq ** 2 / (rsq + p['z_p'] ** 2) ** 2
+            f = f * np.exp(1j * phase)
+        out += f
+    out[0, :] += 1.
+    return np.sum(out.real ** 2 + out.imag ** 2, axis=0)

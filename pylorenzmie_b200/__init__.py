@@ -8,7 +8,8 @@ reference interface.  Importing the package does not touch the GPU.
 __version__ = '0.1.0'
 
 from .lib import meshgrid, LMObject  # noqa: F401
-from .theory import (Particle, Sphere, LayeredSphere, Instrument,  # noqa: F401
-                     LorenzMie)
+from .theory import (Particle, Sphere, LayeredSphere, Cluster,  # noqa: F401
+                     Dimer, Instrument, LorenzMie, Aberrated,
+                     AberratedLorenzMie)
 from .analysis import (Hologram, Mask, Optimizer, DEEstimator,  # noqa: F401
                        RadialEstimator, Feature, Frame)

@@ -78,6 +78,10 @@ _SIGNATURES = {
                        _vp]),
     'lmb_hologram': (_i, [_vp, _ll, _vp, _vp, _i, _vp, _vp, _i, _d, _i, _vp,
                           _vp]),
+    'lmb_field_aberrated': (_i, [_vp, _ll, _vp, _vp, _i, _vp, _vp, _i, _d,
+                                 _i, _d, _vp, _vp]),
+    'lmb_hologram_aberrated': (_i, [_vp, _ll, _vp, _vp, _i, _vp, _vp, _i,
+                                    _d, _i, _d, _vp, _vp]),
     'lmb_jacobian': (_i, [_vp, _ll, _vp, _i, _vp, _vp, _vp, _i, _d, _i, _vp,
                           _vp, _vp]),
     'lmb_vjp_workspace_bytes': (_sz, [_ll, _i]),

@@ -157,6 +157,8 @@ class Optimizer(LMObject):
             return False
         if not set(self.variables) <= set(PARAM_KEYS) or not self.variables:
             return False
+        if getattr(self.model, '_aberration', lambda: 0.)() != 0.:
+            return False  # the device fit models ideal optics
         p = self.model.particle
         return len(p) == 1 and hasattr(p, 'a_p')
 
@@ -296,6 +298,9 @@ class Optimizer(LMObject):
         if not self._device_fit_ok() and not (
                 set(self.variables) <= set(PARAM_KEYS)):
             raise ValueError('optimize_batch fits sphere parameters only')
+        if getattr(self.model, '_aberration', lambda: 0.)() != 0.:
+            raise ValueError('optimize_batch models ideal optics; fit an '
+                             'aberrated model with optimize()')
         layers = None
         if particles is not None:
             layers = _fit.layers_of(list(particles))

@@ -17,6 +17,8 @@ def batchable(model, variables):
     p = model.particle
     if isinstance(p, (list, tuple)) or K.is_layered(p) or not hasattr(p, 'a_p'):
         return False
+    if len(p) != 1 or getattr(model, '_aberration', lambda: 0.)() != 0.:
+        return False
     return all(v in SPHERE_KEYS for v in variables)
 
 

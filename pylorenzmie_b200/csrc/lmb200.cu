@@ -117,8 +117,8 @@ int persistent_grid(const void* fn, int tpb, size_t smem) {
 template <typename R, bool kHolo>
 int field_launch(const double* coords, long long npts, const lmb_sphere* spheres,
                  const int* item_start, int nitems, const double* ab,
-                 const int* nmax, int nmax_cap, double k, int flags, void* out,
-                 void* stream) {
+                 const int* nmax, int nmax_cap, double k, int flags, double aberr,
+                 void* out, void* stream) {
   const int tpb = 256;
   const size_t smem = sizeof(Quad<R>) * 2 * (size_t(nmax_cap) + 1);
   auto fn = k_field<R, kHolo>;
@@ -126,7 +126,7 @@ int field_launch(const double* coords, long long npts, const lmb_sphere* spheres
   dim3 grid(unsigned((npts + tpb - 1) / tpb), unsigned(nitems));
   fn<<<grid, tpb, smem, as_stream(stream)>>>(
       coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
-      nmax_cap + 1, k, flags, out);
+      nmax_cap + 1, k, flags, aberr, out);
   LMB_CK(cudaGetLastError());
   return LMB_OK;
 }
@@ -134,20 +134,22 @@ int field_launch(const double* coords, long long npts, const lmb_sphere* spheres
 int field_common(bool holo, const double* coords, long long npts,
                  const lmb_sphere* spheres, const int* item_start, int nitems,
                  const double* ab, const int* nmax, int nmax_cap, double k,
-                 int flags, void* out, void* stream) {
+                 int flags, void* out, void* stream, double aberr = 0.) {
   if (nitems < 0 || npts < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
   if (nitems == 0 || npts == 0) return LMB_OK;
   if (!coords || !spheres || !item_start || !ab || !nmax || !out) return LMB_ERR_ARG;
   if (nitems > 65535 || (npts + 255) / 256 > 0x7fffffffLL) return LMB_ERR_ARG;
   if (flags & LMB_FP64)
     return holo ? field_launch<double, true>(coords, npts, spheres, item_start, nitems,
-                                             ab, nmax, nmax_cap, k, flags, out, stream)
+                                             ab, nmax, nmax_cap, k, flags, aberr, out,
+                                             stream)
                 : field_launch<double, false>(coords, npts, spheres, item_start, nitems,
-                                              ab, nmax, nmax_cap, k, flags, out, stream);
+                                              ab, nmax, nmax_cap, k, flags, aberr, out,
+                                              stream);
   return holo ? field_launch<float, true>(coords, npts, spheres, item_start, nitems, ab,
-                                          nmax, nmax_cap, k, flags, out, stream)
+                                          nmax, nmax_cap, k, flags, aberr, out, stream)
               : field_launch<float, false>(coords, npts, spheres, item_start, nitems, ab,
-                                           nmax, nmax_cap, k, flags, out, stream);
+                                           nmax, nmax_cap, k, flags, aberr, out, stream);
 }
 
 }  // namespace
@@ -217,6 +219,26 @@ int lmb_hologram(const double* coords, long long npts,
                  int flags, void* out, void* stream) {
   return field_common(true, coords, npts, spheres, item_start, nitems, ab, nmax,
                       nmax_cap, k, flags, out, stream);
+}
+
+int lmb_field_aberrated(const double* coords, long long npts,
+                        const lmb_sphere* spheres, const int* item_start,
+                        int nitems, const double* ab, const int* nmax,
+                        int nmax_cap, double k, int flags, double aberration,
+                        void* out, void* stream) {
+  if (!(aberration == aberration)) return LMB_ERR_ARG;
+  return field_common(false, coords, npts, spheres, item_start, nitems, ab, nmax,
+                      nmax_cap, k, flags, out, stream, aberration);
+}
+
+int lmb_hologram_aberrated(const double* coords, long long npts,
+                           const lmb_sphere* spheres, const int* item_start,
+                           int nitems, const double* ab, const int* nmax,
+                           int nmax_cap, double k, int flags, double aberration,
+                           void* out, void* stream) {
+  if (!(aberration == aberration)) return LMB_ERR_ARG;
+  return field_common(true, coords, npts, spheres, item_start, nitems, ab, nmax,
+                      nmax_cap, k, flags, out, stream, aberration);
 }
 
 size_t lmb_chi2_workspace_bytes(long long npts, int nitems) {

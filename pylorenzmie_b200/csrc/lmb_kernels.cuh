@@ -251,12 +251,25 @@ struct FieldOut<double> {
   typedef double2 C;
 };
 
+// Spherical-aberration phase of one particle at one pixel
+// (theory/Aberrated.py:62-79): Phi = c r^4 / (r^2 + z_p^2)^2 with
+// c = 4 n_m^3 s / k, r the in-plane distance from the particle (pixels).
+template <typename R>
+__device__ inline cplx<R> aberration_phase(double c, double dx, double dy,
+                                           double zp) {
+  const double rsq = dx * dx + dy * dy;
+  const double den = rsq + zp * zp;
+  const double phi = den > 0. ? c * (rsq / den) * (rsq / den) : 0.;
+  return cis(R(reduce_2pi(phi)));
+}
+
+// aberr: the coefficient c above, 0 for an ideal instrument.
 template <typename R, bool kHologram>
 __global__ void __launch_bounds__(256)
 k_field(const double* __restrict__ coords, long long npts,
         const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
         const zd* __restrict__ ab, const int* __restrict__ nmax, int nmaxp, double k,
-        int flags, void* out) {
+        int flags, double aberr, void* out) {
   extern __shared__ __align__(16) char smem[];
   Quad<R>* coef = reinterpret_cast<Quad<R>*>(smem);
   const int item = blockIdx.y;
@@ -285,6 +298,10 @@ k_field(const double* __restrict__ coords, long long npts,
       const Sums<R> s = order_sum<R>(g, coef, nm);
       cplx<R> ep[3];
       epilogue<R>(g, s, cart, ep);
+      if (aberr != 0.) {
+        const cplx<R> ph = aberration_phase<R>(aberr, x - sp.x_p, y - sp.y_p, sp.z_p);
+        for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
+      }
       for (int c = 0; c < 3; ++c) e[c] = e[c] + ep[c];
     }
   }

@@ -1,0 +1,57 @@
+'''Lorenz-Mie model of an instrument with spherical aberration (same
+contract as theory/Aberrated.py).
+
+``Aberrated(base)`` returns a subclass of a LorenzMie model whose scattered
+fields carry the phase exp(i Phi), Phi = (4 n_m^3 / k) s r^4/(r^2 + z_p^2)^2
+(theory/Aberrated.py:41-79), s = ``spherical`` in wavelengths, k the
+in-medium wave number (rad/pixel), r the in-plane distance from each
+particle and z_p its axial position, both in pixels.  Here the phase is
+applied inside the field kernel (lmb_field_aberrated /
+lmb_hologram_aberrated), per particle and pixel, before the superposition.
+The device fit and the analytic Jacobian do not include the aberration:
+with spherical != 0, Optimizer fits through its host loop on this model's
+holograms, and ``jac_params`` is empty.
+'''
+from .LorenzMie import LorenzMie
+
+
+def Aberrated(base_class):
+    '''An aberrated subclass of a LorenzMie model class.'''
+
+    class AberratedLorenzMie(base_class):
+
+        def __init__(self, *args, spherical=0., **kwargs):
+            super().__init__(*args, **kwargs)
+            self.spherical = spherical
+
+        @property
+        def properties(self):
+            return {**super().properties, 'spherical': self.spherical}
+
+        @properties.setter
+        def properties(self, properties):
+            base_class.properties.fset(self, properties)
+
+        @property
+        def jac_params(self):
+            return (base_class.jac_params if self.spherical == 0.
+                    else frozenset())
+
+        def _aberration(self):
+            if self.spherical == 0.:
+                return 0.
+            inst = self.instrument
+            return 4. * inst.n_m ** 3 / inst.wavenumber() * self.spherical
+
+        def jac(self, *args, **kwargs):
+            if self.spherical != 0.:
+                raise TypeError('jac() does not include spherical aberration')
+            return super().jac(*args, **kwargs)
+
+    return AberratedLorenzMie
+
+
+AberratedLorenzMie = Aberrated(LorenzMie)
+# a module-level name, so that instances pickle
+AberratedLorenzMie.__qualname__ = 'AberratedLorenzMie'
+AberratedLorenzMie.__name__ = 'AberratedLorenzMie'

@@ -153,17 +153,22 @@ class LorenzMie(LMObject):
                                           device=self.device)
         return sp, item_start, ab, dab, nmax, cap
 
+    def _aberration(self):
+        '''Coefficient of a spherical-aberration phase applied to every
+        particle's field (0: ideal optics; see theory/Aberrated.py).'''
+        return 0.
+
     def _field_items(self, particle_lists, cartesian, bohren):
         sp, item_start, ab, _, nmax, cap = self._prepare(particle_lists)
         return K.field(self._coords, sp, item_start, ab, nmax, cap,
                        self.instrument.wavenumber(), cartesian, bohren,
-                       self.double_precision)
+                       self.double_precision, self._aberration())
 
     def _hologram_items(self, particle_lists, cartesian, bohren):
         sp, item_start, ab, _, nmax, cap = self._prepare(particle_lists)
         return K.hologram(self._coords, sp, item_start, ab, nmax, cap,
                           self.instrument.wavenumber(), cartesian, bohren,
-                          self.double_precision)
+                          self.double_precision, self._aberration())
 
     # ------------------------------------------------------------------
     def field(self, cartesian=True, bohren=True, device=False):

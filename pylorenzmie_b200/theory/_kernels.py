@@ -89,8 +89,10 @@ def _flags(cartesian, bohren, fp64):
 
 
 def hologram(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
-             bohren=True, fp64=False):
-    '''(nitems, npts) holograms; float32, or float64 when fp64.'''
+             bohren=True, fp64=False, aberration=0.):
+    '''(nitems, npts) holograms; float32, or float64 when fp64.
+    ``aberration``: coefficient 4 n_m^3 s / k of a spherical-aberration
+    phase (0: none).'''
     coords, spheres, item_start, ab, nmax = _contiguous(
         coords, spheres, item_start, ab, nmax)
     lib = _native.load()
@@ -100,10 +102,16 @@ def hologram(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
     out = torch.empty((nitems, npts),
                       dtype=torch.float64 if fp64 else torch.float32,
                       device=dev)
+    flags = _flags(cartesian, bohren, fp64)
+    if aberration:
+        _native.check(lib.lmb_hologram_aberrated(
+            ptr(coords), npts, ptr(spheres), ptr(item_start), nitems, ptr(ab),
+            ptr(nmax), cap, float(k), flags, float(aberration), ptr(out),
+            stream_handle(dev)), 'lmb_hologram_aberrated')
+        return out
     _native.check(lib.lmb_hologram(ptr(coords), npts, ptr(spheres),
                                    ptr(item_start), nitems, ptr(ab), ptr(nmax),
-                                   cap, float(k),
-                                   _flags(cartesian, bohren, fp64), ptr(out),
+                                   cap, float(k), flags, ptr(out),
                                    stream_handle(dev)), 'lmb_hologram')
     return out
 
@@ -137,7 +145,7 @@ def chi2(coords, data, noise, spheres, item_start, ab, nmax, cap, k,
 
 
 def field(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
-          bohren=True, fp64=False):
+          bohren=True, fp64=False, aberration=0.):
     '''(nitems, 3, npts) scattered fields; complex64, or complex128.'''
     coords, spheres, item_start, ab, nmax = _contiguous(
         coords, spheres, item_start, ab, nmax)
@@ -148,10 +156,17 @@ def field(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
     out = torch.empty((nitems, 3, npts),
                       dtype=torch.complex128 if fp64 else torch.complex64,
                       device=dev)
+    flags = _flags(cartesian, bohren, fp64)
+    if aberration:
+        _native.check(lib.lmb_field_aberrated(
+            ptr(coords), npts, ptr(spheres), ptr(item_start), nitems, ptr(ab),
+            ptr(nmax), cap, float(k), flags, float(aberration), ptr(out),
+            stream_handle(dev)), 'lmb_field_aberrated')
+        return out
     _native.check(lib.lmb_field(ptr(coords), npts, ptr(spheres),
                                 ptr(item_start), nitems, ptr(ab), ptr(nmax),
-                                cap, float(k), _flags(cartesian, bohren, fp64),
-                                ptr(out), stream_handle(dev)), 'lmb_field')
+                                cap, float(k), flags, ptr(out),
+                                stream_handle(dev)), 'lmb_field')
     return out
 
 

@@ -57,3 +57,8 @@ def golden_layered():
 @pytest.fixture(scope='session')
 def golden_estimate():
     return load_golden('estimate')
+
+
+@pytest.fixture(scope='session')
+def golden_variants():
+    return load_golden('variants')

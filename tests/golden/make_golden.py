@@ -18,6 +18,7 @@ Outputs (small, committed):
   holo.npz      LorenzMie.field/hologram for the reference tests' geometries
   fit.npz       a seeded 201x201 fit by the reference Optimizer
   estimate.npz  seeded DEEstimator and RadialEstimator searches (81x81 crop)
+  variants.npz  AberratedLorenzMie and Dimer holograms
 '''
 import os
 import sys
@@ -198,6 +199,45 @@ def make_estimate(seed=11):
                         seed=np.array(seed))
 
 
+def make_variants():
+    from pylorenzmie.theory.LorenzMie import LorenzMie
+    from pylorenzmie.theory.Aberrated import Aberrated
+    from pylorenzmie.theory.Sphere import Sphere
+    from pylorenzmie.theory.Dimer import Dimer
+    out = {}
+    shape = (64, 72)
+    coords = LorenzMie.meshgrid(shape)
+    AbLM = Aberrated(LorenzMie)
+    cases = [(0.9, (30.3, 35.2, 140., 0.8, 1.45, 0.)),
+             (-2.5, (10.0, 60.0, 90., 1.2, 1.6, 0.002))]
+    for i, (spherical, p) in enumerate(cases):
+        s = Sphere(a_p=p[3], n_p=p[4], k_p=p[5])
+        s.r_p = list(p[:3])
+        m = AbLM(coordinates=coords, particle=s, spherical=spherical)
+        m.instrument.wavelength = 0.447
+        m.instrument.magnification = 0.048
+        m.instrument.n_m = 1.340
+        out[f'ab_holo_{i}'] = m.hologram()
+        out[f'ab_case_{i}'] = np.array([spherical, *p])
+    d = Dimer(magnification=0.048)
+    d.a_p = 0.5
+    d.n_p = 1.42
+    d.r_p = [36., 30., 250.]
+    d.theta = np.pi / 5.
+    d.phi = np.pi / 3.
+    m = LorenzMie(coordinates=coords, particle=d)
+    m.instrument.wavelength = 0.447
+    m.instrument.magnification = 0.048
+    m.instrument.n_m = 1.340
+    out['dimer_holo'] = m.hologram()
+    out['dimer_case'] = np.array([36., 30., 250., 0.5, 1.42, 0., np.pi / 5.,
+                                  np.pi / 3.])
+    out['dimer_spheres'] = np.array([[*(q.r_p + q.r_0), q.a_p, q.n_p, q.k_p]
+                                     for q in d.particles])
+    out['shape'] = np.array(shape)
+    np.savez_compressed(HERE / 'variants.npz', **out)
+
+
 if __name__ == '__main__':
     import_reference()
     make_ab()
@@ -205,4 +245,5 @@ if __name__ == '__main__':
     make_holo()
     make_fit()
     make_estimate()
+    make_variants()
     print('golden fixtures written to', HERE)

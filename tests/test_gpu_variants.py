@@ -1,0 +1,94 @@
+'''GPU: model variants on the same kernels -- spherical aberration fused
+into the field kernel, Cluster / Dimer superposition -- against the
+reference's own holograms (tests/golden/variants.npz), and fits of
+aberrated models through the host loop.'''
+import numpy as np
+import pytest
+
+from oracle import field as ofield
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+
+
+def _inst():
+    from pylorenzmie_b200 import Instrument
+    return Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
+
+
+@pytest.mark.parametrize('fp64', [True, False])
+def test_aberrated_hologram_matches_reference(golden_variants, fp64):
+    from pylorenzmie_b200 import AberratedLorenzMie, Sphere, LorenzMie
+    g = golden_variants
+    shape = tuple(g['shape'])
+    for i in range(2):
+        case = g[f'ab_case_{i}']
+        s = Sphere(a_p=case[4], n_p=case[5], k_p=case[6])
+        s.r_p = case[1:4]
+        m = AberratedLorenzMie(coordinates=LorenzMie.meshgrid(shape),
+                               particle=s, instrument=_inst(),
+                               spherical=case[0], double_precision=fp64)
+        ref = g[f'ab_holo_{i}']
+        h = m.hologram()
+        tol = 1e-10 if fp64 else 2e-5 + 2e-6 * np.abs(ref)
+        assert np.all(np.abs(h - ref) <= tol), i
+        assert m.properties['spherical'] == case[0]
+        assert m.jac_params == frozenset()
+        with pytest.raises(TypeError):
+            m.jac()
+    # spherical = 0 is the ideal model, analytic Jacobian included
+    m.spherical = 0.
+    plain = LorenzMie(coordinates=m.coordinates, particle=s,
+                      instrument=_inst(), double_precision=fp64)
+    np.testing.assert_array_equal(m.hologram(), plain.hologram())
+    assert 'z_p' in m.jac_params
+
+
+@pytest.mark.parametrize('fp64', [True, False])
+def test_dimer_hologram_matches_reference(golden_variants, fp64):
+    from pylorenzmie_b200 import Dimer, LorenzMie, Sphere
+    g = golden_variants
+    x, y, z, a, n, k, theta, phi = g['dimer_case']
+    d = Dimer(magnification=0.048)
+    d.a_p, d.n_p = a, n
+    d.r_p = [x, y, z]
+    d.theta, d.phi = theta, phi
+    m = LorenzMie(coordinates=LorenzMie.meshgrid(tuple(g['shape'])),
+                  particle=d, instrument=_inst(), double_precision=fp64)
+    ref = g['dimer_holo']
+    tol = 1e-10 if fp64 else 2e-5 + 2e-6 * np.abs(ref)
+    assert np.all(np.abs(m.hologram() - ref) <= tol)
+    # the same pair as two free spheres in one batch item
+    pair = []
+    for q in d.particles:
+        s = Sphere(a_p=q.a_p, n_p=q.n_p, k_p=q.k_p)
+        s.r_p = q.r_p + q.r_0
+        pair.append(s)
+    hb = m.batch_hologram([pair, [pair[0]]])
+    np.testing.assert_allclose(hb[0], m.hologram(), atol=1e-12)
+
+
+def test_aberrated_fit_uses_host_loop():
+    '''With spherical != 0 the Optimizer fits through scipy on the
+    aberrated GPU hologram (the device fit models ideal optics) and
+    recovers the sphere; optimize_batch refuses such a model.'''
+    from pylorenzmie_b200 import (AberratedLorenzMie, Sphere, Optimizer,
+                                  Hologram, LorenzMie)
+    shape = (61, 61)
+    truth = dict(zip(KEYS, [30.4, 29.8, 150., 0.75, 1.45, 0.]))
+    c = ofield.meshgrid(shape)
+    h = ofield.aberrated_hologram(c, [truth], ofield.DEFAULT_INSTRUMENT, 1.5)
+    data = h + np.random.default_rng(3).normal(0., 0.05, h.shape)
+    s = Sphere(a_p=0.78, n_p=1.46, k_p=0.)
+    s.r_p = [30., 30., 158.]
+    m = AberratedLorenzMie(coordinates=LorenzMie.meshgrid(shape), particle=s,
+                           instrument=_inst(), spherical=1.5)
+    opt = Optimizer(model=m)
+    assert not opt._device_fit_ok()
+    r = opt.optimize(Hologram(data.reshape(shape)))
+    assert r['success']
+    assert abs(r['a_p'] - 0.75) < 0.01 and abs(r['z_p'] - 150.) < 1.
+    with pytest.raises(ValueError):
+        opt.optimize_batch([Hologram(data.reshape(shape))],
+                           starts=np.array([[30., 30., 158., 0.78, 1.46, 0.]]))

@@ -106,3 +106,45 @@ def test_oracle_estimators_match_reference(golden_estimate):
                                     seed=int(g['de_seed']))
     got = np.array([p[k] for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')])
     np.testing.assert_allclose(got, g['radial'][:5], rtol=1e-9)
+
+
+def test_oracle_aberrated_and_dimer(golden_variants):
+    '''Aberrated holograms and a Dimer (two spheres placed by the cluster
+    geometry) against the reference's own output.'''
+    g = golden_variants
+    shape = tuple(g['shape'])
+    c = field.meshgrid(shape)
+    keys = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+    for i in range(2):
+        case = g[f'ab_case_{i}']
+        h = field.aberrated_hologram(c, [dict(zip(keys, case[1:]))],
+                                     field.DEFAULT_INSTRUMENT, case[0])
+        assert np.abs(h - g[f'ab_holo_{i}']).max() < 1e-10
+    h = field.hologram(c, [dict(zip(keys, s)) for s in g['dimer_spheres']],
+                       field.DEFAULT_INSTRUMENT)
+    assert np.abs(h - g['dimer_holo']).max() < 1e-10
+
+
+def test_cluster_and_dimer_geometry(golden_variants):
+    '''Host classes: the Dimer places its spheres where the reference does;
+    moving a Cluster moves its members' origins.'''
+    from pylorenzmie_b200 import Dimer, Cluster, Sphere
+    g = golden_variants
+    x, y, z, a, n, k, theta, phi = g['dimer_case']
+    d = Dimer(magnification=0.048)
+    d.a_p = a
+    d.n_p = n
+    d.r_p = [x, y, z]
+    d.theta = theta
+    d.phi = phi
+    got = np.array([[*(q.r_p + q.r_0), q.a_p, q.n_p, q.k_p]
+                    for q in d.particles])
+    np.testing.assert_allclose(got, g['dimer_spheres'], rtol=1e-13)
+    assert set(d.properties) == {'x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p',
+                                 'theta', 'phi'}
+    s1, s2 = Sphere(), Sphere()
+    s2.r_p = [5., 0., 0.]
+    cl = Cluster(particles=[s1, s2])
+    cl.r_p = [10., 20., 100.]
+    assert list(s2.r_p + s2.r_0) == [15., 20., 100.]
+    assert len(cl) == 2 and list(cl)[1] is s2
