@@ -373,7 +373,7 @@ int lmb_fit_batch_streamed(const lmb_feature *features, int nfeatures,
  * (cudaGetSymbolAddress, with that device current); make that first call
  * before any stream capture.  Requests whose lmb_fit_workspace_bytes
  * exceed LMB_FIT_NOALLOC_SCRATCH_BYTES are rejected with
- * LMB_ERR_WORKSPACE before anything is launched (about 700 features of
+ * LMB_ERR_WORKSPACE before anything is launched (about 500 features of
  * 201x201 pixels fit at the capacity a 0.75 um sphere needs).  All calls share the one array, which keeps the
  * last call's contents; the fit re-initializes every counter, state and
  * table it reads, and the counters are zeroed again at each call.  Calls
