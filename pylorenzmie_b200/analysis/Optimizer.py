@@ -320,6 +320,63 @@ class Optimizer(LMObject):
         return batch_frame(params, res, npix, self.variables)
 
 
+    def optimize_stream(self, batches, autotune=None, depth=2):
+        '''Fit a stream of batches (video frames, say), pipelined: while
+        the GPU fits one batch, the next is converted and copied.  Yields
+        one DataFrame per batch, in order, as optimize_batch returns it.
+
+        batches : iterable of (holograms, starts) or (holograms,
+                  particles) pairs; starts an array (B, 6), particles a
+                  list of Sphere or LayeredSphere start values
+        autotune: time the evaluation kernel's launch shapes on the first
+                  batch (default: when it has 64 features or more)
+        depth   : batches in flight (pinned buffers); 2 overlaps the host
+                  work of one batch with the fit of the previous
+        '''
+        if not self._device_fit_ok() and not (
+                set(self.variables) <= set(PARAM_KEYS)):
+            raise ValueError('optimize_stream fits sphere parameters only')
+        if getattr(self.model, '_aberration', lambda: 0.)() != 0.:
+            raise ValueError('optimize_stream models ideal optics')
+        variables = list(self.variables)
+        first = [True]
+
+        def items():
+            for holograms, second in batches:
+                layers = None
+                if not (len(second) and hasattr(second[0], 'r_p')):
+                    starts = np.asarray(second, dtype=float).reshape(-1, 6)
+                else:
+                    layers = _fit.layers_of(list(second))
+                    starts = np.array([[*(np.asarray(p.r_p, float) +
+                                          np.asarray(getattr(
+                                              p, 'r_0', (0., 0., 0.)),
+                                              float)), p.a_p, p.n_p,
+                                        getattr(p, 'k_p', 0.)]
+                                       for p in second], dtype=float)
+                if first[0]:
+                    first[0] = False
+                    self._stream_tune = (autotune if autotune is not None
+                                         else len(holograms) >= 64)
+                yield [self._pixels(h) for h in holograms], starts, layers
+
+        gen = items()
+        # the first batch decides autotuning before the pipeline starts
+        try:
+            head = next(gen)
+        except StopIteration:
+            return
+
+        def chain():
+            yield head
+            yield from gen
+        for params, res, npix in _fit.fit_stream(
+                chain(), self.model.instrument, variables, self.settings,
+                device=self.model.device, autotune=self._stream_tune,
+                depth=depth):
+            yield batch_frame(params, res, npix, variables)
+
+
 def batch_frame(params, res, npix, variables):
     '''DataFrame of batched fit results in the Optimizer.result layout.'''
     idx = [PARAM_KEYS.index(v) for v in variables]

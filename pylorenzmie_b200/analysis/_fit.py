@@ -537,3 +537,122 @@ def _fit_streamed(stream, d_feat, d_data, d_coords, d_params, n, total,
         res = d_res[:n * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
             _native.RESULT_DTYPE).copy()
     return params, res
+
+
+_stream_staging = []
+_STREAM_WORKER = None
+
+
+_stream_fit_streams = {}
+
+
+def _stream_worker(n):
+    '''Threads that drive the fits of fit_stream, one per batch in flight:
+    two consecutive fits run on different streams, so the kernels of one
+    fill the GPU while the other waits on its host round trip.'''
+    global _STREAM_WORKER
+    if _STREAM_WORKER is None or _STREAM_WORKER._max_workers < n:
+        from concurrent.futures import ThreadPoolExecutor
+        _STREAM_WORKER = ThreadPoolExecutor(max_workers=n)
+    return _STREAM_WORKER
+
+
+def _stream_fit_stream(dev, slot):
+    key = (dev, slot)
+    if key not in _stream_fit_streams:
+        _stream_fit_streams[key] = torch.cuda.Stream(dev)
+    return _stream_fit_streams[key]
+
+
+def fit_stream(batches, instrument, variables, settings=None, device=None,
+               autotune=False, depth=2):
+    '''Fit a sequence of batches, pipelined; yields, in order, (params
+    (B, 6), results record array, npix (B,)) per batch.
+
+    ``batches`` yields (items, starts, layers): items as for fit_items.
+    While the device fits batch k (driven by a worker thread, on the fit
+    stream), the caller's thread converts batch k+1 into the next of
+    ``depth`` pinned buffers and copies it on the copy stream; the fit of
+    k+1 waits for that copy on the device, not on the host, and runs on a
+    stream of its own (consecutive fits may overlap on the GPU).  A pinned
+    buffer is rewritten only after its previous copy has completed.'''
+    from collections import deque
+    dev = get_device(device)
+    _, s_copy = _fit_streams(dev)
+    while len(_stream_staging) < depth:
+        _stream_staging.append(_Staging())
+    pending = deque()          # (future, copy-done event)
+    done_events = [None] * depth
+    tile_config = None
+    k = 0
+    try:
+        for items, starts, layers in batches:
+            starts = np.ascontiguousarray(starts, dtype=np.float64
+                                          ).reshape(-1, 6)
+            B = starts.shape[0]
+            packed = PackedFeatures(items)
+            npix = packed.features['npix'].astype(np.int64)
+            if B == 0:
+                pending.append((None, (starts.copy(), np.zeros(
+                    0, dtype=_native.RESULT_DTYPE), npix)))
+                k += 1
+                continue
+            nmax_cap = fit_capacity(starts, float(instrument.n_m),
+                                    float(instrument.wavelength), layers)
+            if tile_config is None:
+                tile_config = 0
+                if autotune:
+                    from .. import autotune as _tuner
+                    tile_config = _tuner.tune(packed, starts, instrument,
+                                              variables, nmax_cap, layers,
+                                              dev)
+            slot = k % depth
+            s_fit = _stream_fit_stream(dev, slot)
+            if done_events[slot] is not None:
+                done_events[slot].synchronize()  # its last copy has landed
+            buf, offs, nbytes = stage(packed, starts, _stream_staging[slot])
+            with torch.cuda.stream(s_copy):
+                views = to_device(buf, offs, nbytes, dev)
+                ev = torch.cuda.Event()
+                ev.record(s_copy)
+            done_events[slot] = ev
+            for v in views:
+                if v is not None:
+                    v.record_stream(s_fit)
+            pending.append((_stream_worker(depth).submit(
+                _fit_after, s_fit, ev, views, B, packed.total, instrument,
+                variables, settings, nmax_cap, starts, tile_config, layers),
+                npix))
+            k += 1
+            while len(pending) >= depth:
+                yield _collect(pending.popleft())
+        while pending:
+            yield _collect(pending.popleft())
+    finally:
+        for fut, _ in pending:
+            if fut is not None:
+                fut.result()
+        s_copy.synchronize()
+
+
+def _collect(entry):
+    fut, extra = entry
+    if fut is None:
+        return extra
+    params, res = fut.result()
+    return params, res, extra
+
+
+def _fit_after(stream, event, views, n, total, instrument, variables,
+               settings, nmax_cap, starts, tile_config, layers):
+    d_feat, d_data, d_coords, d_params = views
+    stream.wait_event(event)
+    with torch.cuda.stream(stream):
+        d_res, _ = fit_device(d_feat, d_data, d_coords, d_params, n, total,
+                              instrument, variables, settings, nmax_cap,
+                              starts, False, tile_config=tile_config,
+                              layers=layers)
+        params = d_params.view(torch.float64).reshape(n, 6).cpu().numpy()
+        res = d_res[:n * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
+            _native.RESULT_DTYPE).copy()
+    return params, res

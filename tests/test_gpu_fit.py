@@ -262,3 +262,28 @@ def test_distributed_fit_single_rank_is_optimize_batch():
     d1 = optimize_batch_distributed(opt, holos, starts=start, autotune=False)
     for col in d0.columns:
         np.testing.assert_array_equal(d0[col].to_numpy(), d1[col].to_numpy())
+
+
+def test_stream_matches_batch():
+    '''optimize_stream (pipelined batches: conversion and copy of one
+    batch overlap the fit of the previous) yields, batch by batch, exactly
+    what optimize_batch returns; an empty batch in the stream gives an
+    empty frame.'''
+    from pylorenzmie_b200 import Hologram, workloads
+    batches = []
+    for seed in range(4):
+        truth, start = workloads.batch_201(6 + seed, seed=30 + seed)
+        truth[:, :2] -= 60.
+        start[:, :2] -= 60.
+        data = workloads.render(truth, (81, 81), seed=30 + seed).cpu().numpy()
+        batches.append(([Hologram(d.astype(float)) for d in data], start))
+    batches.insert(2, ([], np.zeros((0, 6))))
+    opt = make_optimizer(batches[0][1][0], (8, 8))
+    ref = [opt.optimize_batch(h, starts=s, autotune=False, chunks=1)
+           for h, s in batches]
+    got = list(opt.optimize_stream(iter(batches), autotune=False))
+    assert len(got) == len(ref)
+    for a, b in zip(ref, got):
+        assert len(a) == len(b)
+        for col in a.columns:
+            np.testing.assert_array_equal(a[col].to_numpy(), b[col].to_numpy())
