@@ -120,6 +120,18 @@ int field_launch(const double* coords, long long npts, const lmb_sphere* spheres
                  const int* nmax, int nmax_cap, double k, int flags, double aberr,
                  void* out, void* stream) {
   const int tpb = 256;
+  if constexpr (sizeof(R) == sizeof(float)) {
+    // FP32: the packed two-pixel loop, two adjacent pixels per thread
+    const size_t smem = sizeof(float4) * PAIRV_QUADS * (size_t(nmax_cap) + 1);
+    auto fn = k_field_pair<kHolo>;
+    LMB_CK(smem_attr((const void*)fn, smem));
+    dim3 grid(unsigned((npts + 2 * tpb - 1) / (2 * tpb)), unsigned(nitems));
+    fn<<<grid, tpb, smem, as_stream(stream)>>>(
+        coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
+        nmax_cap + 1, k, flags, aberr, out);
+    LMB_CK(cudaGetLastError());
+    return LMB_OK;
+  }
   const size_t smem = sizeof(Quad<R>) * 2 * (size_t(nmax_cap) + 1);
   auto fn = k_field<R, kHolo>;
   LMB_CK(smem_attr((const void*)fn, smem));

@@ -225,6 +225,21 @@ __device__ void stage_coef(const zd* ab, const zd* dab, int nmax,
   }
 }
 
+// Records of order_sum_pair (value only): PAIRV_QUADS float4 per order,
+// i.e. PAIRV_VALUES float2 (v, v).  Three threads per order, so that the
+// FP64 work of staging is spread over the block.
+__device__ void stage_pair_value(const zd* ab, int nmax, float4* sm) {
+  float2* r2 = reinterpret_cast<float2*>(sm);
+  for (int t = threadIdx.x; t < 3 * (nmax + 1); t += blockDim.x) {
+    const int n = t / 3, part = t - 3 * n;
+    float v[PAIRV_VALUES];
+    pair_value_part(ab + 2 * n, n, part, v);
+    const int lo = part == 0 ? 0 : (part == 1 ? 7 : 10);
+    const int hi = part == 0 ? 7 : (part == 1 ? 10 : PAIRV_VALUES);
+    for (int j = lo; j < hi; ++j) r2[PAIRV_VALUES * n + j] = make_float2(v[j], v[j]);
+  }
+}
+
 // Records of order_sum_jac_pair: PAIR_QUADS float4 per order, every value
 // duplicated into both lanes of a float2.
 __device__ void stage_pair(const zd* ab, const zd* dab, int nmax, float4* sm) {
@@ -317,6 +332,79 @@ k_field(const double* __restrict__ coords, long long npts,
       v.x = e[c].re;
       v.y = e[c].im;
       o[c * npts + pix] = v;
+    }
+  }
+}
+
+// FP32 field / hologram with the packed two-pixel loop: each thread takes
+// two adjacent pixels (the last thread of an odd count pairs its pixel with
+// itself).  Same inputs, outputs and arithmetic as k_field<float, holo>;
+// the order loop runs in f32x2 (order_sum_pair).
+template <bool kHologram>
+__global__ void __launch_bounds__(256)
+k_field_pair(const double* __restrict__ coords, long long npts,
+             const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
+             const zd* __restrict__ ab, const int* __restrict__ nmax, int nmaxp,
+             double k, int flags, double aberr, void* out) {
+  extern __shared__ __align__(16) char smem[];
+  float4* rec = reinterpret_cast<float4*>(smem);
+  const int item = blockIdx.y;
+  const long long p0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+  const bool live0 = p0 < npts;
+  const bool live1 = p0 + 1 < npts;
+  const long long p1 = live1 ? p0 + 1 : p0;
+  const bool cart = flags & LMB_CARTESIAN;
+  const bool bohren = flags & LMB_BOHREN;
+  double x[2] = {0., 0.}, y[2] = {0., 0.}, z[2] = {0., 0.};
+  if (live0) {
+    x[0] = coords[p0];
+    y[0] = coords[npts + p0];
+    z[0] = coords[2 * npts + p0];
+    x[1] = coords[p1];
+    y[1] = coords[npts + p1];
+    z[1] = coords[2 * npts + p1];
+  }
+  cplx<float> e[2][3];
+  for (int l = 0; l < 2; ++l)
+    for (int c = 0; c < 3; ++c) e[l][c] = mk(0.f, 0.f);
+  const int pb = item_start[item], pe = item_start[item + 1];
+  for (int p = pb; p < pe; ++p) {
+    const int nm = min(max(nmax[p], 0), nmaxp - 1);
+    __syncthreads();
+    stage_pair_value(ab + size_t(p) * nmaxp * 2, nm, rec);
+    __syncthreads();
+    if (live0) {
+      const lmb_sphere sp = spheres[p];
+      Geometry<float> g[2];
+      for (int l = 0; l < 2; ++l)
+        g[l] = geometry<float>(k, x[l] - sp.x_p, y[l] - sp.y_p, z[l] - sp.z_p, z[l],
+                               sp.z_p, bohren);
+      PairSumsV S;
+      order_sum_pair(pair_in(g[0], g[1]), rec, nm, S);
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        const Sums<float> sl = pair_lane_value(S, l, g[l].smu);
+        cplx<float> ep[3];
+        epilogue<float>(g[l], sl, cart, ep);
+        if (aberr != 0.) {
+          const cplx<float> ph =
+              aberration_phase<float>(aberr, x[l] - sp.x_p, y[l] - sp.y_p, sp.z_p);
+          for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
+        }
+        for (int c = 0; c < 3; ++c) e[l][c] = e[l][c] + ep[c];
+      }
+    }
+  }
+  if (!live0) return;
+  for (int l = 0; l < 2; ++l) {
+    if (l == 1 && !live1) break;
+    const long long pix = l ? p1 : p0;
+    if (kHologram) {
+      float* o = reinterpret_cast<float*>(out) + (size_t)item * npts;
+      o[pix] = intensity<float>(e[l]);
+    } else {
+      float2* o = reinterpret_cast<float2*>(out) + (size_t)item * 3 * npts;
+      for (int c = 0; c < 3; ++c) o[c * npts + pix] = make_float2(e[l][c].re, e[l][c].im);
     }
   }
 }

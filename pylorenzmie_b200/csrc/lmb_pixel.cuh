@@ -459,6 +459,70 @@ LMB_HD void order_sum_jac_pair(const PairIn& in, const Q4* rec, int nmax,
   }
 }
 
+// The value-only loop (field and hologram) for two pixels at once, with
+// the signs and records of order_sum_jac_pair restricted to the value:
+// per order PAIRV_VALUES values, each duplicated into both lanes:
+//   0 n, 1 c_n, 2 (-1)^n (2n-1), 3 (-1)^{n+1} n,
+//   4 sig alpha, 7 -s beta, 10 s n(n+1) alpha (each re, im, -im); 13 unused.
+enum { PAIRV_VALUES = 14, PAIRV_QUADS = PAIRV_VALUES / 2 };
+
+struct PairSumsV {
+  cplx<f2> s[3];
+};
+
+template <typename Q4>
+LMB_HD void order_sum_pair(const PairIn& in, const Q4* rec, int nmax,
+                           PairSumsV& A) {
+  const f2 z2 = pk(0.f, 0.f), m1 = pk(-1.f, -1.f);
+  const cplx<f2> zero = mk(z2, z2);
+  for (int c = 0; c < 3; ++c) A.s[c] = zero;
+  f2 pim1 = z2, pi = pk(1.f, 1.f), nd = m1;
+  cplx<f2> h2 = in.hm1, h1 = in.h0;
+  const f2 sv = in.sv, ikr = in.ikr;
+#pragma unroll 2
+  for (int n = 1; n <= nmax; ++n) {
+    const Q4* r = rec + PAIRV_QUADS * n;
+    f2 v[PAIRV_VALUES];
+#pragma unroll
+    for (int j = 0; j < PAIRV_QUADS; ++j) {
+      const Q4 q = r[j];
+      v[2 * j] = pk(q.x, q.y);
+      v[2 * j + 1] = pk(q.z, q.w);
+    }
+    const f2 fn = v[0], cn = v[1], tns = v[2], fns = v[3];
+    const f2 spi = pmul(sv, pi);
+    const f2 w = padd(nd, spi);
+    const f2 tau = pfma(fn, w, pim1);
+    const f2 ndn = pfma(cn, w, spi);
+    const f2 a2 = pmul(tns, ikr), a1 = pmul(fns, ikr);
+    const cplx<f2> h = mk(pfma(a2, h1.re, h2.re), pfma(a2, h1.im, h2.im));
+    const cplx<f2> dh = mk(pfma(a1, h.re, h1.re), pfma(a1, h.im, h1.im));
+    const cplx<f2> X = pcmul(v[4], v[5], v[6], dh);
+    const cplx<f2> Y = pcmul(v[7], v[8], v[9], h);
+    const cplx<f2> Z = pcmul(v[10], v[11], v[12], h);
+    A.s[0] = pacc(A.s[0], pi, Z);
+    A.s[1] = pacc(pacc(A.s[1], tau, X), pi, Y);
+    A.s[2] = pacc(pacc(A.s[2], pi, X), tau, Y);
+    pim1 = pi;
+    pi = pfma(m1, ndn, pi);
+    nd = ndn;
+    h2 = h1;
+    h1 = h;
+  }
+}
+
+// One lane of the value sums, with order_sum's parity unfolding.
+LMB_HD Sums<float> pair_lane_value(const PairSumsV& P, int lane, float sg) {
+  Sums<float> S;
+  cplx<float> t[3];
+  for (int c = 0; c < 3; ++c)
+    t[c] = lane ? mk(P.s[c].re.y, P.s[c].im.y) : mk(P.s[c].re.x, P.s[c].im.x);
+  S.s0 = t[0];
+  S.s1 = t[1];
+  S.s2 = sg * t[2];
+  return S;
+}
+
 // One lane of the packed sums as the scalar loop's JacSums, with the same
 // parity unfolding and s -> mu conversion at the end of order_sum_jac.
 LMB_HD JacSums<float> pair_lane(const PairSums& P, int lane, float sg) {

@@ -80,4 +80,43 @@ LMB_HD void pair_record(const zd* ab, const zd* dab, int n, float* v) {
   }
 }
 
+// Part `part` (0, 1, 2) of the PAIRV_VALUES values of order n for
+// order_sum_pair (value only; the first 13 values of pair_record): part 0
+// writes v[0..6] (n, c_n, the signed recurrence factors and sig alpha),
+// part 1 v[7..9] (-s beta), part 2 v[10..13] (s n(n+1) alpha, and the
+// unused v[13] = 0).  The parts let a block stage an order on 3 threads.
+LMB_HD void pair_value_part(const zd* ab, int n, int part, float* v) {
+  const int lo = part == 0 ? 0 : (part == 1 ? 7 : 10);
+  const int hi = part == 0 ? 7 : (part == 1 ? 10 : PAIRV_VALUES);
+  for (int j = lo; j < hi; ++j) v[j] = 0.f;
+  if (n == 0) return;
+  const double fn = double(n);
+  const double nn1 = fn * (fn + 1.);
+  const double en = (2. * fn + 1.) / nn1;
+  const double s = ((n & 3) == 1 || (n & 3) == 2) ? -1. : 1.;
+  const double odd = (n & 1) ? 1. : -1.;  // (-1)^{n+1}
+  const double sig = odd * s;
+  zd c;
+  if (part == 0) {
+    v[0] = float(fn);
+    v[1] = float(1. + 1. / fn);
+    v[2] = float(-odd * (2. * fn - 1.));
+    v[3] = float(odd * fn);
+    c = sig * (en * rot_i(ab[0], n + 1));
+  } else if (part == 1) {
+    c = (-s) * (en * rot_i(ab[1], n));
+  } else {
+    c = (s * nn1) * (en * rot_i(ab[0], n + 1));
+  }
+  const int k = 4 + 3 * part;
+  v[k] = float(c.re);
+  v[k + 1] = float(c.im);
+  v[k + 2] = -float(c.im);
+}
+
+// All PAIRV_VALUES values of order n.
+LMB_HD void pair_value_record(const zd* ab, int n, float* v) {
+  for (int part = 0; part < 3; ++part) pair_value_part(ab, n, part, v);
+}
+
 }  // namespace lmb

@@ -130,22 +130,37 @@ class LorenzMie(LMObject):
         flat = [p for plist in particle_lists for p in plist]
         inst = self.instrument
         counts = [len(pl) for pl in particle_lists]
-        item_start = torch.tensor(np.concatenate([[0], np.cumsum(counts)]),
-                                  dtype=torch.int32, device=self.device)
+        item_start = K.to_device_async(
+            np.concatenate([[0], np.cumsum(counts)]).astype(np.int32),
+            self.device)
         rec = _records(flat)
         if len(flat) == 0:
             cap = 1
+        elif not any(K.is_layered(p) for p in flat):
+            cap = int(K.wiscombe_yang(rec['a_p'], rec['n_p'], rec['k_p'],
+                                      inst.n_m, inst.wavelength).max()) + 2
         else:
             cap = max(K.particle_nmax(p, inst.n_m, inst.wavelength)
                       for p in flat) + 2
-            if cap > K._native.LMB_NMAX_LIMIT:
-                raise ValueError(f'a particle needs {cap - 2} partial-wave '
-                                 f'orders; the limit is '
-                                 f'{K._native.LMB_NMAX_LIMIT}')
+        if cap > K._native.LMB_NMAX_LIMIT:
+            raise ValueError(f'a particle needs {cap - 2} partial-wave '
+                             f'orders; the limit is '
+                             f'{K._native.LMB_NMAX_LIMIT}')
         sp = K.spheres_tensor(rec, self.device)
         if len(flat):
+            # The capacity comes from the particles themselves, so the
+            # coefficient kernel can fail only on invalid parameters:
+            # checked here on the host, which spares homogeneous spheres
+            # a device round trip before the field launch.
+            plain = not any(K.is_layered(p) for p in flat)
+            if plain:
+                v = rec.view(np.float64).reshape(-1, 6)
+                if not (np.isfinite(v).all() and (rec['a_p'] > 0.).all()):
+                    raise ValueError('particle parameters must be finite '
+                                     'with a_p > 0')
             ab, dab, nmax = K.particle_ab(flat, sp, inst.n_m,
-                                          inst.wavelength, cap, deriv)
+                                          inst.wavelength, cap, deriv,
+                                          check=not plain)
         else:
             ab = torch.zeros((1, 2, 2, 2), dtype=torch.float64,
                              device=self.device)

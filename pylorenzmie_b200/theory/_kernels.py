@@ -34,10 +34,20 @@ def nmax_cap_for(a_p, n_p, k_p, n_m, wavelength, margin=2):
     return max(cap, 1)
 
 
+def to_device_async(array, device):
+    '''Device copy of a small host array through pinned memory, queued on
+    the current stream without waiting for the work already queued there
+    (a pageable copy would wait for it).'''
+    host = torch.from_numpy(np.ascontiguousarray(array).copy())
+    if torch.cuda.is_available():
+        host = host.pin_memory()
+    return host.to(device, non_blocking=True)
+
+
 def spheres_tensor(records, device):
     '''(n, 6) float64 device tensor from a SPHERE_DTYPE array.'''
     a = np.ascontiguousarray(records).view(np.float64).reshape(-1, 6)
-    return torch.from_numpy(a.copy()).to(device, non_blocking=False)
+    return to_device_async(a, device)
 
 
 def sphere_ab(spheres, n_m, wavelength, cap, deriv=False, check=True):
@@ -257,14 +267,17 @@ def particle_nmax(p, n_m, wavelength):
                              wavelength))
 
 
-def particle_ab(particles, spheres, n_m, wavelength, cap, deriv=False):
+def particle_ab(particles, spheres, n_m, wavelength, cap, deriv=False,
+                check=True):
     '''Coefficients for a list of Sphere / LayeredSphere particles (in
-    order); spheres is their (n, 6) device tensor.'''
+    order); spheres is their (n, 6) device tensor.  ``check=False`` skips
+    the status read-back (a device round trip) for homogeneous spheres
+    whose parameters the caller has validated.'''
     dev = spheres.device
     n = len(particles)
     layered = [i for i, p in enumerate(particles) if is_layered(p)]
     if not layered:
-        return sphere_ab(spheres, n_m, wavelength, cap, deriv)
+        return sphere_ab(spheres, n_m, wavelength, cap, deriv, check=check)
     ab = torch.zeros((n, cap + 1, 2, 2), dtype=torch.float64, device=dev)
     dab = (torch.zeros((n, cap + 1, 4, 2), dtype=torch.float64, device=dev)
            if deriv else None)

@@ -160,6 +160,42 @@ API void h_field(const double* coords, long long npts, const double* p,
     field_one<float>(coords, npts, p, ab, nmax, k, flags, out);
 }
 
+// Field of one sphere through the packed two-pixel value loop (pixels i and
+// i + 1 share one pass; an odd last pixel is paired with itself), FP32.
+API void h_field_pair(const double* coords, long long npts, const double* p,
+                  const double* ab, int nmax, double k, int flags,
+                  double* out) {
+  std::vector<Quad<float>> q(PAIRV_QUADS * (nmax + 1));
+  for (int n = 0; n <= nmax; ++n) {
+    zd a[2];
+    for (int j = 0; j < 2; ++j) a[j] = mk(ab[4 * n + 2 * j], ab[4 * n + 2 * j + 1]);
+    float v[PAIRV_VALUES];
+    pair_value_record(a, n, v);
+    for (int j = 0; j < PAIRV_QUADS; ++j)
+      q[PAIRV_QUADS * n + j] = Quad<float>{v[2 * j], v[2 * j], v[2 * j + 1], v[2 * j + 1]};
+  }
+  for (long long i = 0; i < npts; i += 2) {
+    const long long i1 = i + 1 < npts ? i + 1 : i;
+    Geometry<float> g[2];
+    for (int l = 0; l < 2; ++l) {
+      const long long ii = l ? i1 : i;
+      const double x = coords[ii], y = coords[npts + ii], z = coords[2 * npts + ii];
+      g[l] = geometry<float>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
+    }
+    PairSumsV S;
+    order_sum_pair(pair_in(g[0], g[1]), q.data(), nmax, S);
+    for (int l = 0; l < 2; ++l) {
+      const long long ii = l ? i1 : i;
+      cplx<float> e[3];
+      epilogue<float>(g[l], pair_lane_value(S, l, g[l].smu), flags & 1, e);
+      for (int c = 0; c < 3; ++c) {
+        out[2 * (c * npts + ii)] = e[c].re;
+        out[2 * (c * npts + ii) + 1] = e[c].im;
+      }
+    }
+  }
+}
+
 // Hologram and Jacobian of one sphere: holo [npts], jac [6][npts].
 template <typename R>
 static void jac_one(const double* coords, long long npts, const double* p,

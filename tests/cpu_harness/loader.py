@@ -44,6 +44,9 @@ def load():
     lib.h_jacobian.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
                                ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                ctypes.c_int, _dp, _dp]
+    lib.h_field_pair.argtypes = [_dp, ctypes.c_longlong, _dp, _dp,
+                                 ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                 _dp]
     lib.h_jacobian_pair.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
                                     ctypes.c_int, ctypes.c_double,
                                     ctypes.c_int, _dp, _dp]
@@ -151,3 +154,16 @@ class Harness:
                                  1 | (2 if bohren else 0), ptr(holo),
                                  ptr(jac))
         return holo, jac
+
+    def field_pair(self, coords, p, ab, k, cartesian=True, bohren=True):
+        '''(3, npts) complex field of one sphere through the packed
+        two-pixel value loop (FP32).'''
+        c = np.ascontiguousarray(coords, dtype=float)
+        npts = c.shape[1]
+        n, a, _ = self._pack_ab(ab)
+        out = np.zeros((3, npts, 2))
+        pv = np.asarray(p, dtype=float)
+        self.lib.h_field_pair(ptr(c), npts, ptr(pv), ptr(a), n, k,
+                              (1 if cartesian else 0) | (2 if bohren else 0),
+                              ptr(out))
+        return out[..., 0] + 1j * out[..., 1]

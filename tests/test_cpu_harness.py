@@ -214,3 +214,23 @@ def test_jacobian_pair_loop(h, shape, p):
               field.hologram(c, [dict(zip(KEYS, pm))], inst)) / (2 * step)
         err = np.abs(J2[j] - fd).max() / np.abs(fd).max()
         assert err < 3e-4, (KEYS[j], err)
+
+
+@pytest.mark.parametrize('name', ['torch64', 'cupy128', 'pair96', 'absorb48',
+                                  'below40', 'sph_nb32', 'sph_b32',
+                                  'cart_nb32', 'big64'])
+def test_pixel_sums_pair_loop(h, golden_holo, name):
+    '''The packed two-pixel value loop (the FP32 field/hologram kernel)
+    against the reference's own fields and holograms.'''
+    shape = tuple(golden_holo[name + '_shape'])
+    cart, bohren = (bool(v) for v in golden_holo[name + '_flags'])
+    c = field.coordinates3(field.meshgrid(shape))
+    E = np.zeros((3, c.shape[1]), complex)
+    for p in golden_holo[name + '_particles']:
+        ab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447)
+        E += h.field_pair(c, p[:3], ab, K, cart, bohren)
+    holo = np.sum(np.abs(E + np.array([[1], [0], [0]])) ** 2, axis=0)
+    ref = golden_holo[name + '_holo']
+    assert np.all(np.abs(holo - ref) <= 2e-5 + 2e-6 * np.abs(ref))
+    if name + '_field' in golden_holo:
+        assert np.abs(E - golden_holo[name + '_field']).max() <= 2e-5

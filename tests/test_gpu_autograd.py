@@ -73,11 +73,13 @@ def test_vjp_equals_jacobian_transpose_at_large_sizes():
     jtg = torch.einsum('bjp,bp->bj', J, g.double()).cpu().numpy()
     scale = torch.einsum('bjp,bp->bj', J.abs(), g.double().abs()).cpu().numpy()
     assert np.all(np.abs(vjp - jtg) <= 1e-5 * scale)
-    # forward values equal the hologram kernel's (both FP32 sums, with
-    # different operation orders): within 2e-5 + 2e-6 H
+    # forward values equal the hologram kernel's: both FP32 sums (the
+    # hologram kernel's packed two-pixel loop, the Jacobian kernel's scalar
+    # loop), each within 7.7e-6 max(1, H) of the FP64 kernel on these
+    # spheres (measured), so within twice that of each other
     hf = h.detach().double().cpu().numpy()
     Hj = H.cpu().numpy()
-    assert np.all(np.abs(hf - Hj) <= 2e-5 + 2e-6 * np.abs(Hj))
+    assert np.all(np.abs(hf - Hj) <= 2e-5 + 1.5e-5 * np.abs(Hj))
 
 
 @pytest.mark.parametrize('p', [[50.3, 49.6, 300., 4.0, 1.7, 0.0],
