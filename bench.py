@@ -503,7 +503,8 @@ def run_extras(dev, inst, chosen_value):
             inst.wavelength).mean())}
     del H, J
 
-    # layered spheres in a stream: 8 frames x 32 features per call
+    # layered spheres from a video stream: frames of 32 features each,
+    # 8 frames per device batch, batches pipelined by optimize_stream
     sides, truth, start, frac, core = workloads.layered(256, seed=13)
     parts = workloads.layered_spheres(truth, frac, core)
     imgs = workloads.render_particles(parts, [(s, s) for s in sides],
@@ -512,27 +513,39 @@ def run_extras(dev, inst, chosen_value):
     starts = workloads.layered_spheres(start, frac, core)
     opt = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1)),
                                     instrument=inst, device=dev))
-    opt.optimize_batch(holos, particles=starts)
+    for _ in opt.optimize_stream(iter([(holos, starts)])):
+        pass
     torch.cuda.synchronize()
+    nbatch = 4
     t0 = time.perf_counter()
-    reps = 4
-    for _ in range(reps):
-        df = opt.optimize_batch(holos, particles=starts)
+    dfs = list(opt.optimize_stream(iter([(holos, starts)] * nbatch)))
     torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    df = dfs[0]
     err = np.abs(df['a_p'].to_numpy() - truth[:, 3])
+    sub = list(range(0, 256, 32))          # one feature per frame
+    ref = oracle_fits([(imgs[i], (sides[i], sides[i]), start[i], frac[i],
+                        core[i]) for i in sub])
     out['layered_stream_e2e'] = {
-        'value': 256 * reps / (time.perf_counter() - t0), 'unit': UNIT,
-        'features_per_call': 256, 'layers': 3,
+        'value': 256 * nbatch / dt, 'unit': UNIT,
+        'frames_per_s': 8 * nbatch / dt,
+        'api': 'Optimizer.optimize_stream, 8 frames x 32 features per batch',
+        'features': 256 * nbatch, 'layers': 3,
         'success_fraction': float(df['success'].mean()),
-        'median_abs_a_p_error_vs_truth_um': float(np.median(err))}
+        'mean_nfev': float(df['nfev'].mean()),
+        'max_nfev': int(df['nfev'].max()),
+        'median_abs_a_p_error_vs_truth_um': float(np.median(err)),
+        'vs_oracle_fit': compare_fits(df.iloc[sub].reset_index(drop=True),
+                                      ref)}
 
     # mixed crop sizes 51..301, 256 features per launch
     sides, truth, start = workloads.mixed_crops(256, seed=9)
-    holos = []
+    holos, raw = [], []
     for i in range(256):
         s = int(sides[i])
         d = workloads.render(truth[i:i + 1], (s, s), seed=i, device=dev)[0]
-        holos.append(Hologram(d.cpu().numpy().astype(np.float64)))
+        raw.append(d.cpu().numpy().astype(np.float64))
+        holos.append(Hologram(raw[-1]))
     opt = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1)),
                                     instrument=inst, device=dev))
     opt.optimize_batch(holos, starts=start)
@@ -542,10 +555,46 @@ def run_extras(dev, inst, chosen_value):
     for _ in range(reps):
         df = opt.optimize_batch(holos, starts=start)
     torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    sub = list(range(0, 256, 16))
+    ref = oracle_fits([(raw[i], (sides[i], sides[i]), start[i], None, None)
+                       for i in sub])
     out['mixed_crops_e2e'] = {
-        'value': 256 * reps / (time.perf_counter() - t0), 'unit': UNIT,
+        'value': 256 * reps / dt, 'unit': UNIT,
         'success_fraction': float(df['success'].mean()),
-        'mean_pixels': float(np.mean(sides.astype(float) ** 2))}
+        'mean_pixels': float(np.mean(sides.astype(float) ** 2)),
+        'vs_oracle_fit': compare_fits(df.iloc[sub].reset_index(drop=True),
+                                      ref)}
+    return out
+
+
+def oracle_fits(tasks):
+    '''The reference fitting algorithm (oracle) on a subset of crops,
+    over a spawn pool of the host cores: tasks of (data, shape, start,
+    fractions or None, core indices or None).'''
+    import multiprocessing as mp
+    from oracle import bench_tasks
+    for var in ('OMP_NUM_THREADS', 'MKL_NUM_THREADS', 'OPENBLAS_NUM_THREADS'):
+        os.environ[var] = '1'
+    with mp.get_context('spawn').Pool(min(len(tasks), os.cpu_count() or 1)
+                                      ) as pool:
+        return pool.starmap(bench_tasks.fit_crop, tasks)
+
+
+def compare_fits(df, ref):
+    '''Largest |device - oracle| per fitted parameter over a subset, in
+    its units and in units of the oracle's uncertainty.'''
+    import numpy as np
+    out = {'features': len(ref),
+           'oracle_success': float(np.mean([r['success'] for r in ref])),
+           'max_redchi_rel_diff': float(np.max(np.abs(
+               df['redchi'].to_numpy() / np.array([r['redchi'] for r in ref])
+               - 1.)))}
+    for k in ('x_p', 'y_p', 'z_p', 'a_p', 'n_p'):
+        d = np.abs(df[k].to_numpy() - np.array([r[k] for r in ref]))
+        sig = np.array([r['d' + k] for r in ref])
+        out[k] = {'max_abs': float(d.max()),
+                  'max_in_sigma': float((d / np.maximum(sig, 1e-300)).max())}
     return out
 
 

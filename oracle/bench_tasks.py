@@ -24,3 +24,14 @@ def render_201(truth, seed):
 def fit_201(data, start):
     return fit(data, meshgrid((201, 201)), dict(zip(KEYS, start)),
                DEFAULT_INSTRUMENT)
+
+
+def fit_crop(data, shape, start, fractions=None, core_indices=None):
+    '''The reference fitting algorithm on one crop of any shape; a layered
+    sphere keeps its inner radius fractions and indices.'''
+    particle = dict(zip(KEYS, start))
+    if fractions is not None:
+        particle['fractions'] = list(fractions)
+        particle['core_indices'] = list(core_indices)
+    return fit(np.asarray(data).ravel(), meshgrid(tuple(shape)), particle,
+               DEFAULT_INSTRUMENT)

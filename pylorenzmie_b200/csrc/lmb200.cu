@@ -70,8 +70,8 @@ constexpr int kNumEvalShapes = int(sizeof(kEvalShapes) / sizeof(kEvalShapes[0]))
 constexpr int kScalarShape = 1;  // scalar loop, used when pair records do not fit
 
 struct FitLayout {
-  size_t state, ev, base, ab, dab, coef32, nmax, tile_begin, tiles, partial,
-      counters, total;
+  size_t state, ev, base, ab, dab, coef32, nmax, tile_begin, tiles,
+      active_tiles, partial, counters, total;
   int max_tiles;
 };
 
@@ -98,6 +98,7 @@ FitLayout fit_layout(int nf, long long total_pixels, int nmax_cap) {
   L.nmax = take(sizeof(int) * nf);
   L.tile_begin = take(sizeof(int) * (nf + 1));
   L.tiles = take(sizeof(int2) * size_t(L.max_tiles));
+  L.active_tiles = take(sizeof(int) * size_t(L.max_tiles));
   L.partial = take(sizeof(double) * FIT_NSUM * size_t(L.max_tiles));
   L.counters = take(sizeof(int) * 16);
   L.total = align_up(off, 256);
@@ -421,6 +422,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   c.nmax = reinterpret_cast<int*>(ws + L.nmax);
   c.tile_begin = reinterpret_cast<int*>(ws + L.tile_begin);
   c.tiles = reinterpret_cast<int2*>(ws + L.tiles);
+  c.active_tiles = reinterpret_cast<int*>(ws + L.active_tiles);
   c.partial = reinterpret_cast<double*>(ws + L.partial);
   c.counters = reinterpret_cast<int*>(ws + L.counters);
   c.work = reinterpret_cast<unsigned long long*>(ws + L.counters + 8 * sizeof(int));
@@ -529,7 +531,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
         std::this_thread::sleep_for(std::chrono::microseconds(20));
       }
       cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
-      cudaMemsetAsync(c.counters + 4, 0, sizeof(int), st);
+      cudaMemsetAsync(c.counters + 4, 0, 2 * sizeof(int), st);  // [4], [5]
       k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
       launches += 1;
       ++iterations;

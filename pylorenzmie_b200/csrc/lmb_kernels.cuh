@@ -638,7 +638,9 @@ struct FitCtx {
   int2* tiles;         // [max_tiles]
   double* partial;     // [max_tiles][FIT_NSUM]
   int* counters;       // [0] tile queue, [1] running, [2] ntiles, [3] overflow,
-                       // [4] waiting for data
+                       // [4] waiting for data, [5] active tiles this round
+  int* active_tiles;   // [max_tiles] tiles of the features evaluated this
+                       // round (filled by k_fit_step, in no fixed order)
   unsigned long long* work;  // [0] pixels, [1] pixel-orders evaluated
   long long total_pixels;
   int nf, nmax_cap, max_tiles, tile_pixels;
@@ -695,6 +697,7 @@ __global__ void k_fit_setup(FitCtx c) {
     c.counters[0] = 0;
     c.counters[1] = 0;
     c.counters[4] = 0;
+    c.counters[5] = 0;
     c.work[0] = 0ull;
     c.work[1] = 0ull;
   }
@@ -741,7 +744,7 @@ k_fit_eval(FitCtx c) {
   Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem);
   __shared__ float red[(TPB / 32) * FIT_NSUM];
   __shared__ int s_tile;
-  const int ntiles = c.counters[2];
+  const int ntiles = c.counters[5];  // tiles of active features
   const int nmaxp = c.nmax_cap + 1;
   const bool bohren = c.flags & LMB_BOHREN;
   const float kf = float(c.k);
@@ -749,8 +752,9 @@ k_fit_eval(FitCtx c) {
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(c.counters, 1);
     __syncthreads();
-    const int t = s_tile;
-    if (t >= ntiles) break;
+    const int q = s_tile;
+    if (q >= ntiles) break;
+    const int t = c.active_tiles[q];  // global tile index: fixes partial[]
     const int2 tile = c.tiles[t];
     const int f = tile.x;
     if (!c.ev[f].active) {
@@ -875,7 +879,7 @@ k_fit_eval_pair(FitCtx c) {
   float4* rec = reinterpret_cast<float4*>(smem);
   __shared__ float red[(TPB / 32) * FIT_NSUM];
   __shared__ int s_tile;
-  const int ntiles = c.counters[2];
+  const int ntiles = c.counters[5];  // tiles of active features
   const int nmaxp = c.nmax_cap + 1;
   const bool bohren = c.flags & LMB_BOHREN;
   const float kf = float(c.k);
@@ -883,8 +887,9 @@ k_fit_eval_pair(FitCtx c) {
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(c.counters, 1);
     __syncthreads();
-    const int t = s_tile;
-    if (t >= ntiles) break;
+    const int q = s_tile;
+    if (q >= ntiles) break;
+    const int t = c.active_tiles[q];  // global tile index: fixes partial[]
     const int2 tile = c.tiles[t];
     const int f = tile.x;
     if (!c.ev[f].active) {
@@ -962,17 +967,18 @@ k_fit_eval_warp(FitCtx c) {
   const int nmaxp = c.nmax_cap + 1;
   Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem) +
                       size_t(warp) * JAC_QUADS * nmaxp;
-  const int ntiles = c.counters[2];
+  const int ntiles = c.counters[5];  // tiles of active features
   const bool bohren = c.flags & LMB_BOHREN;
   const float kf = float(c.k);
   const float inv_noise = float(c.inv_noise);
   constexpr int PPL = 16;  // pixels per lane: 32 x 16 = 512 = one tile
   int cur = -1, nm = 0;
   for (;;) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(c.counters, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= ntiles) break;
+    int q = 0;
+    if (lane == 0) q = atomicAdd(c.counters, 1);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= ntiles) break;
+    const int t = c.active_tiles[q];
     const int2 tile = c.tiles[t];
     const int f = tile.x;
     if (!c.ev[f].active) continue;
@@ -1144,6 +1150,8 @@ k_fit_step(FitCtx c) {
     else
       stage_coef<float, true>(abf, dabf, nm, c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
   }
+  int base = -1;
+  const int tb = c.tile_begin[f], nt = c.tile_begin[f + 1] - tb;
   if (lane == 0) {
     if (st != LMB_OK) {
       gs->phase = LM_PHASE_DONE;
@@ -1154,8 +1162,12 @@ k_fit_step(FitCtx c) {
       for (int j = 0; j < 6; ++j) c.ev[f].p[j] = s_p[j];
       c.ev[f].active = 1;
       atomicAdd(c.counters + 1, 1);
+      base = atomicAdd(c.counters + 5, nt);  // this feature's tiles join
     }
   }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (base >= 0)
+    for (int j = lane; j < nt; j += 32) c.active_tiles[base + j] = tb + j;
 }
 
 // Results: fitted parameters, uncertainties, redchi; one thread per feature.
