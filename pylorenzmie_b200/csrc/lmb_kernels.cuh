@@ -506,14 +506,7 @@ __device__ inline void holo_jac_pixel(const Geometry<float>& g,
                                       const Quad<float>* coef, int nm, float kf,
                                       float* H, float* dH) {
   const JacSums<float> A = order_sum_jac<float>(g, coef, nm);
-  cplx<float> e[3], de[6][3];
-  epilogue_jac<float>(g, A, kf, e, de);
-  *H = intensity<float>(e);
-  const cplx<float> et0 = mk(e[0].re + 1.f, e[0].im);
-  for (int j = 0; j < 6; ++j)
-    dH[j] = 2.f * (et0.re * de[j][0].re + et0.im * de[j][0].im +
-                   e[1].re * de[j][1].re + e[1].im * de[j][1].im +
-                   e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+  holo_jac_reverse<float>(g, A, kf, H, dH);
 }
 
 __global__ void __launch_bounds__(128)
@@ -844,14 +837,7 @@ __device__ inline void holo_jac_pair(double k, const double* dx,
   for (int lane = 0; lane < 2; ++lane) {
     const Geometry<float>& gl = g[lane];
     const JacSums<float> A = pair_lane(P, lane, gl.smu);
-    cplx<float> e[3], de[6][3];
-    epilogue_jac<float>(gl, A, kf, e, de);
-    H[lane] = intensity<float>(e);
-    const cplx<float> et0 = mk(e[0].re + 1.f, e[0].im);
-    for (int j = 0; j < 6; ++j)
-      dH[lane][j] = 2.f * (et0.re * de[j][0].re + et0.im * de[j][0].im +
-                           e[1].re * de[j][1].re + e[1].im * de[j][1].im +
-                           e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+    holo_jac_reverse<float>(gl, A, kf, &H[lane], dH[lane]);
   }
 }
 

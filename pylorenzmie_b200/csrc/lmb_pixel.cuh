@@ -693,6 +693,103 @@ LMB_HD void epilogue_jac(const Geometry<R>& g, const JacSums<R>& A, R k,
   }
 }
 
+// Hologram and its six parameter derivatives in reverse mode: the same
+// quantities as epilogue_jac followed by dH_j = 2 Re(conj(E + x) dE_j), at a
+// third of the arithmetic.  Forward: E_c = phase * sum_k q_ck G_k S_k with
+// the geometric factors G = (cos(phi) sin(theta)/kr^2, cos(phi)/kr,
+// sin(phi)/kr) and the Cartesian projection q_ck(theta, phi).  Reverse:
+// from Ebar = 2 (E + x) the adjoints of the projected sums, of the sums
+// S_k (which carry the a_p, n_p, k_p columns, since the material sums enter
+// where S_k does) and of the real geometric variables, which the chain rule
+// then maps onto (kx, ky, kz).  The phase's kz rate and the on-axis branch
+// are those of epilogue_jac.  For a complex z, zbar = dH/dRe z + i dH/dIm z.
+template <typename R>
+LMB_HD void holo_jac_reverse(const Geometry<R>& g, const JacSums<R>& A, R k,
+                             R* H, R* dH) {
+  const R ikr = g.ikr, mu = g.mu, st = g.sint, cp = g.cosp, sp = g.sinp;
+  const R ikr2 = ikr * ikr;
+  // forward
+  const R G[3] = {cp * st * ikr2, cp * ikr, sp * ikr};
+  cplx<R> es[3];
+  for (int j = 0; j < 3; ++j) es[j] = G[j] * A.s[j];
+  const R q00 = st * cp, q01 = mu * cp, q10 = st * sp, q11 = mu * sp;
+  cplx<R> c[3];
+  c[0] = q00 * es[0] + q01 * es[1] - sp * es[2];
+  c[1] = q10 * es[0] + q11 * es[1] + cp * es[2];
+  c[2] = mu * es[0] - st * es[1];
+  cplx<R> et[3];
+  for (int j = 0; j < 3; ++j) et[j] = g.phase * c[j];
+  et[0].re += R(1);
+  *H = norm2(et[0]) + norm2(et[1]) + norm2(et[2]);
+  // reverse: E = phase c
+  cplx<R> cb[3], phb = mk(R(0), R(0));
+  const cplx<R> cph = conj(g.phase);
+  for (int j = 0; j < 3; ++j) {
+    const cplx<R> eb = R(2) * et[j];
+    cb[j] = cph * eb;
+    phb = phb + eb * conj(c[j]);
+  }
+  const cplx<R> zp = conj(phb) * g.phase;
+  const R thb = -zp.im;  // d/dtheta of phase = i phase
+  // c = q es
+  cplx<R> esb[3];
+  esb[0] = q00 * cb[0] + q10 * cb[1] + mu * cb[2];
+  esb[1] = q01 * cb[0] + q11 * cb[1] - st * cb[2];
+  esb[2] = cp * cb[1] - sp * cb[0];
+  auto re_dot = [](cplx<R> a, cplx<R> b) { return a.re * b.re + a.im * b.im; };
+  const R q00b = re_dot(cb[0], es[0]), q01b = re_dot(cb[0], es[1]);
+  const R q02b = re_dot(cb[0], es[2]);  // coefficient -sp
+  const R q10b = re_dot(cb[1], es[0]), q11b = re_dot(cb[1], es[1]);
+  const R q12b = re_dot(cb[1], es[2]);  // coefficient cp
+  const R q20b = re_dot(cb[2], es[0]), q21b = re_dot(cb[2], es[1]);  // mu, -st
+  // es = G S
+  cplx<R> sb[3];
+  R Gb[3];
+  for (int j = 0; j < 3; ++j) {
+    sb[j] = G[j] * esb[j];
+    Gb[j] = re_dot(esb[j], A.s[j]);
+  }
+  R krb = 0, mub = 0, da = 0, dn = 0, dk = 0;
+  for (int j = 0; j < 3; ++j) {
+    krb += re_dot(sb[j], A.t[j]);
+    mub += re_dot(sb[j], A.u[j]);
+    da += re_dot(sb[j], A.a[j]);
+    dn += re_dot(sb[j], A.p[j]);
+    dk += sb[j].im * A.p[j].re - sb[j].re * A.p[j].im;  // Re(conj(sb) i p)
+  }
+  // real geometric variables
+  R stb = q00b * cp + q10b * sp - q21b + Gb[0] * cp * ikr2;
+  R cpb = q00b * st + q01b * mu + q12b + Gb[0] * st * ikr2 + Gb[1] * ikr;
+  R spb = q10b * st + q11b * mu - q02b + Gb[2] * ikr;
+  mub += q01b * cp + q11b * sp + q20b;
+  const R ikrb = Gb[0] * R(2) * cp * st * ikr + Gb[1] * cp + Gb[2] * sp;
+  // chain to (kx, ky, kz)
+  const R krg[3] = {st * cp, st * sp, mu};
+  const R dmu[3] = {-mu * krg[0] * ikr, -mu * krg[1] * ikr, st * st * ikr};
+  const R dst[3] = {cp * mu * mu * ikr, sp * mu * mu * ikr, -st * mu * ikr};
+  R dcp[3] = {R(0), R(0), R(0)}, dsp[3] = {R(0), R(0), R(0)};
+  if (g.krho > R(0)) {
+    const R ik = R(1) / g.krho;
+    dcp[0] = sp * sp * ik;
+    dcp[1] = -cp * sp * ik;
+    dsp[0] = -cp * sp * ik;
+    dsp[1] = cp * cp * ik;
+  }
+  const R rate = (g.sigma != R(0) && g.sigma == g.smu) ? -g.s1mu
+                                                       : g.sigma * mu - R(1);
+  const R dth[3] = {g.sigma * krg[0], g.sigma * krg[1], rate};
+  R dk3[3];
+  for (int i = 0; i < 3; ++i)
+    dk3[i] = (krb - ikrb * ikr2) * krg[i] + mub * dmu[i] + stb * dst[i] +
+             cpb * dcp[i] + spb * dsp[i] + thb * dth[i];
+  dH[0] = (-k) * dk3[0];
+  dH[1] = (-k) * dk3[1];
+  dH[2] = k * dk3[2];
+  dH[3] = da;
+  dH[4] = dn;
+  dH[5] = dk;
+}
+
 // Hologram from the total scattered field: |E + x|^2 = |E|^2 + 2 Re(E_x) + 1
 template <typename R>
 LMB_HD R intensity(const cplx<R>* e) {

@@ -248,16 +248,40 @@ API void h_jacobian_pair(const double* coords, long long npts, const double* p,
     for (int l = 0; l < 2; ++l) {
       const long long ii = l ? i1 : i;
       const JacSums<float> A = pair_lane(P, l, g[l].smu);
-      cplx<float> e[3], de[6][3];
-      epilogue_jac<float>(g[l], A, float(k), e, de);
-      holo[ii] = intensity<float>(e);
-      const cplx<float> et0 = mk(e[0].re + 1.f, e[0].im);
-      for (int j = 0; j < 6; ++j)
-        jac[j * npts + ii] = 2.f * (et0.re * de[j][0].re + et0.im * de[j][0].im +
-                                    e[1].re * de[j][1].re + e[1].im * de[j][1].im +
-                                    e[2].re * de[j][2].re + e[2].im * de[j][2].im);
+      float H, dH[6];
+      holo_jac_reverse<float>(g[l], A, float(k), &H, dH);
+      holo[ii] = H;
+      for (int j = 0; j < 6; ++j) jac[j * npts + ii] = dH[j];
     }
   }
+}
+
+// Hologram and Jacobian of one sphere with the reverse-mode epilogue
+// (holo_jac_reverse) after the scalar order loop.
+template <typename R>
+static void jac_rev_one(const double* coords, long long npts, const double* p,
+                        const double* ab, const double* dab, int nmax, double k,
+                        int flags, double* holo, double* jac) {
+  std::vector<Quad<R>> q(JAC_QUADS * (nmax + 1));
+  stage<R>(ab, dab, nmax, q.data(), JAC_QUADS);
+  for (long long i = 0; i < npts; ++i) {
+    const double x = coords[i], y = coords[npts + i], z = coords[2 * npts + i];
+    Geometry<R> g = geometry<R>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
+    JacSums<R> A = order_sum_jac<R>(g, q.data(), nmax);
+    R H, dH[6];
+    holo_jac_reverse<R>(g, A, R(k), &H, dH);
+    holo[i] = H;
+    for (int j = 0; j < 6; ++j) jac[j * npts + i] = dH[j];
+  }
+}
+
+API void h_jacobian_rev(const double* coords, long long npts, const double* p,
+                    const double* ab, const double* dab, int nmax, double k,
+                    int flags, int fp64, double* holo, double* jac) {
+  if (fp64)
+    jac_rev_one<double>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac);
+  else
+    jac_rev_one<float>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac);
 }
 
 // Levenberg-Marquardt state machine driven from Python.

@@ -234,3 +234,27 @@ def test_pixel_sums_pair_loop(h, golden_holo, name):
     assert np.all(np.abs(holo - ref) <= 2e-5 + 2e-6 * np.abs(ref))
     if name + '_field' in golden_holo:
         assert np.abs(E - golden_holo[name + '_field']).max() <= 2e-5
+
+
+@pytest.mark.parametrize('shape,p', [
+    ((48, 48), [20.3, 25.7, 120., 0.9, 1.6, 0.01]),
+    ((40, 40), [20., 20., -130., 0.6, 1.5, 0.]),
+    ((33, 33), [16., 16., 80., 1.0, 1.4, 0.]),
+    ((21, 31), [15.2, 10.1, 60., 2.5, 1.7, 0.002]),
+])
+@pytest.mark.parametrize('bohren', [True, False])
+def test_reverse_epilogue_matches_forward(h, shape, p, bohren):
+    '''The reverse-mode epilogue gives the forward-mode (dual-number)
+    epilogue's hologram and Jacobian: to FP64 rounding in FP64, to FP32
+    rounding in FP32 (on-axis pixels included: the grids contain x_p, y_p
+    in the first three cases).'''
+    c = field.coordinates3(field.meshgrid(shape))
+    ab, dab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447, deriv=True)
+    for fp64, rtol in ((1, 1e-10), (0, 2e-5)):
+        H1, J1 = h.jacobian(c, p[:3], ab, dab, K, bohren, fp64)
+        H2, J2 = h.jacobian_rev(c, p[:3], ab, dab, K, bohren, fp64)
+        assert np.all(np.abs(H2 - H1) <= rtol * (1 + np.abs(H1)))
+        for j in range(6):
+            scale = np.abs(J1[j]).max() + 1e-30
+            assert np.abs(J2[j] - J1[j]).max() <= 10 * rtol * scale, \
+                (KEYS[j], fp64, np.abs(J2[j] - J1[j]).max() / scale)
