@@ -68,6 +68,9 @@ const EvalShape kEvalShapes[] = {
 };
 constexpr int kNumEvalShapes = int(sizeof(kEvalShapes) / sizeof(kEvalShapes[0]));
 constexpr int kScalarShape = 1;  // scalar loop, used when pair records do not fit
+// pair records take 256 B per order: above this they no longer fit in
+// shared memory beside the kernels' own buffers, and the scalar loop runs
+constexpr size_t kPairSmemLimit = size_t(200) * 1024;
 
 struct FitLayout {
   size_t state, ev, base, ab, dab, coef32, nmax, tile_begin, tiles,
@@ -316,6 +319,16 @@ int lmb_jacobian(const double* coords, long long npts,
   if (!(flags & LMB_CARTESIAN) || (flags & LMB_FP64)) return LMB_ERR_UNSUPPORTED;
   if (nitems > 65535) return LMB_ERR_ARG;
   const int tpb = 128;
+  const size_t psmem = sizeof(float4) * PAIR_QUADS * (size_t(nmax_cap) + 1);
+  if (psmem <= kPairSmemLimit) {  // packed two-pixel loop
+    LMB_CK(smem_attr((const void*)k_jacobian_pair, psmem));
+    dim3 grid(unsigned((npts + 2 * tpb - 1) / (2 * tpb)), unsigned(nitems));
+    k_jacobian_pair<<<grid, tpb, psmem, as_stream(stream)>>>(
+        coords, npts, spheres, reinterpret_cast<const zd*>(ab),
+        reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, holo, jac);
+    LMB_CK(cudaGetLastError());
+    return LMB_OK;
+  }
   const size_t smem = sizeof(Quad<float>) * JAC_QUADS * (size_t(nmax_cap) + 1);
   LMB_CK(smem_attr((const void*)k_jacobian, smem));
   dim3 grid(unsigned((npts + tpb - 1) / tpb), unsigned(nitems));
@@ -350,13 +363,25 @@ int lmb_hologram_vjp(const double* coords, long long npts,
   if (!workspace || workspace_bytes < lmb_vjp_workspace_bytes(npts, nitems))
     return LMB_ERR_WORKSPACE;
   const int tpb = 128;
-  const int nb = int((npts + tpb - 1) / tpb);
-  const size_t smem = sizeof(Quad<float>) * JAC_QUADS * (size_t(nmax_cap) + 1);
-  LMB_CK(smem_attr((const void*)k_vjp, smem));
   double* partial = reinterpret_cast<double*>(workspace);
-  k_vjp<<<dim3(nb, nitems), tpb, smem, as_stream(stream)>>>(
-      coords, npts, spheres, reinterpret_cast<const zd*>(ab),
-      reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, gout, partial);
+  const size_t psmem = sizeof(float4) * PAIR_QUADS * (size_t(nmax_cap) + 1);
+  int nb;
+  if (psmem <= kPairSmemLimit) {  // packed two-pixel loop: 256 pixels a block
+    nb = int((npts + 2 * tpb - 1) / (2 * tpb));
+    LMB_CK(smem_attr((const void*)k_vjp_pair, psmem));
+    k_vjp_pair<<<dim3(nb, nitems), tpb, psmem, as_stream(stream)>>>(
+        coords, npts, spheres, reinterpret_cast<const zd*>(ab),
+        reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, gout,
+        partial);
+  } else {
+    nb = int((npts + tpb - 1) / tpb);
+    const size_t smem = sizeof(Quad<float>) * JAC_QUADS * (size_t(nmax_cap) + 1);
+    LMB_CK(smem_attr((const void*)k_vjp, smem));
+    k_vjp<<<dim3(nb, nitems), tpb, smem, as_stream(stream)>>>(
+        coords, npts, spheres, reinterpret_cast<const zd*>(ab),
+        reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, gout,
+        partial);
+  }
   LMB_CK(cudaGetLastError());
   const int nt = nitems * 6;
   k_vjp_reduce<<<(nt + 127) / 128, 128, 0, as_stream(stream)>>>(partial, nb, nitems, grad);
@@ -462,7 +487,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   // in shared memory next to the reduction buffer, so such batches use the
   // scalar loop
   if (shape.pair && sizeof(float4) * PAIR_QUADS * (size_t(nmax_cap) + 1) >
-                        size_t(200) * 1024)
+                        kPairSmemLimit)
     shape = kEvalShapes[kScalarShape];
   c.pair_records = shape.pair;
   const size_t coef_smem = (shape.pair ? sizeof(float4) * PAIR_QUADS

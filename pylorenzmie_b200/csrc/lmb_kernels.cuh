@@ -534,6 +534,44 @@ k_jacobian(const double* __restrict__ coords, long long npts,
   for (int j = 0; j < 6; ++j) jo[j * npts + pix] = dH[j];
 }
 
+// k_jacobian with the packed two-pixel loop: each thread takes two adjacent
+// pixels (pair records, stage_pair).
+__global__ void __launch_bounds__(128, 3)
+k_jacobian_pair(const double* __restrict__ coords, long long npts,
+                const lmb_sphere* __restrict__ spheres, const zd* __restrict__ ab,
+                const zd* __restrict__ dab, const int* __restrict__ nmax, int nmaxp,
+                double k, int flags, double* holo, double* jac) {
+  extern __shared__ __align__(16) char smem[];
+  float4* rec = reinterpret_cast<float4*>(smem);
+  const int item = blockIdx.y;
+  const int nm = min(max(nmax[item], 0), nmaxp - 1);
+  stage_pair(ab + size_t(item) * nmaxp * 2, dab + size_t(item) * nmaxp * 4, nm, rec);
+  __syncthreads();
+  const long long p0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+  if (p0 >= npts) return;
+  const bool live1 = p0 + 1 < npts;
+  const long long p1 = live1 ? p0 + 1 : p0;
+  const lmb_sphere sp = spheres[item];
+  const double dx[2] = {coords[p0] - sp.x_p, coords[p1] - sp.x_p};
+  const double dy[2] = {coords[npts + p0] - sp.y_p, coords[npts + p1] - sp.y_p};
+  const double z0 = coords[2 * npts + p0], z1 = coords[2 * npts + p1];
+  Geometry<float> g[2];
+  g[0] = geometry<float>(k, dx[0], dy[0], z0 - sp.z_p, z0, sp.z_p, flags & LMB_BOHREN);
+  g[1] = geometry<float>(k, dx[1], dy[1], z1 - sp.z_p, z1, sp.z_p, flags & LMB_BOHREN);
+  PairSums P;
+  order_sum_jac_pair(pair_in(g[0], g[1]), rec, nm, P);
+  double* jo = jac + (size_t)item * 6 * npts;
+  for (int l = 0; l < 2; ++l) {
+    if (l == 1 && !live1) break;
+    const long long pix = l ? p1 : p0;
+    const JacSums<float> A = pair_lane(P, l, g[l].smu);
+    float H, dH[6];
+    holo_jac_reverse<float>(g[l], A, float(k), &H, dH);
+    if (holo) holo[(size_t)item * npts + pix] = H;
+    for (int j = 0; j < 6; ++j) jo[j * npts + pix] = dH[j];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Block reduction of NV floats held by every thread; result in red[0..NV-1]
 // of thread 0's view (shared).  Fixed order: deterministic.
@@ -586,6 +624,48 @@ k_vjp(const double* __restrict__ coords, long long npts,
     holo_jac_pixel(g, coef, nm, float(k), &H, dH);
     const float go = gout[(size_t)item * npts + pix];
     for (int j = 0; j < 6; ++j) acc[j] = go * dH[j];
+  }
+  block_reduce<6, 128>(acc, red);
+  if (threadIdx.x < 6)
+    partial[((size_t)item * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = red[threadIdx.x];
+}
+
+// k_vjp with the packed two-pixel loop (two adjacent pixels per thread).
+__global__ void __launch_bounds__(128, 3)
+k_vjp_pair(const double* __restrict__ coords, long long npts,
+           const lmb_sphere* __restrict__ spheres, const zd* __restrict__ ab,
+           const zd* __restrict__ dab, const int* __restrict__ nmax, int nmaxp,
+           double k, int flags, const float* __restrict__ gout, double* partial) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ float red[(128 / 32) * 6];
+  float4* rec = reinterpret_cast<float4*>(smem);
+  const int item = blockIdx.y;
+  const int nm = min(max(nmax[item], 0), nmaxp - 1);
+  stage_pair(ab + size_t(item) * nmaxp * 2, dab + size_t(item) * nmaxp * 4, nm, rec);
+  __syncthreads();
+  const long long p0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (p0 < npts) {
+    const bool live1 = p0 + 1 < npts;
+    const long long p1 = live1 ? p0 + 1 : p0;
+    const lmb_sphere sp = spheres[item];
+    const double z0 = coords[2 * npts + p0], z1 = coords[2 * npts + p1];
+    Geometry<float> g[2];
+    g[0] = geometry<float>(k, coords[p0] - sp.x_p, coords[npts + p0] - sp.y_p,
+                           z0 - sp.z_p, z0, sp.z_p, flags & LMB_BOHREN);
+    g[1] = geometry<float>(k, coords[p1] - sp.x_p, coords[npts + p1] - sp.y_p,
+                           z1 - sp.z_p, z1, sp.z_p, flags & LMB_BOHREN);
+    PairSums P;
+    order_sum_jac_pair(pair_in(g[0], g[1]), rec, nm, P);
+    for (int l = 0; l < 2; ++l) {
+      if (l == 1 && !live1) break;
+      const long long pix = l ? p1 : p0;
+      const JacSums<float> A = pair_lane(P, l, g[l].smu);
+      float H, dH[6];
+      holo_jac_reverse<float>(g[l], A, float(k), &H, dH);
+      const float go = gout[(size_t)item * npts + pix];
+      for (int j = 0; j < 6; ++j) acc[j] += go * dH[j];
+    }
   }
   block_reduce<6, 128>(acc, red);
   if (threadIdx.x < 6)
