@@ -212,7 +212,7 @@ int lmb_layered_ab(const double* radii, const double* indices, int nlayers,
   if (nspheres == 0) return LMB_OK;
   if (!radii || !indices || !ab || !nmax || !status) return LMB_ERR_ARG;
   if (!(wavelength > 0.) || !(n_m > 0.)) return LMB_ERR_ARG;
-  const size_t smem = layered_scratch_bytes(nmax_cap + 1);
+  const size_t smem = layered_scratch_bytes(nmax_cap + 1, nlayers);
   LMB_CK(smem_attr((const void*)k_layered_ab, smem));
   k_layered_ab<<<nspheres, 32, smem, as_stream(stream)>>>(
       radii, indices, nlayers, nspheres, n_m, wavelength, nmax_cap,
@@ -478,7 +478,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   c.max_iterations = settings->max_iterations > 0 ? settings->max_iterations : 1;
   if (c.max_iterations > c.set.maxfev) c.max_iterations = c.set.maxfev;
 
-  const size_t ab_smem = nlayers > 1 ? layered_scratch_bytes(nmax_cap + 1)
+  const size_t ab_smem = nlayers > 1 ? layered_scratch_bytes(nmax_cap + 1, nlayers)
                                      : ab_scratch_bytes(nmax_cap + 1);
   const int shape_index = settings->tile_config;
   if (shape_index < 0 || shape_index >= kNumEvalShapes) return LMB_ERR_ARG;

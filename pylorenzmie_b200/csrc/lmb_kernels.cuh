@@ -116,8 +116,26 @@ __global__ void k_sphere_ab(const lmb_sphere* spheres, int n, double n_m,
 // each shell, lane 1 the medium's recurrences meanwhile; then all lanes form
 // a_n, b_n over n.
 
-__host__ __device__ inline size_t layered_scratch_bytes(int nmaxp) {
+__host__ __device__ inline size_t layered_scratch_serial_bytes(int nmaxp) {
   return 4 * size_t(nmaxp + 1) * sizeof(dz) + ab_scratch_bytes(nmaxp);
+}
+
+// The warp-parallel form keeps every shell's downward D1 at both of its
+// arguments and its upward recurrences (5 arrays a shell), the core's D1,
+// and Ha, Hb.
+__host__ __device__ inline size_t layered_scratch_parallel_bytes(int nmaxp, int L) {
+  return size_t(3 + 5 * (L - 1)) * size_t(nmaxp + 1) * sizeof(dz) +
+         ab_scratch_bytes(nmaxp);
+}
+
+// The parallel form is used when its scratch fits in shared memory.
+__host__ __device__ inline bool layered_parallel(int nmaxp, int L) {
+  return layered_scratch_parallel_bytes(nmaxp, L) <= size_t(200) * 1024;
+}
+
+__host__ __device__ inline size_t layered_scratch_bytes(int nmaxp, int L) {
+  return layered_parallel(nmaxp, L) ? layered_scratch_parallel_bytes(nmaxp, L)
+                                    : layered_scratch_serial_bytes(nmaxp);
 }
 
 // radii [L] ascending (um), idx [L][2] (re, im), core first.
@@ -145,36 +163,95 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     __syncwarp();
     return LMB_ERR_NMAX;
   }
-  dz* d1a = reinterpret_cast<dz*>(scratch);
-  dz* d1b = d1a + (nmaxp + 1);
-  dz* ha = d1b + (nmaxp + 1);
-  dz* hb = ha + (nmaxp + 1);
-  AbScratch w = carve_ab_scratch(reinterpret_cast<char*>(hb + (nmaxp + 1)), nmaxp);
   MieScalars med;
   med.k = s.k;
   med.x = s.x[L - 1];
   med.n_m = n_m;
   med.m = s.m[L - 1];
   med.nmax = s.nmax;
-  if (lane == 0) layered_core(s, d1a, ha, hb);
-  if (lane == 1) {
-    mie_d1_medium(med, w.d1m, w.d1mx);
-    mie_upward(med, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
-  }
-  __syncwarp();
-  for (int ii = 1; ii < L; ++ii) {
-    const bool outer = ii == L - 1;
-    if (lane < 2) {
+  const size_t na = size_t(nmaxp + 1);
+  dz* ha;
+  dz* hb;
+  AbScratch w;
+  if (layered_parallel(nmaxp, L)) {
+    // Warp-parallel: all downward recurrences on lanes of their own
+    // (core, medium and two per shell), then every shell's upward
+    // recurrences on one lane each, then the shells in order with their
+    // Ha/Hb updates spread over the orders.  Same arithmetic per order as
+    // the serial form below.
+    dz* d1c = reinterpret_cast<dz*>(scratch);
+    dz* sh = d1c + na;  // shell ii: d1a, d1b, d3a, d3b, q at sh + 5 (ii-1) na
+    ha = sh + 5 * (L - 1) * na;
+    hb = ha + na;
+    w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
+    if (lane == 0) {
+      dz z1;
+      z1.v = s.x[0] * s.m[0];
+      z1.s = z1.v;
+      z1.m = (L == 1) ? mk(s.x[0], 0.) : mk(0., 0.);
+      layered_d1_down(z1, s.nmax, d1c);
+    } else if (lane == 1) {
+      mie_d1_medium(med, w.d1m, w.d1mx);
+      mie_upward(med, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+    } else if (lane < 2 * L) {
+      const int ii = (lane - 2) / 2 + 1, which = (lane - 2) & 1;
+      const bool outer = ii == L - 1;
       dz z;
-      const double xx = lane == 0 ? s.x[ii] : s.x[ii - 1];
+      const double xx = which == 0 ? s.x[ii] : s.x[ii - 1];
       z.v = xx * s.m[ii];
       z.s = z.v;
       z.m = outer ? mk(xx, 0.) : mk(0., 0.);
-      layered_d1_down(z, s.nmax, lane == 0 ? d1a : d1b);
+      layered_d1_down(z, s.nmax, sh + (5 * (ii - 1) + which) * na);
     }
     __syncwarp();
-    if (lane == 0) layered_shell_up(s, ii, d1a, d1b, ha, hb);
+    if (lane >= 1 && lane < L) {
+      dz* b = sh + 5 * (lane - 1) * na;
+      layered_shell_rec(s, layered_shell_setup(s, lane), b, b + na, b + 2 * na,
+                        b + 3 * na, b + 4 * na);
+    }
+    for (int n = lane; n <= s.nmax; n += 32) {
+      ha[n] = d1c[n];
+      hb[n] = d1c[n];
+    }
     __syncwarp();
+    for (int ii = 1; ii < L; ++ii) {
+      const ShellSetup h = layered_shell_setup(s, ii);
+      const dz* b = sh + 5 * (ii - 1) * na;
+      if (lane == 0) {
+        ha[0] = dconst(mk(0., 0.));
+        hb[0] = dconst(mk(0., 0.));
+      }
+      for (int n = 1 + lane; n <= s.nmax; n += 32)
+        layered_shell_update(h, n, b, b + na, b + 2 * na, b + 3 * na, b + 4 * na,
+                             ha, hb);
+      __syncwarp();
+    }
+  } else {
+    dz* d1a = reinterpret_cast<dz*>(scratch);
+    dz* d1b = d1a + na;
+    ha = d1b + na;
+    hb = ha + na;
+    w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
+    if (lane == 0) layered_core(s, d1a, ha, hb);
+    if (lane == 1) {
+      mie_d1_medium(med, w.d1m, w.d1mx);
+      mie_upward(med, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+    }
+    __syncwarp();
+    for (int ii = 1; ii < L; ++ii) {
+      const bool outer = ii == L - 1;
+      if (lane < 2) {
+        dz z;
+        const double xx = lane == 0 ? s.x[ii] : s.x[ii - 1];
+        z.v = xx * s.m[ii];
+        z.s = z.v;
+        z.m = outer ? mk(xx, 0.) : mk(0., 0.);
+        layered_d1_down(z, s.nmax, lane == 0 ? d1a : d1b);
+      }
+      __syncwarp();
+      if (lane == 0) layered_shell_up(s, ii, d1a, d1b, ha, hb);
+      __syncwarp();
+    }
   }
   for (int n = lane; n < nmaxp; n += 32) {
     if (n == 0 || n > s.nmax) {

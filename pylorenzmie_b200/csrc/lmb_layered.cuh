@@ -130,53 +130,115 @@ LMB_HD void layered_core(const LayeredScalars& s, dz* d1a, dz* ha, dz* hb) {
   }
 }
 
-// One shell ii >= 1 given the downward D1 at z1 (d1a) and z2 (d1b):
-// upward psi*zeta, D3, Q, and Ha/Hb updated in place for n = 1..nmax.
-LMB_HD void layered_shell_up(const LayeredScalars& s, int ii, const dz* d1a,
-                             const dz* d1b, dz* ha, dz* hb) {
+// Constants of shell ii >= 1: the layer's arguments z1 = m_ii x_ii,
+// z2 = m_ii x_{ii-1}, its index and its inner neighbour's (with the outer
+// layer's index tangent), and the starting values of the upward
+// recurrences.
+struct ShellSetup {
+  dz z1, z2, mi, mo;
+  double xr2;
+};
+
+LMB_HD ShellSetup layered_shell_setup(const LayeredScalars& s, int ii) {
   const int L = s.L;
   const bool outer = (ii == L - 1);
-  dz z1, z2, mi, mo;
-  z1.v = s.x[ii] * s.m[ii];
-  z1.s = z1.v;
-  z1.m = outer ? mk(s.x[ii], 0.) : mk(0., 0.);
-  z2.v = s.x[ii - 1] * s.m[ii];
-  z2.s = z2.v;
-  z2.m = outer ? mk(s.x[ii - 1], 0.) : mk(0., 0.);
-  mi = dconst(s.m[ii]);
-  if (outer) mi.m = mk(1., 0.);
-  mo = dconst(s.m[ii - 1]);  // the inner neighbour is never the outer layer
+  ShellSetup h;
+  h.z1.v = s.x[ii] * s.m[ii];
+  h.z1.s = h.z1.v;
+  h.z1.m = outer ? mk(s.x[ii], 0.) : mk(0., 0.);
+  h.z2.v = s.x[ii - 1] * s.m[ii];
+  h.z2.s = h.z2.v;
+  h.z2.m = outer ? mk(s.x[ii - 1], 0.) : mk(0., 0.);
+  h.mi = dconst(s.m[ii]);
+  if (outer) h.mi.m = mk(1., 0.);
+  h.mo = dconst(s.m[ii - 1]);  // the inner neighbour is never the outer layer
   const double xr = s.x[ii - 1] / s.x[ii];
-  const double xr2 = xr * xr;  // independent of the radius scale
+  h.xr2 = xr * xr;  // independent of the radius scale
+  return h;
+}
+
+// Upward recurrences of shell ii for n = 1..nmax: psi*zeta at z1 and z2,
+// D3 at both, and the ratio Q (Eqs. (13)-(15)); stores D3(z1), D3(z2) and
+// Q after step n in d3a[n], d3b[n], q[n].  Serial in n.
+LMB_HD void layered_shell_rec(const LayeredScalars& s, const ShellSetup& h,
+                              const dz* d1a, const dz* d1b, dz* d3a_out,
+                              dz* d3b_out, dz* q_out) {
   const zd ii1 = mk(0., 1.);
-  dz pza = 0.5 * (1. - dexpi(2., z1));
-  dz pzb = 0.5 * (1. - dexpi(2., z2));
+  dz pza = 0.5 * (1. - dexpi(2., h.z1));
+  dz pzb = 0.5 * (1. - dexpi(2., h.z2));
   dz d3a = dconst(ii1), d3b = dconst(ii1);
-  dz q = (dexpi(-2., z2) + (-1.)) / (dexpi(-2., z1) + (-1.));
-  ha[0] = dconst(mk(0., 0.));
-  hb[0] = dconst(mk(0., 0.));
+  dz q = (dexpi(-2., h.z2) + (-1.)) / (dexpi(-2., h.z1) + (-1.));
   for (int n = 1; n <= s.nmax; ++n) {
     const double fn = double(n);
-    const dz nz1 = fn / z1, nz2 = fn / z2;
+    const dz nz1 = fn / h.z1, nz2 = fn / h.z2;
     const dz d3a_prev = d3a, d3b_prev = d3b;
     pza = pza * ((nz1 - d1a[n - 1]) * (nz1 - d3a_prev));
     pzb = pzb * ((nz2 - d1b[n - 1]) * (nz2 - d3b_prev));
     d3a = d1a[n] + ii1 * dinv(pza);
     d3b = d1b[n] + ii1 * dinv(pzb);
-    const dz num = (z1 * d1a[n] + fn) * (fn - z1 * d3a_prev);
-    const dz den = (z2 * d1b[n] + fn) * (fn - z2 * d3b_prev);
-    q = xr2 * (q * num / den);
-    // Ha, Eqs. (7b), (12)-(15)
+    const dz num = (h.z1 * d1a[n] + fn) * (fn - h.z1 * d3a_prev);
+    const dz den = (h.z2 * d1b[n] + fn) * (fn - h.z2 * d3b_prev);
+    q = h.xr2 * (q * num / den);
+    d3a_out[n] = d3a;
+    d3b_out[n] = d3b;
+    q_out[n] = q;
+  }
+}
+
+// Ha, Hb of order n >= 1 carried through shell ii (Eqs. (7b), (8b),
+// (12)-(15)), in place.  Orders are independent here.
+LMB_HD void layered_shell_update(const ShellSetup& h, int n, const dz* d1a,
+                                 const dz* d1b, const dz* d3a, const dz* d3b,
+                                 const dz* q, dz* ha, dz* hb) {
+  {
+    const dz g1 = h.mi * ha[n] - h.mo * d1b[n];
+    const dz g2 = h.mi * ha[n] - h.mo * d3b[n];
+    const dz t = q[n] * g1;
+    ha[n] = (g2 * d1a[n] - t * d3a[n]) / (g2 - t);
+  }
+  {
+    const dz g1 = h.mo * hb[n] - h.mi * d1b[n];
+    const dz g2 = h.mo * hb[n] - h.mi * d3b[n];
+    const dz t = q[n] * g1;
+    hb[n] = (g2 * d1a[n] - t * d3a[n]) / (g2 - t);
+  }
+}
+
+// One shell ii >= 1 given the downward D1 at z1 (d1a) and z2 (d1b):
+// upward psi*zeta, D3, Q, and Ha/Hb updated in place for n = 1..nmax, in
+// one serial pass (no scratch).  The same arithmetic as
+// layered_shell_rec + layered_shell_update, which the warp-parallel form
+// uses.
+LMB_HD void layered_shell_up(const LayeredScalars& s, int ii, const dz* d1a,
+                             const dz* d1b, dz* ha, dz* hb) {
+  const ShellSetup h = layered_shell_setup(s, ii);
+  const zd ii1 = mk(0., 1.);
+  dz pza = 0.5 * (1. - dexpi(2., h.z1));
+  dz pzb = 0.5 * (1. - dexpi(2., h.z2));
+  dz d3a = dconst(ii1), d3b = dconst(ii1);
+  dz q = (dexpi(-2., h.z2) + (-1.)) / (dexpi(-2., h.z1) + (-1.));
+  ha[0] = dconst(mk(0., 0.));
+  hb[0] = dconst(mk(0., 0.));
+  for (int n = 1; n <= s.nmax; ++n) {
+    const double fn = double(n);
+    const dz nz1 = fn / h.z1, nz2 = fn / h.z2;
+    const dz d3a_prev = d3a, d3b_prev = d3b;
+    pza = pza * ((nz1 - d1a[n - 1]) * (nz1 - d3a_prev));
+    pzb = pzb * ((nz2 - d1b[n - 1]) * (nz2 - d3b_prev));
+    d3a = d1a[n] + ii1 * dinv(pza);
+    d3b = d1b[n] + ii1 * dinv(pzb);
+    const dz num = (h.z1 * d1a[n] + fn) * (fn - h.z1 * d3a_prev);
+    const dz den = (h.z2 * d1b[n] + fn) * (fn - h.z2 * d3b_prev);
+    q = h.xr2 * (q * num / den);
     {
-      const dz g1 = mi * ha[n] - mo * d1b[n];
-      const dz g2 = mi * ha[n] - mo * d3b;
+      const dz g1 = h.mi * ha[n] - h.mo * d1b[n];
+      const dz g2 = h.mi * ha[n] - h.mo * d3b;
       const dz t = q * g1;
       ha[n] = (g2 * d1a[n] - t * d3a) / (g2 - t);
     }
-    // Hb, Eqs. (8b), (12)-(15)
     {
-      const dz g1 = mo * hb[n] - mi * d1b[n];
-      const dz g2 = mo * hb[n] - mi * d3b;
+      const dz g1 = h.mo * hb[n] - h.mi * d1b[n];
+      const dz g2 = h.mo * hb[n] - h.mi * d3b;
       const dz t = q * g1;
       hb[n] = (g2 * d1a[n] - t * d3a) / (g2 - t);
     }

@@ -54,8 +54,26 @@ API int h_sphere_ab(double a_p, double n_p, double k_p, double n_m, double lam,
 }
 
 // Multilayer coefficients: radii [L], idx [L][2]; outputs as h_sphere_ab.
+static int layered_ab_impl(const double* radii, const double* idx, int L,
+                           double n_m, double lam, int cap, double* ab,
+                           double* dab, int* nmax, bool split);
+
 API int h_layered_ab(const double* radii, const double* idx, int L, double n_m,
                      double lam, int cap, double* ab, double* dab, int* nmax) {
+  return layered_ab_impl(radii, idx, L, n_m, lam, cap, ab, dab, nmax, false);
+}
+
+// The same through the split shell functions that the warp-parallel
+// kernel path uses (upward recurrences stored, then per-order updates).
+API int h_layered_ab_split(const double* radii, const double* idx, int L,
+                           double n_m, double lam, int cap, double* ab,
+                           double* dab, int* nmax) {
+  return layered_ab_impl(radii, idx, L, n_m, lam, cap, ab, dab, nmax, true);
+}
+
+static int layered_ab_impl(const double* radii, const double* idx, int L,
+                           double n_m, double lam, int cap, double* ab,
+                           double* dab, int* nmax, bool split) {
   LayeredScalars s = layered_setup(radii, idx, L, n_m, lam);
   *nmax = s.nmax;
   if (s.nmax > cap) return 3;
@@ -73,7 +91,19 @@ API int h_layered_ab(const double* radii, const double* idx, int L, double n_m,
     z2.m = outer ? mk(s.x[ii - 1], 0.) : mk(0., 0.);
     layered_d1_down(z1, nm, d1a.data());
     layered_d1_down(z2, nm, d1b.data());
-    layered_shell_up(s, ii, d1a.data(), d1b.data(), ha.data(), hb.data());
+    if (split) {
+      std::vector<dz> d3a(nm + 2), d3b(nm + 2), q(nm + 2);
+      const ShellSetup h = layered_shell_setup(s, ii);
+      layered_shell_rec(s, h, d1a.data(), d1b.data(), d3a.data(), d3b.data(),
+                        q.data());
+      ha[0] = dconst(mk(0., 0.));
+      hb[0] = dconst(mk(0., 0.));
+      for (int n = 1; n <= nm; ++n)
+        layered_shell_update(h, n, d1a.data(), d1b.data(), d3a.data(),
+                             d3b.data(), q.data(), ha.data(), hb.data());
+    } else {
+      layered_shell_up(s, ii, d1a.data(), d1b.data(), ha.data(), hb.data());
+    }
   }
   MieScalars med;
   med.k = s.k;

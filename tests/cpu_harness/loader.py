@@ -39,6 +39,7 @@ def load():
     lib.h_sphere_ab.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, _dp, _dp, _ip]
     lib.h_layered_ab.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_double, ctypes.c_int, _dp, _dp, _ip]
+    lib.h_layered_ab_split.argtypes = lib.h_layered_ab.argtypes
     lib.h_field.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, ctypes.c_int,
                             ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
     lib.h_jacobian.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
@@ -89,7 +90,7 @@ class Harness:
         return ab
 
     def layered_ab(self, radii, indices, n_m, wavelength, cap=1024,
-                   deriv=False):
+                   deriv=False, split=False):
         r = np.ascontiguousarray(radii, dtype=float)
         idx = np.zeros((r.size, 2))
         idx[:, 0] = np.real(indices)
@@ -97,9 +98,9 @@ class Harness:
         ab = np.zeros((cap + 1, 2, 2))
         dab = np.zeros((cap + 1, 4, 2)) if deriv else None
         nmax = ctypes.c_int()
-        st = self.lib.h_layered_ab(ptr(r), ptr(idx), r.size, n_m, wavelength,
-                                   cap, ptr(ab), ptr(dab) if deriv else None,
-                                   ctypes.byref(nmax))
+        fn = self.lib.h_layered_ab_split if split else self.lib.h_layered_ab
+        st = fn(ptr(r), ptr(idx), r.size, n_m, wavelength, cap, ptr(ab),
+                ptr(dab) if deriv else None, ctypes.byref(nmax))
         if st != 0:
             raise ValueError(f'nmax {nmax.value} above cap')
         n = nmax.value

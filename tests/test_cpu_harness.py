@@ -258,3 +258,19 @@ def test_reverse_epilogue_matches_forward(h, shape, p, bohren):
             scale = np.abs(J1[j]).max() + 1e-30
             assert np.abs(J2[j] - J1[j]).max() <= 10 * rtol * scale, \
                 (KEYS[j], fp64, np.abs(J2[j] - J1[j]).max() / scale)
+
+
+@pytest.mark.parametrize('radii,idx', [
+    ([0.3, 0.75], [1.6, 1.45 + 0.002j]),
+    ([0.4, 0.8, 1.2], [1.8 + 0.01j, 1.33, 1.5]),
+    ([0.5, 1.2, 2.0], [1.4, 1.7, 1.55 + 0.001j]),
+    ([0.2, 0.5, 0.9, 1.4, 2.4], [1.35, 1.7, 1.4, 1.6 + 0.003j, 1.5]),
+])
+def test_layered_split_shell_is_identical(h, radii, idx):
+    '''The split shell functions (upward recurrences stored, then
+    independent per-order updates: the warp-parallel kernel path) give
+    bit-identical coefficients and tangents to the fused serial pass.'''
+    a1, d1 = h.layered_ab(radii, idx, 1.34, 0.447, deriv=True)
+    a2, d2 = h.layered_ab(radii, idx, 1.34, 0.447, deriv=True, split=True)
+    np.testing.assert_array_equal(a1, a2)
+    np.testing.assert_array_equal(d1, d2)
