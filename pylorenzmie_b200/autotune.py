@@ -73,7 +73,8 @@ def _store(key, entry):
         path.parent.mkdir(parents=True, exist_ok=True)
         data = _load_file()
         data[key] = entry
-        tmp = path.with_suffix('.tmp')
+        # one temporary file per process: ranks on one host may store at once
+        tmp = path.with_suffix(f'.{os.getpid()}.tmp')
         tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
         tmp.replace(path)
     except OSError:

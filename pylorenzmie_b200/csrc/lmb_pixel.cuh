@@ -343,7 +343,7 @@ enum { PAIR_VALUES = 32, PAIR_QUADS = PAIR_VALUES / 2 };
 struct PairIn {
   f2 sv;              // s = 1 - |cos(theta)|
   f2 ikr;             // sign(mu) / kr
-  f2 nikr2;           // -sign(mu) / kr^2
+  f2 mkr;             // -1 / kr
   cplx<f2> hm1, h0;   // h_{-1}, h~_0
 };
 
@@ -377,7 +377,7 @@ LMB_HD void order_sum_jac_pair(const PairIn& in, const Q4* rec, int nmax,
   f2 pim1 = z2, pi = pk(1.f, 1.f), nd = m1;  // nd = -Delta
   f2 dpim1 = z2, dpi = z2, ndd = z2;         // d/ds
   cplx<f2> h2 = in.hm1, h1 = in.h0, hp2 = zero, hp1 = zero;
-  const f2 sv = in.sv, ikr = in.ikr, nikr2 = in.nikr2;
+  const f2 sv = in.sv, ikr = in.ikr, mkr = in.mkr;
 #pragma unroll 2
   for (int n = 1; n <= nmax; ++n) {
     const Q4* r = rec + PAIR_QUADS * n;
@@ -400,13 +400,14 @@ LMB_HD void order_sum_jac_pair(const PairIn& in, const Q4* rec, int nmax,
     const f2 nddn = pfma(cn, wd, dspi);
     // Riccati-Bessel recurrences (signed as described above)
     const f2 a2 = pmul(tns, ikr), a1 = pmul(fns, ikr);
-    const f2 b2 = pmul(tns, nikr2), b1 = pmul(fns, nikr2);
     const cplx<f2> h = mk(pfma(a2, h1.re, h2.re), pfma(a2, h1.im, h2.im));
     const cplx<f2> dh = mk(pfma(a1, h.re, h1.re), pfma(a1, h.im, h1.im));
-    const cplx<f2> hp = mk(pfma(a2, hp1.re, pfma(b2, h1.re, hp2.re)),
-                           pfma(a2, hp1.im, pfma(b2, h1.im, hp2.im)));
-    const cplx<f2> dhp = mk(pfma(a1, hp.re, pfma(b1, h.re, hp1.re)),
-                            pfma(a1, hp.im, pfma(b1, h.im, hp1.im)));
+    // kr tangents: the chain-rule terms -a2 h'/kr and -a1 h/kr are folded
+    // into the recurrence coefficients' arguments (a (hp - h/kr))
+    const cplx<f2> hp = mk(pfma(a2, pfma(mkr, h1.re, hp1.re), hp2.re),
+                           pfma(a2, pfma(mkr, h1.im, hp1.im), hp2.im));
+    const cplx<f2> dhp = mk(pfma(a1, pfma(mkr, h.re, hp.re), hp1.re),
+                            pfma(a1, pfma(mkr, h.im, hp.im), hp1.im));
     // value and the s tangent
     {
       const cplx<f2> X = pcmul(v[4], v[5], v[6], dh);
@@ -551,7 +552,7 @@ LMB_HD PairIn pair_in(const Geometry<float>& g0, const Geometry<float>& g1) {
   PairIn in;
   in.sv = pk(g0.s1mu, g1.s1mu);
   in.ikr = pk(g0.ikrs, g1.ikrs);
-  in.nikr2 = pk(-(g0.ikrs * g0.ikr), -(g1.ikrs * g1.ikr));
+  in.mkr = pk(-g0.ikr, -g1.ikr);
   in.hm1 = mk(pk(g0.hm1.re, g1.hm1.re), pk(g0.hm1.im, g1.hm1.im));
   in.h0 = mk(pk(g0.h0.re, g1.h0.re), pk(g0.h0.im, g1.h0.im));
   return in;
