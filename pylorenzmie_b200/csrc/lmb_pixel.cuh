@@ -607,6 +607,9 @@ LMB_HD dc3<R> dsub(dc3<R> a, dc3<R> b) {
 // parameters, in the order x_p, y_p, z_p, a_p, n_p, k_p:
 //   e[c]        field component c (Cartesian)
 //   de[j][c]    d e[c] / d param_j
+// Forward mode (dual numbers).  The kernels need only the hologram's
+// derivatives and use holo_jac_reverse; this form gives the field's own
+// derivatives and is the reference the reverse form is checked against.
 template <typename R>
 LMB_HD void epilogue_jac(const Geometry<R>& g, const JacSums<R>& A, R k,
                          cplx<R>* e, cplx<R> (*de)[3]) {
