@@ -538,6 +538,69 @@ def run_extras(dev, inst, chosen_value):
         'vs_oracle_fit': compare_fits(df.iloc[sub].reset_index(drop=True),
                                       ref)}
 
+    # global estimates of a frame's features (DEEstimator defaults: 2 % of
+    # each 121x121 crop's pixels, popsize 10, tol 0.01): the searches side
+    # by side (Frame.estimate, one lmb_chi2_crops launch per generation of
+    # all of them) against one feature at a time (one lmb_chi2_batch
+    # launch per generation of each), and the oracle's numpy search
+    from pylorenzmie_b200 import Frame
+    from oracle import estimate as oest, field as ofield
+    rng = np.random.default_rng(21)
+    nest = 32
+    P = np.zeros((nest, 6))
+    P[:, 0] = 80. + 160. * (np.arange(nest) % 8) + rng.uniform(-3., 3., nest)
+    P[:, 1] = 80. + 160. * (np.arange(nest) // 8) + rng.uniform(-3., 3., nest)
+    P[:, 2] = rng.uniform(100., 300., nest)
+    P[:, 3] = rng.uniform(0.5, 1.5, nest)
+    P[:, 4] = rng.uniform(1.38, 1.60, nest)
+    fm = LorenzMie(coordinates=LorenzMie.meshgrid((640, 1280)),
+                   particle=workloads.spheres(P), instrument=inst, device=dev)
+    fdata = (fm.hologram() + rng.normal(0., inst.noise, 640 * 1280)
+             ).reshape(640, 1280)
+    boxes = [((int(x) - 60, int(y) - 60), 121, 121) for x, y in P[:, :2]]
+
+    def estimate_frame(side):
+        f = Frame(instrument=inst)
+        f.data = fdata
+        f.bboxes = boxes
+        for i, feat in enumerate(f.features):
+            feat.estimator.seed = 40 + i
+        np.random.seed(41)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if side:
+            f.estimate()
+        else:
+            for feat in f.features:
+                feat.estimate()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        return dt, np.array([[ft.particle.z_p, ft.particle.a_p,
+                              ft.particle.n_p] for ft in f.features]), f
+    estimate_frame(True)                           # warm-up
+    t_side, est_side, f = estimate_frame(True)
+    t_one, est_one, _ = estimate_frame(False)
+    nref = 2
+    np.random.seed(41)
+    t0 = time.perf_counter()
+    for ft in f.features[:nref]:
+        oest.de_estimate(ft.data, ft.coordinates,
+                         dict(zip(('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p'),
+                                  [0., 0., 100., 1., 1.5, 0.])),
+                         ofield.DEFAULT_INSTRUMENT, exclude=ft.mask.exclude,
+                         seed=40 + f.features.index(ft))
+    t_ref = time.perf_counter() - t0
+    out['frame_estimate'] = {
+        'value': nest / t_side, 'unit': 'feature estimates/s',
+        'api': 'Frame.estimate, 32 features of 121x121 px, DEEstimator '
+               'defaults, searches side by side',
+        'one_by_one_per_s': nest / t_one,
+        'side_by_side_over_one_by_one': t_one / t_side,
+        'identical_to_one_by_one': bool(np.array_equal(est_side, est_one)),
+        'oracle_numpy_per_s': nref / t_ref,
+        'median_abs_a_p_error_vs_truth_um': float(
+            np.median(np.abs(est_side[:, 1] - P[:, 3])))}
+
     # mixed crop sizes 51..301, 256 features per launch
     sides, truth, start = workloads.mixed_crops(256, seed=9)
     holos, raw = [], []

@@ -162,6 +162,32 @@ int lmb_chi2_batch(const double *coords, long long npts, const double *data,
                    size_t workspace_bytes, void *stream);
 
 /*
+ * lmb_chi2_batch for the searches of many features at once: item i is
+ * compared with the pixels of its own crop item_crop[i].  Replaces the
+ * serial Frame.estimate loop (analysis/Frame.py:158-161), whose features
+ * each run DEEstimator.estimate (analysis/DEEstimator.py:132-173) one
+ * candidate at a time; here one generation of every feature's search is
+ * one launch.
+ *   coords     [3][npts] FP64: the crops' pixels, concatenated
+ *   data       [npts] FP64
+ *   crop_start [ncrops + 1] int64 on the device: crop c is pixels
+ *              [crop_start[c], crop_start[c + 1])
+ *   item_crop  [nitems] int on the device, each in [0, ncrops)
+ *   max_crop_npts  the largest crop (sets the grid; a crop larger than it,
+ *              or a range outside [0, npts), gives that item NaN)
+ *   workspace  of lmb_chi2_workspace_bytes(max_crop_npts, nitems) bytes
+ * Every other argument as lmb_chi2_batch; each item's chi2 is bit-identical
+ * to lmb_chi2_batch over its crop alone.
+ */
+int lmb_chi2_crops(const double *coords, long long npts, const double *data,
+                   double noise, const long long *crop_start, int ncrops,
+                   const int *item_crop, long long max_crop_npts,
+                   const lmb_sphere *spheres, const int *item_start, int nitems,
+                   const double *ab, const int *nmax, int nmax_cap, double k,
+                   int flags, double *chi2, int *nonfinite, void *workspace,
+                   size_t workspace_bytes, void *stream);
+
+/*
  * Hologram and its Jacobian for nitems single-sphere items, FP32 sums,
  * Cartesian field (LMB_BOHREN honoured).  Fills the analytic-Jacobian
  * slot of the reference: jaxLorenzMie.jac / jac_params

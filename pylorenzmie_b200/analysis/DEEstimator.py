@@ -21,7 +21,8 @@ from scipy.optimize import differential_evolution
 
 from .BaseEstimator import BaseEstimator
 from .Mask import Mask
-from ._population import PopulationChi2, batchable
+from ._population import (CropPopulations, PopulationChi2, batchable,
+                          de_settings, lockstep_de)
 
 DEFAULT_BOUNDS = {
     'z_p': (10., 600.),
@@ -56,10 +57,6 @@ def run_search(model, data, coords, variables, bounds, noise, popsize, seed,
     '''scipy differential_evolution over ``variables`` with the population
     objective; returns the OptimizeResult.  The model's coordinates are
     restored on exit.'''
-    settings = dict(settings)
-    settings.pop('workers', None)
-    settings['updating'] = 'deferred'
-    settings['vectorized'] = True
     saved = model.coordinates
     try:
         if batchable(model, variables):
@@ -69,9 +66,59 @@ def run_search(model, data, coords, variables, bounds, noise, popsize, seed,
             objective = _HostObjective(model, data, variables, noise)
         with np.errstate(over='ignore', invalid='ignore'):
             return differential_evolution(objective, bounds, popsize=popsize,
-                                          seed=seed, **settings)
+                                          seed=seed, **de_settings(settings))
     finally:
         model.coordinates = saved
+
+
+def run_searches(searches, workers=256):
+    '''run_search for each of ``searches`` (dicts of its arguments); returns
+    the OptimizeResults in order.  Searches whose models share the device,
+    the instrument, the noise and the precision run side by side, every
+    generation of all of them in one lmb_chi2_crops launch (lockstep_de);
+    the rest one at a time.  Each result is the one run_search gives.'''
+    import torch
+    results = [None] * len(searches)
+    groups = {}
+    for i, sr in enumerate(searches):
+        m = sr['model']
+        if not batchable(m, sr['variables']):
+            groups.setdefault(None, []).append(i)
+            continue
+        inst = m.instrument
+        key = (str(m.device), float(inst.n_m), float(inst.wavelength),
+               float(inst.magnification), float(sr['noise']),
+               bool(getattr(m, 'double_precision', False)))
+        groups.setdefault(key, []).append(i)
+    for key, idx in groups.items():
+        if key is None or len(idx) == 1:
+            for i in idx:
+                results[i] = run_search(**searches[i])
+            continue
+        members = [searches[i] for i in idx]
+        pop = CropPopulations([(sr['model'], sr['data'], sr['coords'],
+                                sr['variables']) for sr in members],
+                              members[0]['noise'])
+        dev = pop.device
+        out = lockstep_de(members, pop.evaluate, workers, dev,
+                          torch.cuda.current_stream(dev))
+        for i, r in zip(idx, out):
+            results[i] = r
+    return results
+
+
+def estimate_many(estimators, holograms):
+    '''estimator.estimate(hologram) for each pair, the searches side by
+    side (run_searches); returns the Series in order.  Estimators that
+    share a model run one after another, as the model carries each
+    search's start.'''
+    estimators, holograms = list(estimators), list(holograms)
+    if len({id(e.model) for e in estimators}) < len(estimators):
+        return [e.estimate(h) for e, h in zip(estimators, holograms)]
+    searches = [e.search(h) for e, h in zip(estimators, holograms)]
+    results = run_searches(searches)
+    return [e.accept(sr, r) for e, sr, r in zip(estimators, searches,
+                                                 results)]
 
 
 @dataclass
@@ -100,19 +147,30 @@ class DEEstimator(BaseEstimator):
             if hasattr(self, name):
                 setattr(self, name, value)
 
-    def estimate(self, hologram):
-        '''Estimate particle parameters; returns the particle's properties
-        as a pandas Series and leaves the model at the estimate.'''
+    def search(self, hologram):
+        '''The arguments of run_search for this hologram: x_p, y_p pinned
+        to the crop's centre and a fresh random pixel subset drawn
+        (analysis/DEEstimator.py:146-156).'''
         self.model.particle.x_p = float(hologram.coordinates[0].mean())
         self.model.particle.y_p = float(hologram.coordinates[1].mean())
         mask = Mask(fraction=self.fraction)
         if self.exclude is not None:
             mask.exclude = self.exclude
         data, coords = mask.apply(hologram)
-        variables = list(self.bounds.keys())
-        result = run_search(self.model, data, coords, variables,
-                            list(self.bounds.values()),
-                            self.model.instrument.noise, self.popsize,
-                            self.seed, self.settings)
-        self.model.properties = dict(zip(variables, result.x))
+        return dict(model=self.model, data=data, coords=coords,
+                    variables=list(self.bounds.keys()),
+                    bounds=list(self.bounds.values()),
+                    noise=self.model.instrument.noise, popsize=self.popsize,
+                    seed=self.seed, settings=self.settings)
+
+    def accept(self, search, result):
+        '''Leave the model at the search's result; its properties as a
+        Series.'''
+        self.model.properties = dict(zip(search['variables'], result.x))
         return pd.Series(self.model.particle.properties)
+
+    def estimate(self, hologram):
+        '''Estimate particle parameters; returns the particle's properties
+        as a pandas Series and leaves the model at the estimate.'''
+        search = self.search(hologram)
+        return self.accept(search, run_search(**search))

@@ -20,6 +20,7 @@ from ..theory.Instrument import Instrument
 from ..theory.LorenzMie import LorenzMie
 from .Hologram import Hologram
 from .Feature import Feature
+from .DEEstimator import estimate_many
 from . import _fit
 
 
@@ -117,10 +118,19 @@ class Frame(Hologram):
         return len(self._features)
 
     def estimate(self):
-        '''Estimate parameters of every feature (DEEstimator; each
-        generation of each search is one population launch).'''
-        for feature in self.features:
-            feature.estimate()
+        '''Estimate parameters of every feature.  The features' searches
+        run side by side: each generation of all of them is one population
+        launch (estimate_many); estimators without that form run one by
+        one.'''
+        feats = self.features
+        side = [f for f in feats if hasattr(f.estimator, 'search') and
+                hasattr(f.estimator, 'accept')]
+        rest = feats
+        if len(side) > 1:
+            estimate_many([f.estimator for f in side], side)
+            rest = [f for f in feats if not any(f is g for g in side)]
+        for f in rest:
+            f.estimate()
 
     def optimize(self):
         '''Fit every feature; one batched device fit per group of

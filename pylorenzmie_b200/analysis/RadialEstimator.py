@@ -41,7 +41,10 @@ class RadialEstimator(BaseEstimator):
             if hasattr(self, name):
                 setattr(self, name, value)
 
-    def estimate(self, hologram):
+    def search(self, hologram):
+        '''The arguments of run_search for this hologram: the azimuthal
+        profile about the crop's centre along the radial spoke
+        (analysis/RadialEstimator.py:134-147).'''
         x_p = float(hologram.coordinates[0].mean())
         y_p = float(hologram.coordinates[1].mean())
         self.model.particle.x_p = x_p
@@ -50,10 +53,18 @@ class RadialEstimator(BaseEstimator):
         profile = Azimuthal.avg(hologram.data, center=(x_p - cx, y_p - cy))
         radii = np.arange(len(profile), dtype=float)
         coords = np.vstack([x_p + radii, np.full(len(profile), y_p)])
-        variables = list(self.bounds.keys())
-        result = run_search(self.model, profile, coords, variables,
-                            list(self.bounds.values()),
-                            self.model.instrument.noise, self.popsize,
-                            self.seed, self.settings)
-        self.model.properties = dict(zip(variables, result.x))
+        return dict(model=self.model, data=profile, coords=coords,
+                    variables=list(self.bounds.keys()),
+                    bounds=list(self.bounds.values()),
+                    noise=self.model.instrument.noise, popsize=self.popsize,
+                    seed=self.seed, settings=self.settings)
+
+    def accept(self, search, result):
+        '''Leave the model at the search's result; its properties as a
+        Series.'''
+        self.model.properties = dict(zip(search['variables'], result.x))
         return pd.Series(self.model.particle.properties)
+
+    def estimate(self, hologram):
+        search = self.search(hologram)
+        return self.accept(search, run_search(**search))

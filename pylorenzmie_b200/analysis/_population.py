@@ -2,13 +2,25 @@
 one launch (lmb_chi2_batch): the batched form of the reference's per-
 candidate objectives (analysis/DEEstimator.py:23-37,
 analysis/RadialEstimator.py:17-37), which evaluate model.hologram() once per
-candidate, in worker processes.'''
+candidate, in worker processes.
+
+The searches of many features (Frame.estimate, analysis/Frame.py:158-161,
+runs them one after another) go further: ``lockstep_de`` runs scipy's
+differential_evolution for each on a thread of its own, and every
+generation of all of them is evaluated together by ``CropPopulations`` in
+one lmb_chi2_crops launch.  Each search keeps scipy's own code and random
+stream, and each candidate's value is bit-identical to the one-search
+launch, so a seeded search ends where it ends alone.'''
+import threading
+
 import numpy as np
 import torch
+from scipy.optimize import differential_evolution
 
 from ..theory import _kernels as K
 
 SPHERE_KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
+MAX_ITEMS = 65535          # candidates per launch (the grid's y extent)
 
 
 def batchable(model, variables):
@@ -22,6 +34,50 @@ def batchable(model, variables):
     return all(v in SPHERE_KEYS for v in variables)
 
 
+def de_settings(settings):
+    '''scipy settings of a population search: one objective call per
+    generation (vectorized, deferred updating, as the reference's
+    'deferred'); the reference's worker processes have no role here.'''
+    settings = dict(settings)
+    settings.pop('workers', None)
+    settings['updating'] = 'deferred'
+    settings['vectorized'] = True
+    return settings
+
+
+def _coords3(coords):
+    c = np.atleast_2d(np.asarray(coords, dtype=float))
+    c3 = np.zeros((3, c.shape[1]))
+    c3[:c.shape[0]] = c
+    return c3
+
+
+def _records(P):
+    rec = np.zeros(len(P), dtype=K.SPHERE_DTYPE)
+    for j, key in enumerate(SPHERE_KEYS):
+        rec[key] = P[:, j]
+    return rec
+
+
+class _Candidates:
+    '''The fixed sphere parameters of one search and the slots its
+    variables fill: candidates(x) -> (S, 6) sphere parameters.'''
+
+    def __init__(self, model, variables):
+        p = model.particle
+        r = np.asarray(p.r_p, float) + np.asarray(
+            getattr(p, 'r_0', (0., 0., 0.)), float)
+        self.base = np.array([r[0], r[1], r[2], p.a_p, p.n_p,
+                              getattr(p, 'k_p', 0.)])
+        self.slots = [SPHERE_KEYS.index(v) for v in variables]
+
+    def __call__(self, x):
+        X = np.asarray(x, dtype=float).reshape(len(self.slots), -1)
+        P = np.tile(self.base, (X.shape[1], 1))
+        P[:, self.slots] = X.T
+        return P
+
+
 class PopulationChi2:
     '''callable(x) for scipy.optimize.differential_evolution with
     vectorized=True: x is (nvar, S) (or (nvar,)); returns the S values of
@@ -30,18 +86,10 @@ class PopulationChi2:
     def __init__(self, model, data, coords, variables, noise):
         self.model = model
         dev = model.device
-        c = np.atleast_2d(np.asarray(coords, dtype=float))
-        c3 = np.zeros((3, c.shape[1]))
-        c3[:c.shape[0]] = c
-        self.coords = torch.from_numpy(c3).to(dev)
+        self.coords = torch.from_numpy(_coords3(coords)).to(dev)
         self.data = torch.from_numpy(
             np.ascontiguousarray(data, dtype=np.float64)).to(dev)
-        p = model.particle
-        r = np.asarray(p.r_p, float) + np.asarray(
-            getattr(p, 'r_0', (0., 0., 0.)), float)
-        self.base = np.array([r[0], r[1], r[2], p.a_p, p.n_p,
-                              getattr(p, 'k_p', 0.)])
-        self.slots = [SPHERE_KEYS.index(v) for v in variables]
+        self.candidates = _Candidates(model, variables)
         inst = model.instrument
         self.n_m, self.wavelength = inst.n_m, inst.wavelength
         self.k = inst.wavenumber()
@@ -52,15 +100,10 @@ class PopulationChi2:
     def __call__(self, x):
         x = np.asarray(x, dtype=float)
         single = x.ndim == 1
-        X = x.reshape(len(self.slots), -1)
-        S = X.shape[1]
-        P = np.tile(self.base, (S, 1))
-        P[:, self.slots] = X.T
-        rec = np.zeros(S, dtype=K.SPHERE_DTYPE)
-        for j, key in enumerate(SPHERE_KEYS):
-            rec[key] = P[:, j]
+        P = self.candidates(x)
+        S = len(P)
         dev = self.coords.device
-        sp = K.spheres_tensor(rec, dev)
+        sp = K.spheres_tensor(_records(P), dev)
         cap = K.nmax_cap_for(P[:, 3], P[:, 4], P[:, 5], self.n_m,
                              self.wavelength)
         ab, _, nmax = K.sphere_ab(sp, self.n_m, self.wavelength, cap,
@@ -82,3 +125,195 @@ class PopulationChi2:
                 ab[sel], nmax[sel], cap, self.k, fp64=True).cpu().numpy()
         self.evaluations += S
         return float(chi2[0]) if single else chi2
+
+
+class CropPopulations:
+    '''The objectives of several searches, each over a crop of its own,
+    evaluated together: ``evaluate({search: x})`` computes every population
+    it is given in one lmb_chi2_crops launch (per 65535 candidates).  The
+    searches share the instrument, the noise and the precision.
+
+    searches : list of (model, data, coords, variables), as PopulationChi2.
+    '''
+
+    def __init__(self, searches, noise):
+        model = searches[0][0]
+        self.device = dev = model.device
+        c3 = [_coords3(c) for _, _, c, _ in searches]
+        sizes = [c.shape[1] for c in c3]
+        self.coords = torch.from_numpy(
+            np.ascontiguousarray(np.hstack(c3))).to(dev)
+        self.data = torch.from_numpy(np.concatenate(
+            [np.asarray(d, dtype=np.float64).ravel() for _, d, _, _ in searches]
+        )).to(dev)
+        self.crop_start = torch.from_numpy(np.concatenate(
+            [[0], np.cumsum(sizes)]).astype(np.int64)).to(dev)
+        self.max_npts = max(sizes)
+        self.candidates = [_Candidates(m, v) for m, _, _, v in searches]
+        inst = model.instrument
+        self.n_m, self.wavelength = inst.n_m, inst.wavelength
+        self.k = inst.wavenumber()
+        self.noise = float(noise)
+        self.fp64 = bool(getattr(model, 'double_precision', False))
+        self.evaluations = 0
+
+    def evaluate(self, batch):
+        '''batch: {search index: x}, x as scipy passes it ((nvar, S), or
+        (nvar,) for one candidate); returns {search index: values}.'''
+        order = sorted(batch)
+        P = [self.candidates[i](batch[i]) for i in order]
+        counts = [len(p) for p in P]
+        crop = np.concatenate([np.full(n, i, dtype=np.int32)
+                               for i, n in zip(order, counts)])
+        P = np.vstack(P)
+        chi2 = np.empty(len(P))
+        for a in range(0, len(P), MAX_ITEMS):
+            b = min(a + MAX_ITEMS, len(P))
+            chi2[a:b] = self._launch(P[a:b], crop[a:b])
+        self.evaluations += len(P)
+        out, at = {}, 0
+        for i, n in zip(order, counts):
+            v = chi2[at:at + n]
+            at += n
+            out[i] = float(v[0]) if np.ndim(batch[i]) == 1 else v
+        return out
+
+    def _launch(self, P, crop):
+        dev = self.device
+        sp = K.spheres_tensor(_records(P), dev)
+        cap = K.nmax_cap_for(P[:, 3], P[:, 4], P[:, 5], self.n_m,
+                             self.wavelength)
+        ab, _, nmax = K.sphere_ab(sp, self.n_m, self.wavelength, cap,
+                                  check=False)
+        n = len(P)
+        item_start = torch.arange(n + 1, dtype=torch.int32, device=dev)
+        item_crop = K.to_device_async(crop, dev)
+        chi2, bad = K.chi2_crops(self.coords, self.data, self.noise,
+                                 self.crop_start, item_crop, self.max_npts,
+                                 sp, item_start, ab, nmax, cap, self.k,
+                                 fp64=self.fp64)
+        bad = bad.cpu().numpy()
+        chi2 = chi2.cpu().numpy()
+        redo = np.flatnonzero(bad) if not self.fp64 else []
+        if len(redo):
+            # FP32 overflow where the focal plane cuts the sphere: FP64
+            sel = torch.from_numpy(redo).to(dev)
+            m = len(redo)
+            chi2[redo] = K.chi2_crops(
+                self.coords, self.data, self.noise, self.crop_start,
+                item_crop[sel], self.max_npts, sp[sel],
+                torch.arange(m + 1, dtype=torch.int32, device=dev), ab[sel],
+                nmax[sel], cap, self.k, fp64=True)[0].cpu().numpy()
+        return chi2
+
+
+class _Aborted(Exception):
+    '''Ends a search whose companions failed.'''
+
+
+class Lockstep:
+    '''Gathers one objective call from every running search and evaluates
+    them together.  ``workers`` threads take part; each runs one search at a
+    time and calls ``leave()`` when it has no more.  A generation runs when
+    every live worker has submitted, on the thread that completed it, under
+    ``device`` and ``stream`` (the caller's; worker threads start on the
+    default device and stream).'''
+
+    def __init__(self, workers, evaluate, device=None, stream=None):
+        self._cv = threading.Condition()
+        self._live = workers
+        self._pending = {}
+        self._results = {}
+        self.error = None
+        self._evaluate = evaluate
+        self._device, self._stream = device, stream
+        self.generations = 0
+
+    def objective(self, i):
+        return lambda x: self._submit(i, x)
+
+    def _submit(self, i, x):
+        with self._cv:
+            if self.error is not None:
+                raise _Aborted()
+            self._pending[i] = x
+            if len(self._pending) == self._live:
+                self._run()
+            while i not in self._results and self.error is None:
+                self._cv.wait(1.0)
+            if i in self._results:
+                return self._results.pop(i)
+            raise _Aborted()
+
+    def leave(self):
+        with self._cv:
+            self._live -= 1
+            if self._pending and len(self._pending) == self._live:
+                self._run()
+
+    def fail(self, error):
+        with self._cv:
+            if self.error is None:
+                self.error = error
+            self._cv.notify_all()
+
+    def _run(self):
+        batch, self._pending = self._pending, {}
+        if self.error is None:
+            try:
+                if self._device is None:
+                    self._results.update(self._evaluate(batch))
+                else:
+                    with torch.cuda.device(self._device), \
+                            torch.cuda.stream(self._stream):
+                        self._results.update(self._evaluate(batch))
+                self.generations += 1
+            except BaseException as e:   # handed to every search
+                self.error = e
+        self._cv.notify_all()
+
+
+def lockstep_de(problems, evaluate, workers=256, device=None, stream=None):
+    '''scipy differential_evolution for each of ``problems`` (dicts with
+    bounds, popsize, seed, settings), side by side: every generation's
+    populations of all running searches go to ``evaluate`` together (see
+    Lockstep).  Returns the OptimizeResults in order; an exception of any
+    search or of ``evaluate`` is raised after every thread has ended.'''
+    n = len(problems)
+    results = [None] * n
+    if n == 0:
+        return results
+    nw = max(1, min(n, int(workers)))
+    step = Lockstep(nw, evaluate, device, stream)
+    queue = iter(range(n))
+    qlock = threading.Lock()
+
+    def worker():
+        try:
+            while step.error is None:
+                with qlock:
+                    j = next(queue, None)
+                if j is None:
+                    break
+                pr = problems[j]
+                with np.errstate(over='ignore', invalid='ignore'):
+                    results[j] = differential_evolution(
+                        step.objective(j), pr['bounds'],
+                        popsize=pr['popsize'], seed=pr['seed'],
+                        **de_settings(pr['settings']))
+        except _Aborted:
+            pass
+        except BaseException as e:
+            step.fail(e)
+        finally:
+            step.leave()
+
+    threads = [threading.Thread(target=worker, daemon=True)
+               for _ in range(nw)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if step.error is not None:
+        raise step.error
+    return results

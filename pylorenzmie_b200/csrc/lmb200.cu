@@ -263,27 +263,31 @@ size_t lmb_chi2_workspace_bytes(long long npts, int nitems) {
   return align_up(n * sizeof(double), 256) + n * sizeof(int);
 }
 
-int lmb_chi2_batch(const double* coords, long long npts, const double* data,
-                   double noise, const lmb_sphere* spheres,
-                   const int* item_start, int nitems, const double* ab,
-                   const int* nmax, int nmax_cap, double k, int flags,
-                   double* chi2, int* nonfinite, void* workspace,
-                   size_t workspace_bytes, void* stream) {
-  if (nitems < 0 || npts < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
+// Shared by lmb_chi2_batch (one pixel set) and lmb_chi2_crops (a crop per
+// item): grid (blocks over the largest pixel set) x items.
+static int chi2_launch(const double* coords, long long npts, const double* data,
+                       double noise, const long long* crop_start, int ncrops,
+                       const int* item_crop, long long span,
+                       const lmb_sphere* spheres, const int* item_start,
+                       int nitems, const double* ab, const int* nmax,
+                       int nmax_cap, double k, int flags, double* chi2,
+                       int* nonfinite, void* workspace, size_t workspace_bytes,
+                       void* stream) {
+  if (nitems < 0 || npts < 0 || span < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
   if (nitems == 0) return LMB_OK;
   if (!chi2 || !(noise > 0.)) return LMB_ERR_ARG;
   cudaStream_t st = as_stream(stream);
-  if (npts == 0) {
+  if (span == 0) {
     LMB_CK(cudaMemsetAsync(chi2, 0, sizeof(double) * nitems, st));
     if (nonfinite) LMB_CK(cudaMemsetAsync(nonfinite, 0, sizeof(int) * nitems, st));
     return LMB_OK;
   }
   if (!coords || !data || !spheres || !item_start || !ab || !nmax) return LMB_ERR_ARG;
-  if (nitems > 65535 || (npts + 255) / 256 > 0x7fffffffLL) return LMB_ERR_ARG;
-  if (!workspace || workspace_bytes < lmb_chi2_workspace_bytes(npts, nitems))
+  if (nitems > 65535 || (span + 255) / 256 > 0x7fffffffLL) return LMB_ERR_ARG;
+  if (!workspace || workspace_bytes < lmb_chi2_workspace_bytes(span, nitems))
     return LMB_ERR_WORKSPACE;
   const int tpb = 256;
-  const int nb = int((npts + tpb - 1) / tpb);
+  const int nb = int((span + tpb - 1) / tpb);
   double* partial = reinterpret_cast<double*>(workspace);
   int* partial_bad = reinterpret_cast<int*>(
       reinterpret_cast<char*>(workspace) +
@@ -293,20 +297,48 @@ int lmb_chi2_batch(const double* coords, long long npts, const double* data,
     const size_t smem = sizeof(Quad<double>) * 2 * (size_t(nmax_cap) + 1);
     LMB_CK(smem_attr((const void*)k_chi2<double>, smem));
     k_chi2<double><<<grid, tpb, smem, st>>>(
-        coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
-        nmax_cap + 1, k, flags, data, 1. / noise, partial, partial_bad);
+        coords, npts, crop_start, item_crop, ncrops, spheres, item_start,
+        reinterpret_cast<const zd*>(ab), nmax, nmax_cap + 1, k, flags, data,
+        1. / noise, partial, partial_bad);
   } else {
     const size_t smem = sizeof(Quad<float>) * 2 * (size_t(nmax_cap) + 1);
     LMB_CK(smem_attr((const void*)k_chi2<float>, smem));
     k_chi2<float><<<grid, tpb, smem, st>>>(
-        coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
-        nmax_cap + 1, k, flags, data, 1. / noise, partial, partial_bad);
+        coords, npts, crop_start, item_crop, ncrops, spheres, item_start,
+        reinterpret_cast<const zd*>(ab), nmax, nmax_cap + 1, k, flags, data,
+        1. / noise, partial, partial_bad);
   }
   LMB_CK(cudaGetLastError());
   k_chi2_reduce<<<(nitems + 127) / 128, 128, 0, st>>>(partial, partial_bad, nb,
                                                        nitems, chi2, nonfinite);
   LMB_CK(cudaGetLastError());
   return LMB_OK;
+}
+
+int lmb_chi2_batch(const double* coords, long long npts, const double* data,
+                   double noise, const lmb_sphere* spheres,
+                   const int* item_start, int nitems, const double* ab,
+                   const int* nmax, int nmax_cap, double k, int flags,
+                   double* chi2, int* nonfinite, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  return chi2_launch(coords, npts, data, noise, nullptr, 0, nullptr, npts,
+                     spheres, item_start, nitems, ab, nmax, nmax_cap, k, flags,
+                     chi2, nonfinite, workspace, workspace_bytes, stream);
+}
+
+int lmb_chi2_crops(const double* coords, long long npts, const double* data,
+                   double noise, const long long* crop_start, int ncrops,
+                   const int* item_crop, long long max_crop_npts,
+                   const lmb_sphere* spheres, const int* item_start, int nitems,
+                   const double* ab, const int* nmax, int nmax_cap, double k,
+                   int flags, double* chi2, int* nonfinite, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  if (ncrops <= 0 || !crop_start || !item_crop || max_crop_npts > npts)
+    return nitems == 0 ? LMB_OK : LMB_ERR_ARG;
+  return chi2_launch(coords, npts, data, noise, crop_start, ncrops, item_crop,
+                     max_crop_npts, spheres, item_start, nitems, ab, nmax,
+                     nmax_cap, k, flags, chi2, nonfinite, workspace,
+                     workspace_bytes, stream);
 }
 
 int lmb_jacobian(const double* coords, long long npts,

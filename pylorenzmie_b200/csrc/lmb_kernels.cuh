@@ -491,27 +491,54 @@ k_field_pair(const double* __restrict__ coords, long long npts,
 // of nitems particle lists (the objective of a differential-evolution
 // generation), NaN residuals skipped as numpy.nansum does.  Per (item,
 // block) partial sums in FP64; k_chi2_reduce adds them in a fixed order.
+// With crop_start, item i is compared with the pixels of its own crop
+// item_crop[i], [crop_start[c], crop_start[c + 1]) of coords and data (the
+// searches of many features in one launch); the grid covers the largest
+// crop, and blocks past an item's crop add zeros.  An item whose crop range
+// is invalid gets NaN.
 template <typename R>
 __global__ void __launch_bounds__(256)
 k_chi2(const double* __restrict__ coords, long long npts,
-       const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
-       const zd* __restrict__ ab, const int* __restrict__ nmax, int nmaxp, double k,
-       int flags, const double* __restrict__ data, double inv_noise,
+       const long long* __restrict__ crop_start, const int* __restrict__ item_crop,
+       int ncrops, const lmb_sphere* __restrict__ spheres,
+       const int* __restrict__ item_start, const zd* __restrict__ ab,
+       const int* __restrict__ nmax, int nmaxp, double k, int flags,
+       const double* __restrict__ data, double inv_noise,
        double* __restrict__ partial, int* __restrict__ partial_bad) {
   extern __shared__ __align__(16) char smem[];
   __shared__ double red[256 / 32];
   __shared__ int redb[256 / 32];
   Quad<R>* coef = reinterpret_cast<Quad<R>*>(smem);
   const int item = blockIdx.y;
+  const size_t slot = (size_t)item * gridDim.x + blockIdx.x;
+  long long base = 0, count = npts;
+  if (crop_start) {
+    const int c = item_crop[item];
+    bool ok = c >= 0 && c < ncrops;
+    if (ok) {
+      base = crop_start[c];
+      count = crop_start[c + 1] - base;
+      ok = base >= 0 && count >= 0 && base + count <= npts &&
+           count <= (long long)gridDim.x * blockDim.x;
+    }
+    // uniform over the block: before any barrier
+    if (!ok || (long long)blockIdx.x * blockDim.x >= count) {
+      if (threadIdx.x == 0) {
+        partial[slot] = ok ? 0. : __longlong_as_double(0x7ff8000000000000LL);
+        partial_bad[slot] = 0;
+      }
+      return;
+    }
+  }
   const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = pix < npts;
+  const bool live = pix < count;
   const bool cart = flags & LMB_CARTESIAN;
   const bool bohren = flags & LMB_BOHREN;
   double x = 0., y = 0., z = 0.;
   if (live) {
-    x = coords[pix];
-    y = coords[npts + pix];
-    z = coords[2 * npts + pix];
+    x = coords[base + pix];
+    y = coords[npts + base + pix];
+    z = coords[2 * npts + base + pix];
   }
   cplx<R> e[3];
   for (int c = 0; c < 3; ++c) e[c] = mk(R(0), R(0));
@@ -536,7 +563,7 @@ k_chi2(const double* __restrict__ coords, long long npts,
   if (live) {
     const R h = intensity<R>(e);
     bad = isfinite(h) ? 0 : 1;
-    const double r = (double(h) - data[pix]) * inv_noise;
+    const double r = (double(h) - data[base + pix]) * inv_noise;
     if (r == r) v = r * r;  // nansum
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -556,8 +583,8 @@ k_chi2(const double* __restrict__ coords, long long npts,
       t += red[w];
       b += redb[w];
     }
-    partial[(size_t)item * gridDim.x + blockIdx.x] = t;
-    partial_bad[(size_t)item * gridDim.x + blockIdx.x] = b;
+    partial[slot] = t;
+    partial_bad[slot] = b;
   }
 }
 

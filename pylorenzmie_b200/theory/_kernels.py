@@ -154,6 +154,34 @@ def chi2(coords, data, noise, spheres, item_start, ab, nmax, cap, k,
     return out[:nitems]
 
 
+def chi2_crops(coords, data, noise, crop_start, item_crop, max_crop_npts,
+               spheres, item_start, ab, nmax, cap, k, cartesian=True,
+               bohren=True, fp64=False):
+    '''chi2 as above with item i compared with the pixels of its own crop
+    item_crop[i], [crop_start[c], crop_start[c + 1]) of coords and data
+    (lmb_chi2_crops): (nitems,) float64 sums and (nitems,) int32 counts of
+    NaN or infinite hologram pixels.'''
+    coords, data, crop_start, item_crop, spheres, item_start, ab, nmax = \
+        _contiguous(coords, data, crop_start, item_crop, spheres, item_start,
+                    ab, nmax)
+    lib = _native.load()
+    dev = coords.device
+    npts = coords.shape[1]
+    nitems = item_start.shape[0] - 1
+    ncrops = crop_start.shape[0] - 1
+    out = torch.empty(max(nitems, 1), dtype=torch.float64, device=dev)
+    bad = torch.empty(max(nitems, 1), dtype=torch.int32, device=dev)
+    nbytes = lib.lmb_chi2_workspace_bytes(int(max_crop_npts), nitems)
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    _native.check(lib.lmb_chi2_crops(
+        ptr(coords), npts, ptr(data), float(noise), ptr(crop_start), ncrops,
+        ptr(item_crop), int(max_crop_npts), ptr(spheres), ptr(item_start),
+        nitems, ptr(ab), ptr(nmax), cap, float(k),
+        _flags(cartesian, bohren, fp64), ptr(out), ptr(bad), ptr(ws), nbytes,
+        stream_handle(dev)), 'lmb_chi2_crops')
+    return out[:nitems], bad[:nitems]
+
+
 def field(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
           bohren=True, fp64=False, aberration=0.):
     '''(nitems, 3, npts) scattered fields; complex64, or complex128.'''

@@ -73,6 +73,113 @@ def test_population_chi2_matches_oracle():
     np.testing.assert_allclose(obj(P[:, 2:5].T), ref, rtol=2e-5)
 
 
+def test_chi2_crops_matches_each_crop():
+    '''lmb_chi2_crops: every candidate's value is bit-identical to
+    lmb_chi2_batch over its own crop alone (FP32 and FP64 sums, including
+    the non-finite counts); an item whose crop index is out of range gets
+    NaN.'''
+    import torch
+    from pylorenzmie_b200.theory import _kernels as K
+    rng = np.random.default_rng(8)
+    dev = torch.device('cuda')
+    inst = ofield.DEFAULT_INSTRUMENT
+    k = ofield.wavenumber(1.34, 0.447, 0.048)
+    sizes = [300, 1031, 37, 0, 513]
+    crops, datas = [], []
+    for n in sizes:
+        c = np.vstack([rng.uniform(0., 80., n), rng.uniform(0., 80., n),
+                       np.zeros(n)])
+        t = dict(zip(KEYS, [40., 40., 150., 0.9, 1.45, 0.]))
+        d = ofield.hologram(c, [t], inst) + rng.normal(0., 0.05, n) \
+            if n else np.zeros(0)
+        if n > 5:
+            d[5] = np.nan
+        crops.append(c)
+        datas.append(d)
+    counts = [7, 3, 5, 2, 6]
+    P = np.vstack([np.column_stack([
+        np.full(m, 40.), np.full(m, 40.), rng.uniform(20., 300., m),
+        rng.uniform(0.3, 2.5, m), rng.uniform(1.2, 2.2, m), np.zeros(m)])
+        for m in counts])
+    crop = np.concatenate([np.full(m, i) for i, m in enumerate(counts)]
+                          ).astype(np.int32)
+    rec = np.zeros(len(P), dtype=K.SPHERE_DTYPE)
+    for j, key in enumerate(KEYS):
+        rec[key] = P[:, j]
+    sp = K.spheres_tensor(rec, dev)
+    cap = K.nmax_cap_for(P[:, 3], P[:, 4], P[:, 5], 1.34, 0.447)
+    ab, _, nmax = K.sphere_ab(sp, 1.34, 0.447, cap)
+    allc = torch.from_numpy(np.hstack(crops)).to(dev)
+    alld = torch.from_numpy(np.concatenate(datas)).to(dev)
+    cs = torch.from_numpy(np.concatenate([[0], np.cumsum(sizes)])
+                          .astype(np.int64)).to(dev)
+    n = len(P)
+    istart = torch.arange(n + 1, dtype=torch.int32, device=dev)
+    for fp64 in (False, True):
+        got, bad = K.chi2_crops(allc, alld, 0.05, cs,
+                                torch.from_numpy(crop).to(dev), max(sizes),
+                                sp, istart, ab, nmax, cap, k, fp64=fp64)
+        got, bad = got.cpu().numpy(), bad.cpu().numpy()
+        at = 0
+        for i, m in enumerate(counts):
+            sel = torch.arange(at, at + m, device=dev)
+            ref, rbad = K.chi2(
+                torch.from_numpy(crops[i]).to(dev),
+                torch.from_numpy(datas[i]).to(dev), 0.05, sp[sel],
+                torch.arange(m + 1, dtype=torch.int32, device=dev), ab[sel],
+                nmax[sel], cap, k, fp64=fp64, nonfinite=True)
+            np.testing.assert_array_equal(got[at:at + m], ref.cpu().numpy())
+            np.testing.assert_array_equal(bad[at:at + m], rbad.cpu().numpy())
+            at += m
+        assert np.all(got[sum(counts[:3]):sum(counts[:4])] == 0.)  # empty
+    wrong = crop.copy()
+    wrong[[0, 9]] = [len(sizes), -1]
+    got, _ = K.chi2_crops(allc, alld, 0.05, cs, torch.from_numpy(wrong).to(dev),
+                          max(sizes), sp, istart, ab, nmax, cap, k)
+    got = got.cpu().numpy()
+    assert np.isnan(got[[0, 9]]).all() and np.isfinite(got[1:9]).all()
+
+
+@pytest.mark.parametrize('kind', ['de', 'radial'])
+def test_frame_estimate_side_by_side(kind):
+    '''Frame.estimate runs the features' searches side by side (one
+    lmb_chi2_crops launch per generation of all of them); with seeded
+    searches each feature's estimate is bit-identical to its own
+    Feature.estimate, FP32 sums.'''
+    from pylorenzmie_b200 import Frame, Instrument, RadialEstimator
+    data, truth, bboxes = _frame_data(seed=9)
+    inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
+    bounds = {'z_p': (50., 400.), 'a_p': (0.3, 2.0), 'n_p': (1.35, 1.8)}
+    serial = {'tol': 0.01, 'polish': False, 'updating': 'deferred',
+              'workers': 1}
+    out = []
+    for side in (True, False):
+        f = Frame(instrument=inst)
+        f.data = data
+        f.bboxes = bboxes
+        for i, feat in enumerate(f.features):
+            if kind == 'radial':
+                feat.estimator = RadialEstimator(model=feat.model)
+            else:
+                feat.estimator.fraction = 0.1
+            feat.estimator.bounds = dict(bounds)
+            feat.estimator.seed = 20 + i
+            feat.estimator.settings = dict(serial)
+        np.random.seed(7)
+        if side:
+            f.estimate()
+        else:
+            for feat in f.features:
+                feat.estimate()
+        out.append(np.array([[feat.particle.x_p, feat.particle.y_p,
+                              feat.particle.z_p, feat.particle.a_p,
+                              feat.particle.n_p] for feat in f.features]))
+    np.testing.assert_array_equal(out[0], out[1])
+    lo = [b[0] for b in bounds.values()]
+    hi = [b[1] for b in bounds.values()]
+    assert np.all((out[0][:, 2:] >= lo) & (out[0][:, 2:] <= hi))
+
+
 @pytest.mark.parametrize('which', ['de', 'radial'])
 def test_estimators_follow_reference_search(golden_estimate, which):
     '''FP64 model: the population search reproduces the reference's seeded
