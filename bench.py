@@ -542,7 +542,10 @@ def run_extras(dev, inst, chosen_value):
     # each 121x121 crop's pixels, popsize 10, tol 0.01): the searches side
     # by side (Frame.estimate, one lmb_chi2_crops launch per generation of
     # all of them) against one feature at a time (one lmb_chi2_batch
-    # launch per generation of each), and the oracle's numpy search
+    # launch per generation of each), both with and without scipy's own
+    # per-candidate code (a callback that never stops the search selects
+    # it), and the
+    # oracle's numpy search
     from pylorenzmie_b200 import Frame
     from oracle import estimate as oest, field as ofield
     rng = np.random.default_rng(21)
@@ -559,12 +562,18 @@ def run_extras(dev, inst, chosen_value):
              ).reshape(640, 1280)
     boxes = [((int(x) - 60, int(y) - 60), 121, 121) for x, y in P[:, :2]]
 
-    def estimate_frame(side):
+    def _no_stop(xk, convergence):
+        return False
+
+    def estimate_frame(side, scipy_code=False):
         f = Frame(instrument=inst)
         f.data = fdata
         f.bboxes = boxes
         for i, feat in enumerate(f.features):
             feat.estimator.seed = 40 + i
+            if scipy_code:
+                feat.estimator.settings = dict(feat.estimator.settings,
+                                               callback=_no_stop)
         np.random.seed(41)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -580,6 +589,8 @@ def run_extras(dev, inst, chosen_value):
     estimate_frame(True)                           # warm-up
     t_side, est_side, f = estimate_frame(True)
     t_one, est_one, _ = estimate_frame(False)
+    t_side_sp, est_side_sp, _ = estimate_frame(True, True)
+    t_one_sp, est_one_sp, _ = estimate_frame(False, True)
     nref = 2
     np.random.seed(41)
     t0 = time.perf_counter()
@@ -595,8 +606,12 @@ def run_extras(dev, inst, chosen_value):
         'api': 'Frame.estimate, 32 features of 121x121 px, DEEstimator '
                'defaults, searches side by side',
         'one_by_one_per_s': nest / t_one,
-        'side_by_side_over_one_by_one': t_one / t_side,
-        'identical_to_one_by_one': bool(np.array_equal(est_side, est_one)),
+        'scipy_code_side_by_side_per_s': nest / t_side_sp,
+        'scipy_code_one_by_one_per_s': nest / t_one_sp,
+        'identical_all_four': bool(
+            np.array_equal(est_side, est_one) and
+            np.array_equal(est_side, est_side_sp) and
+            np.array_equal(est_side, est_one_sp)),
         'oracle_numpy_per_s': nref / t_ref,
         'median_abs_a_p_error_vs_truth_um': float(
             np.median(np.abs(est_side[:, 1] - P[:, 3])))}

@@ -7,11 +7,14 @@ subset of ``fraction`` of the pixels (minus ``exclude``) is drawn once per
 call (:143-146), and scipy's differential_evolution minimizes
 sum(((H - data)/noise)^2) with NaN residuals skipped (:32-37) over
 ``bounds`` (:153-166).  The reference evaluates each candidate with one
-model.hologram() call, spread over worker processes; here the search runs
-scipy's same algorithm with ``vectorized=True`` and ``updating='deferred'``
-(the reference's setting), so a generation is one lmb_chi2_batch launch.
-With the same seed and an FP64 model the search follows the reference's
-trajectory; with FP32 sums the energies differ by rounding only.
+model.hologram() call, spread over worker processes; here a generation is
+one lmb_chi2_batch launch, and the search is scipy's algorithm with
+``updating='deferred'`` (the reference's setting) either as run_populations
+restates it (the estimators' settings; no per-candidate Python) or as
+scipy itself with ``vectorized=True``.  With the same seed and an FP64
+model the search follows the reference's trajectory; with FP32 sums the
+energies differ by rounding only.  run_searches / estimate_many search many
+features together, one lmb_chi2_crops launch per generation of all of them.
 '''
 from dataclasses import dataclass, field
 
@@ -21,6 +24,7 @@ from scipy.optimize import differential_evolution
 
 from .BaseEstimator import BaseEstimator
 from .Mask import Mask
+from ._de import run_populations, supported
 from ._population import (CropPopulations, PopulationChi2, batchable,
                           de_settings, lockstep_de)
 
@@ -61,6 +65,12 @@ def run_search(model, data, coords, variables, bounds, noise, popsize, seed,
     try:
         if batchable(model, variables):
             objective = PopulationChi2(model, data, coords, variables, noise)
+            if supported(settings):
+                problem = dict(bounds=bounds, popsize=popsize, seed=seed,
+                               settings=settings)
+                with np.errstate(over='ignore', invalid='ignore'):
+                    return run_populations(
+                        [problem], lambda b: {0: objective(b[0])})[0]
         else:
             model.coordinates = coords
             objective = _HostObjective(model, data, variables, noise)
@@ -75,8 +85,10 @@ def run_searches(searches, workers=256):
     '''run_search for each of ``searches`` (dicts of its arguments); returns
     the OptimizeResults in order.  Searches whose models share the device,
     the instrument, the noise and the precision run side by side, every
-    generation of all of them in one lmb_chi2_crops launch (lockstep_de);
-    the rest one at a time.  Each result is the one run_search gives.'''
+    generation of all of them in one lmb_chi2_crops launch (run_populations,
+    or scipy on threads in lockstep_de for settings that form does not
+    cover); the rest one at a time.  Each result is the one run_search
+    gives.'''
     import torch
     results = [None] * len(searches)
     groups = {}
@@ -99,9 +111,13 @@ def run_searches(searches, workers=256):
         pop = CropPopulations([(sr['model'], sr['data'], sr['coords'],
                                 sr['variables']) for sr in members],
                               members[0]['noise'])
-        dev = pop.device
-        out = lockstep_de(members, pop.evaluate, workers, dev,
-                          torch.cuda.current_stream(dev))
+        if all(supported(sr['settings']) for sr in members):
+            with np.errstate(over='ignore', invalid='ignore'):
+                out = run_populations(members, pop.evaluate)
+        else:
+            dev = pop.device
+            out = lockstep_de(members, pop.evaluate, workers, dev,
+                              torch.cuda.current_stream(dev))
         for i, r in zip(idx, out):
             results[i] = r
     return results

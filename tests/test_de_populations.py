@@ -1,0 +1,148 @@
+'''The thread-free form of scipy's differential evolution (run_populations)
+against scipy.optimize.differential_evolution itself: for every setting the
+estimators use, each search returns exactly what scipy returns for it
+(solution, energies, whole final population, nit, nfev, message), with
+int, RandomState, Generator and global-generator seeds, scalar and
+dithered mutation, exits at maxiter, fixed bounds, NaN energies and the
+re-evaluation of an all-infinite first population.'''
+import numpy as np
+import pytest
+from scipy.optimize import differential_evolution
+
+from pylorenzmie_b200.analysis._de import Population, run_populations, supported
+from pylorenzmie_b200.analysis._population import de_settings
+
+
+def _objective(c, w, nan_band=None, inf_calls=0):
+    calls = [0]
+
+    def f(x):
+        calls[0] += 1
+        X = np.asarray(x, dtype=float).reshape(len(c), -1)
+        v = np.sum(((X - np.asarray(c)[:, None]) / np.asarray(w)[:, None])
+                   ** 2, axis=0)
+        v = v + np.sin(3. * X[0]) ** 2            # a few local minima
+        if nan_band is not None:
+            v[(X[0] > nan_band[0]) & (X[0] < nan_band[1])] = np.nan
+        if calls[0] <= inf_calls:
+            v[:] = np.inf
+        return v
+    return f
+
+
+def _cases():
+    base = {'tol': 0.01, 'polish': False, 'updating': 'deferred',
+            'workers': -1}
+    return [
+        dict(bounds=[(10., 600.), (0.25, 10.), (1., 3.)], popsize=10,
+             seed=3, settings=dict(base),
+             f=(_objective, ([200., 1., 1.5], [100., 0.3, 0.1]))),
+        dict(bounds=[(-2., 2.), (-2., 2.)], popsize=7,
+             seed=np.random.RandomState(11),
+             settings=dict(base, tol=1e-4, mutation=0.8, recombination=0.5),
+             f=(_objective, ([0.3, -0.2], [1., 1.]))),
+        dict(bounds=[(-2., 2.), (0.5, 0.5), (0., 1.)], popsize=6,
+             seed=np.random.default_rng(5),
+             settings=dict(base, maxiter=7),
+             f=(_objective, ([0.1, 0.5, 0.4], [1., 1., 0.3]))),
+        dict(bounds=[(-3., 3.)] * 4, popsize=5, seed=19,
+             settings=dict(base, tol=0., atol=1e-3, maxiter=40,
+                           mutation=(0.2, 1.5)),
+             f=(_objective, ([0.5, 0.1, -0.3, 1.], [1., 2., 1., 0.5]),
+                {'nan_band': (-0.5, 0.2)})),
+        dict(bounds=[(0., 5.), (0., 5.)], popsize=8, seed=23,
+             settings=dict(base),
+             f=(_objective, ([2., 3.], [1., 1.]), {'inf_calls': 1})),
+    ]
+
+
+def _fresh_seed(seed, k):
+    # an equal, independent generator for each of the two runs
+    if isinstance(seed, np.random.RandomState):
+        return np.random.RandomState(11)
+    if isinstance(seed, np.random.Generator):
+        return np.random.default_rng(5)
+    return seed
+
+
+def _make(case):
+    fn, args, *kw = case['f']
+    return fn(*args, **(kw[0] if kw else {}))
+
+
+def _scipy(case, k):
+    f = _make(case)
+    with np.errstate(invalid='ignore'):
+        return differential_evolution(f, case['bounds'],
+                                      popsize=case['popsize'],
+                                      seed=_fresh_seed(case['seed'], k),
+                                      **de_settings(case['settings']))
+
+
+def _assert_same(r, ref):
+    np.testing.assert_array_equal(r.x, ref.x)
+    np.testing.assert_array_equal(r.population, ref.population)
+    np.testing.assert_array_equal(r.population_energies,
+                                  ref.population_energies)
+    assert (r.fun == ref.fun) or (np.isnan(r.fun) and np.isnan(ref.fun))
+    assert (r.nit, r.nfev, r.message, r.success) == \
+        (ref.nit, ref.nfev, ref.message, ref.success)
+
+
+def test_each_search_matches_scipy_alone():
+    cases = _cases()
+    for k, case in enumerate(cases):
+        assert supported(case['settings'])
+        f = _make(case)
+        pr = dict(case, seed=_fresh_seed(case['seed'], k))
+        with np.errstate(invalid='ignore'):
+            r = run_populations([pr], lambda b: {0: f(b[0])})[0]
+        _assert_same(r, _scipy(case, k))
+
+
+def test_searches_together_match_scipy():
+    '''All cases stepped together (each evaluation sees every unfinished
+    search); seeded searches are unaffected by their companions.'''
+    cases = _cases()
+    fs = [_make(c) for c in cases]
+    problems = [dict(c, seed=_fresh_seed(c['seed'], k))
+                for k, c in enumerate(cases)]
+    rounds = []
+
+    def evaluate(batch):
+        rounds.append(sorted(batch))
+        return {i: fs[i](x) for i, x in batch.items()}
+    with np.errstate(invalid='ignore'):
+        got = run_populations(problems, evaluate)
+    for k, (case, r) in enumerate(zip(cases, got)):
+        _assert_same(r, _scipy(case, k))
+    assert rounds[0] == list(range(len(cases)))
+    assert len(rounds) == max(r.nfev for r in got)
+
+
+def test_global_generator_search_matches_scipy():
+    case = _cases()[0]
+    f = _make(case)
+    np.random.seed(31)
+    r = run_populations([dict(case, seed=None)], lambda b: {0: f(b[0])})[0]
+    np.random.seed(31)
+    ref = differential_evolution(_make(case), case['bounds'],
+                                 popsize=case['popsize'], seed=None,
+                                 **de_settings(case['settings']))
+    _assert_same(r, ref)
+
+
+@pytest.mark.parametrize('extra', [{'polish': True}, {'strategy': 'rand1bin'},
+                                   {'init': 'sobol'}, {'maxfun': 100},
+                                   {'x0': [1., 1.]}, {'callback': print},
+                                   {'mutation': (0.5, 2.5)}, {'maxiter': 0},
+                                   {'unknown': 1}])
+def test_other_settings_go_to_scipy(extra):
+    s = {'tol': 0.01, 'polish': False, 'updating': 'deferred'}
+    assert supported(s)
+    assert not supported(dict(s, **extra))
+
+
+def test_bad_bounds_raise():
+    with pytest.raises(ValueError):
+        Population([(0., np.inf)], popsize=5, seed=1)

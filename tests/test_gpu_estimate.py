@@ -140,12 +140,18 @@ def test_chi2_crops_matches_each_crop():
     assert np.isnan(got[[0, 9]]).all() and np.isfinite(got[1:9]).all()
 
 
+def _no_stop(xk, convergence):
+    return False
+
+
 @pytest.mark.parametrize('kind', ['de', 'radial'])
 def test_frame_estimate_side_by_side(kind):
     '''Frame.estimate runs the features' searches side by side (one
     lmb_chi2_crops launch per generation of all of them); with seeded
     searches each feature's estimate is bit-identical to its own
-    Feature.estimate, FP32 sums.'''
+    Feature.estimate, FP32 sums, and to scipy's differential_evolution
+    itself (a callback that never stops them sends the searches through
+    scipy, on threads for the frame).'''
     from pylorenzmie_b200 import Frame, Instrument, RadialEstimator
     data, truth, bboxes = _frame_data(seed=9)
     inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
@@ -153,7 +159,9 @@ def test_frame_estimate_side_by_side(kind):
     serial = {'tol': 0.01, 'polish': False, 'updating': 'deferred',
               'workers': 1}
     out = []
-    for side in (True, False):
+    for side, settings in ((True, serial), (False, serial),
+                           (True, dict(serial, callback=_no_stop)),
+                           (False, dict(serial, callback=_no_stop))):
         f = Frame(instrument=inst)
         f.data = data
         f.bboxes = bboxes
@@ -164,7 +172,7 @@ def test_frame_estimate_side_by_side(kind):
                 feat.estimator.fraction = 0.1
             feat.estimator.bounds = dict(bounds)
             feat.estimator.seed = 20 + i
-            feat.estimator.settings = dict(serial)
+            feat.estimator.settings = dict(settings)
         np.random.seed(7)
         if side:
             f.estimate()
@@ -174,7 +182,8 @@ def test_frame_estimate_side_by_side(kind):
         out.append(np.array([[feat.particle.x_p, feat.particle.y_p,
                               feat.particle.z_p, feat.particle.a_p,
                               feat.particle.n_p] for feat in f.features]))
-    np.testing.assert_array_equal(out[0], out[1])
+    for o in out[1:]:
+        np.testing.assert_array_equal(out[0], o)
     lo = [b[0] for b in bounds.values()]
     hi = [b[1] for b in bounds.values()]
     assert np.all((out[0][:, 2:] >= lo) & (out[0][:, 2:] <= hi))
