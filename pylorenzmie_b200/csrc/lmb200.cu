@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <mutex>
 #include <thread>
@@ -569,29 +570,44 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
     // by wait_seconds without progress.
     int since_admission = 0, pending = cnt[4];
     auto wait_start = std::chrono::steady_clock::now();
+    // In the tail (every feature admitted, at most 1/16 of them running)
+    // several rounds go out per read of the counters: a round with nothing
+    // left to do is an evaluation launch that finds no tiles and a step
+    // launch whose features are all done, cheaper than the host round
+    // trip.  The burst doubles while the tail lasts, from 2 up to 16.
+    int burst = 1;
+    bool capped = false;
     while (cnt[1] > 0 || cnt[4] > 0) {
-      if (cnt[1] > 0) {
-        if (++since_admission > c.max_iterations + 1) break;
-        if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) {
-          status = LMB_ERR_CUDA;
-          break;
+      const bool tail = cnt[4] == 0 && cnt[1] > 0 && cnt[1] * 16 <= nfeatures;
+      burst = tail ? std::min(2 * burst, 16) : 1;
+      for (int r = 0; r < burst && status == LMB_OK; ++r) {
+        if (cnt[1] > 0) {
+          if (++since_admission > c.max_iterations + 1) {
+            capped = true;
+            break;
+          }
+          if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) {
+            status = LMB_ERR_CUDA;
+            break;
+          }
+          if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+          eval<<<egrid, shape.tpb, eval_smem, st>>>(c);
+          if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+          launches += 1;
+          ++evals;
+        } else {
+          const double waited = std::chrono::duration<double>(
+              std::chrono::steady_clock::now() - wait_start).count();
+          if (waited > wait_seconds) { status = LMB_ERR_TIMEOUT; break; }
+          std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
-        if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-        eval<<<egrid, shape.tpb, eval_smem, st>>>(c);
-        if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
+        cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
+        cudaMemsetAsync(c.counters + 4, 0, 2 * sizeof(int), st);  // [4], [5]
+        k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
         launches += 1;
-        ++evals;
-      } else {
-        const double waited = std::chrono::duration<double>(
-            std::chrono::steady_clock::now() - wait_start).count();
-        if (waited > wait_seconds) { status = LMB_ERR_TIMEOUT; break; }
-        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        ++iterations;
       }
-      cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
-      cudaMemsetAsync(c.counters + 4, 0, 2 * sizeof(int), st);  // [4], [5]
-      k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
-      launches += 1;
-      ++iterations;
+      if (status != LMB_OK || capped) break;
       if (cudaGetLastError() != cudaSuccess || !read_counts()) {
         status = LMB_ERR_CUDA;
         break;
