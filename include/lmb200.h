@@ -300,7 +300,10 @@ size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
  *   workspace / workspace_bytes: scratch of lmb_fit_workspace_bytes(...)
  *   stats    optional host pointer (NULL: no measurement)
  * The call returns once every feature has terminated (or
- * max_iterations evaluations have run); it synchronizes the stream.
+ * max_iterations evaluations have run).  The last kernel it queues, which
+ * writes params and results, may still be running on the stream then:
+ * read them in stream order (a copy on the same stream, or after
+ * cudaStreamSynchronize).  With stats the call waits for that kernel too.
  * Features whose pixels fall outside [0, total_pixels) end with status -1.
  */
 int lmb_fit_batch(const lmb_feature *features, int nfeatures,

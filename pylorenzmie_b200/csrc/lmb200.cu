@@ -28,10 +28,42 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Opt a kernel in to more than 48 KB of dynamic shared memory when needed.
+// Per-call host work kept off the path between fits: the shared-memory
+// attribute of a kernel is raised once per device to the largest size asked
+// for, and persistent grid sizes are looked up once per (device, kernel,
+// block, shared memory).
+std::mutex g_launch_cache_lock;
+struct AttrEntry {
+  int device;
+  const void* fn;
+  size_t value;
+  int tpb;
+  size_t smem;
+};
+std::vector<AttrEntry> g_smem_set;    // value: bytes set
+std::vector<AttrEntry> g_grid_sizes;  // value: grid
+
+inline int current_device() {
+  int dev = -1;
+  return cudaGetDevice(&dev) == cudaSuccess ? dev : -1;
+}
+
 inline cudaError_t smem_attr(const void* fn, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(bytes));
+  const int dev = current_device();
+  std::lock_guard<std::mutex> hold(g_launch_cache_lock);
+  for (const AttrEntry& e : g_smem_set)
+    if (e.device == dev && e.fn == fn && e.value >= bytes) return cudaSuccess;
+  const cudaError_t r = cudaFuncSetAttribute(
+      fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  if (r != cudaSuccess || dev < 0) return r;
+  for (AttrEntry& e : g_smem_set)
+    if (e.device == dev && e.fn == fn) {
+      e.value = bytes;
+      return r;
+    }
+  g_smem_set.push_back({dev, fn, bytes, 0, 0});
+  return r;
 }
 
 inline bool bad_cap(int nmax_cap) { return nmax_cap < 1 || nmax_cap > LMB_NMAX_LIMIT; }
@@ -110,12 +142,22 @@ FitLayout fit_layout(int nf, long long total_pixels, int nmax_cap) {
 }
 
 int persistent_grid(const void* fn, int tpb, size_t smem) {
-  int dev = 0, sms = 148, per = 1;
-  if (cudaGetDevice(&dev) == cudaSuccess)
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int dev = current_device();
+  {
+    std::lock_guard<std::mutex> hold(g_launch_cache_lock);
+    for (const AttrEntry& e : g_grid_sizes)
+      if (e.device == dev && e.fn == fn && e.tpb == tpb && e.smem == smem)
+        return int(e.value);
+  }
+  int sms = 148, per = 1;
+  if (dev >= 0) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, tpb, smem) != cudaSuccess ||
-      per < 1)
-    per = 1;
+      per < 1) {
+    cudaGetLastError();
+    return sms;  // not cached: asked again next time
+  }
+  std::lock_guard<std::mutex> hold(g_launch_cache_lock);
+  g_grid_sizes.push_back({dev, fn, size_t(sms * per), tpb, smem});
   return sms * per;
 }
 
@@ -441,6 +483,51 @@ size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
 
 namespace {
 
+// Host-side resources of the pipelined round loop, one set per host thread
+// and device: a ring of pinned slots, each taking a copy of the fit's
+// counters (8 ints) and work totals (2 x 64 bit) after a round, and an
+// event per slot.  Made on first use and kept until the process exits.
+constexpr int kRingSlots = 32;
+constexpr int kSlotInts = 16;
+constexpr size_t kSlotCopyBytes = 8 * sizeof(int) + 2 * sizeof(unsigned long long);
+constexpr int kRingDevices = 64;
+struct RoundRing {
+  int* slots = nullptr;
+  cudaEvent_t done[kRingSlots] = {};
+};
+
+std::vector<cudaEvent_t>* timing_pool() {
+  static thread_local std::vector<cudaEvent_t> pools[kRingDevices];
+  const int dev = current_device();
+  if (dev < 0 || dev >= kRingDevices) return nullptr;
+  return &pools[dev];
+}
+
+RoundRing* round_ring() {
+  static thread_local RoundRing rings[kRingDevices];
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kRingDevices)
+    return nullptr;
+  RoundRing& r = rings[dev];
+  if (r.slots) return &r;
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, sizeof(int) * kSlotInts * kRingSlots,
+                    cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  for (int i = 0; i < kRingSlots; ++i) {
+    if (cudaEventCreateWithFlags(&r.done[i], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      for (int j = 0; j < i; ++j) cudaEventDestroy(r.done[j]);
+      cudaFreeHost(p);
+      return nullptr;
+    }
+  }
+  r.slots = static_cast<int*>(p);
+  return &r;
+}
+
 int fit_batch_impl(const lmb_feature* features, int nfeatures,
                    long long total_pixels, const float* data,
                    const float* coords, lmb_sphere* params, double n_m,
@@ -450,7 +537,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
                    size_t workspace_bytes, lmb_fit_stats* stats, void* stream,
                    int nlayers, const double* layer_frac,
                    const double* layer_index, const int* ready = nullptr,
-                   double wait_seconds = 0.) {
+                   double wait_seconds = 0., bool sync_rounds = false) {
   if (nlayers < 1 || nlayers > LMB_MAX_LAYERS) return LMB_ERR_ARG;
   if (nlayers > 1 && nfeatures > 0 && (!layer_frac || !layer_index))
     return LMB_ERR_ARG;
@@ -532,101 +619,171 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   LMB_CK(smem_attr((const void*)eval, eval_smem));
   const int egrid = persistent_grid((const void*)eval, shape.tpb, eval_smem);
 
-  // Optional timing: one event pair per evaluation launch, plus the span.
+  // Optional timing: one event pair per evaluation launch, plus the span;
+  // the events come from a per-thread, per-device pool kept across calls.
   std::vector<cudaEvent_t> ev;
+  std::vector<cudaEvent_t>* pool = stats ? timing_pool() : nullptr;
+  if (stats && !pool) return LMB_ERR_CUDA;
   auto mark = [&](void) -> cudaError_t {
-    cudaEvent_t e;
-    cudaError_t r = cudaEventCreate(&e);
-    if (r != cudaSuccess) return r;
+    if (ev.size() == pool->size()) {
+      cudaEvent_t e;
+      const cudaError_t r = cudaEventCreate(&e);
+      if (r != cudaSuccess) return r;
+      pool->push_back(e);
+    }
+    cudaEvent_t e = (*pool)[ev.size()];
     ev.push_back(e);
     return cudaEventRecord(e, st);
   };
-  auto release = [&]() {
-    for (cudaEvent_t e : ev) cudaEventDestroy(e);
-    ev.clear();
-  };
+  auto release = [&]() { ev.clear(); };
   int launches = 0, evals = 0, iterations = 0;
+  int counted_evals = -1;  // evaluations that found work (pipelined loop)
   int status = LMB_OK;
   // counters[1] (features with an evaluation pending) and counters[4]
   // (features still waiting for their data) after each step
   int cnt[5] = {0, 0, 0, 0, 0};
+  int overflow = 0;
+  unsigned long long work[2] = {0ull, 0ull};
   auto read_counts = [&]() -> bool {
     return cudaMemcpyAsync(cnt, c.counters, sizeof(cnt), cudaMemcpyDeviceToHost,
                            st) == cudaSuccess &&
            cudaStreamSynchronize(st) == cudaSuccess;
   };
+  auto launch_eval = [&]() -> bool {
+    if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) return false;
+    if (stats && mark() != cudaSuccess) return false;
+    eval<<<egrid, shape.tpb, eval_smem, st>>>(c);
+    if (stats && mark() != cudaSuccess) return false;
+    launches += 1;
+    ++evals;
+    return true;
+  };
+  auto launch_step = [&]() {
+    cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
+    cudaMemsetAsync(c.counters + 4, 0, 2 * sizeof(int), st);  // [4], [5]
+    k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
+    launches += 1;
+    ++iterations;
+  };
+  // The pipelined loop (below) keeps rounds queued ahead of the host; it
+  // needs pinned counter slots, so the callers that may not allocate, and
+  // streamed admission (whose rounds wait for data), take this loop.
+  RoundRing* ring = (sync_rounds || ready) ? nullptr : round_ring();
+  bool pipelined = ring != nullptr;
   do {
     if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
     k_fit_setup<<<1, 1024, 0, st>>>(c);
     k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
     launches += 2;
-    if (cudaGetLastError() != cudaSuccess || !read_counts()) {
-      status = LMB_ERR_CUDA;
-      break;
-    }
-    // Every evaluation advances each running feature's nfev, which the
-    // step kernel caps at max_iterations, so the rounds after the last
-    // admission are bounded by max_iterations; waiting for data is bounded
-    // by wait_seconds without progress.
-    int since_admission = 0, pending = cnt[4];
-    auto wait_start = std::chrono::steady_clock::now();
-    // In the tail (every feature admitted, at most 1/16 of them running)
-    // several rounds go out per read of the counters: a round with nothing
-    // left to do is an evaluation launch that finds no tiles and a step
-    // launch whose features are all done, cheaper than the host round
-    // trip.  The burst doubles while the tail lasts, from 2 up to 16.
-    int burst = 1;
-    bool capped = false;
-    while (cnt[1] > 0 || cnt[4] > 0) {
-      const bool tail = cnt[4] == 0 && cnt[1] > 0 && cnt[1] * 16 <= nfeatures;
-      burst = tail ? std::min(2 * burst, 16) : 1;
-      for (int r = 0; r < burst && status == LMB_OK; ++r) {
-        if (cnt[1] > 0) {
-          if (++since_admission > c.max_iterations + 1) {
+    if (pipelined) {
+      // Round r's counters (and the work totals after them) land in slot
+      // r of a ring of pinned buffers, with an event; the host reads round
+      // r while round r + 1 (and, in the tail, up to 15 more) already run,
+      // so the GPU does not wait for the host between rounds.  A round
+      // issued after one that left no feature running finds no tiles and
+      // only finished features: it changes nothing.
+      auto issue_copy = [&](int r) -> bool {
+        int* slot = ring->slots + size_t(r % kRingSlots) * kSlotInts;
+        return cudaMemcpyAsync(slot, c.counters, kSlotCopyBytes,
+                               cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+               cudaEventRecord(ring->done[r % kRingSlots], st) == cudaSuccess;
+      };
+      if (cudaGetLastError() != cudaSuccess || !issue_copy(0)) {
+        status = LMB_ERR_CUDA;
+        break;
+      }
+      int issued = 1, consumed = 0, depth = 2, eval_rounds = 0;
+      bool capped = false;
+      for (;;) {
+        while (!capped && issued - consumed < depth) {
+          // the step kernel caps every feature's evaluations at
+          // max_iterations, so this bound is a safety net only
+          if (++eval_rounds > c.max_iterations + 1) {
             capped = true;
             break;
           }
-          if (cudaMemsetAsync(c.counters + 0, 0, sizeof(int), st) != cudaSuccess) {
+          if (!launch_eval()) { status = LMB_ERR_CUDA; break; }
+          launch_step();
+          if (cudaGetLastError() != cudaSuccess || !issue_copy(issued)) {
             status = LMB_ERR_CUDA;
             break;
           }
-          if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-          eval<<<egrid, shape.tpb, eval_smem, st>>>(c);
-          if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
-          launches += 1;
-          ++evals;
-        } else {
-          const double waited = std::chrono::duration<double>(
-              std::chrono::steady_clock::now() - wait_start).count();
-          if (waited > wait_seconds) { status = LMB_ERR_TIMEOUT; break; }
-          std::this_thread::sleep_for(std::chrono::microseconds(20));
+          ++issued;
         }
-        cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
-        cudaMemsetAsync(c.counters + 4, 0, 2 * sizeof(int), st);  // [4], [5]
-        k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
-        launches += 1;
-        ++iterations;
+        if (status != LMB_OK) break;
+        // with the rounds capped, wait for the last one issued
+        const int r = capped ? issued - 1 : consumed;
+        if (cudaEventSynchronize(ring->done[r % kRingSlots]) != cudaSuccess) {
+          status = LMB_ERR_CUDA;
+          break;
+        }
+        const int* slot = ring->slots + size_t(r % kRingSlots) * kSlotInts;
+        memcpy(cnt, slot, sizeof(cnt));
+        overflow = slot[3];
+        memcpy(work, slot + 8, sizeof(work));
+        consumed = r + 1;
+        // rounds 1..r evaluated; later ones only found nothing to do
+        counted_evals = r;
+        if (capped || cnt[1] == 0) break;
+        const bool tail = cnt[1] * 16 <= nfeatures;
+        depth = tail ? std::min(2 * depth, 16) : 2;
       }
-      if (status != LMB_OK || capped) break;
+      if (status != LMB_OK) break;
+    } else {
       if (cudaGetLastError() != cudaSuccess || !read_counts()) {
         status = LMB_ERR_CUDA;
         break;
       }
-      if (cnt[4] < pending) {  // new features admitted
-        pending = cnt[4];
-        since_admission = 0;
-        wait_start = std::chrono::steady_clock::now();
+      // Every evaluation advances each running feature's nfev, which the
+      // step kernel caps at max_iterations, so the rounds after the last
+      // admission are bounded by max_iterations; waiting for data is
+      // bounded by wait_seconds without progress.
+      int since_admission = 0, pending = cnt[4];
+      auto wait_start = std::chrono::steady_clock::now();
+      // In the tail (every feature admitted, at most 1/16 of them running)
+      // several rounds go out per read of the counters: a round with
+      // nothing left to do is an evaluation launch that finds no tiles and
+      // a step launch whose features are all done, cheaper than the host
+      // round trip.  The burst doubles while the tail lasts, from 2 up to 16.
+      int burst = 1;
+      bool capped = false;
+      while (cnt[1] > 0 || cnt[4] > 0) {
+        const bool tail = cnt[4] == 0 && cnt[1] > 0 && cnt[1] * 16 <= nfeatures;
+        burst = tail ? std::min(2 * burst, 16) : 1;
+        for (int r = 0; r < burst && status == LMB_OK; ++r) {
+          if (cnt[1] > 0) {
+            if (++since_admission > c.max_iterations + 1) {
+              capped = true;
+              break;
+            }
+            if (!launch_eval()) { status = LMB_ERR_CUDA; break; }
+          } else {
+            const double waited = std::chrono::duration<double>(
+                std::chrono::steady_clock::now() - wait_start).count();
+            if (waited > wait_seconds) { status = LMB_ERR_TIMEOUT; break; }
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+          }
+          launch_step();
+        }
+        if (status != LMB_OK || capped) break;
+        if (cudaGetLastError() != cudaSuccess || !read_counts()) {
+          status = LMB_ERR_CUDA;
+          break;
+        }
+        if (cnt[4] < pending) {  // new features admitted
+          pending = cnt[4];
+          since_admission = 0;
+          wait_start = std::chrono::steady_clock::now();
+        }
       }
+      if (status != LMB_OK) break;
     }
-    if (status != LMB_OK) break;
     k_fit_finalize<<<(nfeatures + 127) / 128, 128, 0, st>>>(c);
     launches += 1;
     if (cudaGetLastError() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
     if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
   } while (0);
-  int overflow = 0;
-  unsigned long long work[2] = {0ull, 0ull};
-  if (status == LMB_OK) {
+  if (status == LMB_OK && !pipelined) {
     if (cudaMemcpyAsync(&overflow, c.counters + 3, sizeof(int),
                         cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(work, c.work, sizeof(work), cudaMemcpyDeviceToHost,
@@ -634,6 +791,10 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
         cudaStreamSynchronize(st) != cudaSuccess)
       status = LMB_ERR_CUDA;
   }
+  // the event timings need the last of them complete
+  if (stats && status == LMB_OK && pipelined && !ev.empty() &&
+      cudaEventSynchronize(ev.back()) != cudaSuccess)
+    status = LMB_ERR_CUDA;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     if (status == LMB_OK && ev.size() >= 2) {
@@ -641,7 +802,8 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
       cudaEventElapsedTime(&ms, ev.front(), ev.back());
       stats->total_ms = ms;
       // events: [span start] then pairs around each evaluation, then end
-      for (size_t q = 1; q + 1 < ev.size(); q += 2) {
+      const int useful = counted_evals >= 0 ? counted_evals : evals;
+      for (size_t q = 1; q + 1 < ev.size() && int(q / 2) < useful; q += 2) {
         float e = 0.f;
         cudaEventElapsedTime(&e, ev[q], ev[q + 1]);
         stats->eval_ms += e;
@@ -649,7 +811,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
     }
     stats->pixels = double(work[0]);
     stats->pixel_orders = double(work[1]);
-    stats->eval_launches = evals;
+    stats->eval_launches = counted_evals >= 0 ? counted_evals : evals;
     stats->kernel_launches = launches;
     stats->iterations = iterations;
   }
@@ -813,8 +975,10 @@ extern "C" int lmb_fit_batch_noalloc(const lmb_feature* features, int nfeatures,
   // counters must start at zero; the setup kernel writes them too
   LMB_CK(cudaMemsetAsync(reinterpret_cast<char*>(scratch) + L.counters, 0,
                          sizeof(int) * 16, as_stream(stream)));
-  return lmb_fit_batch(features, nfeatures, total_pixels, data, coords, params,
-                       n_m, wavelength, magnification, noise, nmax_cap,
-                       settings, results, scratch,
-                       size_t(LMB_FIT_NOALLOC_SCRATCH_BYTES), nullptr, stream);
+  // the synchronous round loop: the pipelined one pins host memory
+  return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
+                        n_m, wavelength, magnification, noise, nmax_cap,
+                        settings, results, scratch,
+                        size_t(LMB_FIT_NOALLOC_SCRATCH_BYTES), nullptr, stream,
+                        1, nullptr, nullptr, nullptr, 0., true);
 }

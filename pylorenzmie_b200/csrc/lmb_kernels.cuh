@@ -29,12 +29,12 @@ namespace lmb {
 // Mie coefficients: one warp per sphere.
 
 struct AbScratch {
-  zd *d1in, *d1inz, *zeta, *zetax;
-  double *d1m, *d1mx, *psi, *psix;
+  zd *d1in, *d1inz, *zeta, *zetax, *nz, *nz2;
+  double *d1m, *d1mx, *psi, *psix, *nx, *nx2;
 };
 
 __host__ __device__ inline size_t ab_scratch_bytes(int nmaxp) {
-  return size_t(nmaxp) * (4 * sizeof(zd) + 4 * sizeof(double));
+  return size_t(nmaxp) * (6 * sizeof(zd) + 6 * sizeof(double));
 }
 
 __device__ inline AbScratch carve_ab_scratch(char* base, int nmaxp) {
@@ -43,10 +43,14 @@ __device__ inline AbScratch carve_ab_scratch(char* base, int nmaxp) {
   s.d1inz = s.d1in + nmaxp;
   s.zeta = s.d1inz + nmaxp;
   s.zetax = s.zeta + nmaxp;
-  s.d1m = reinterpret_cast<double*>(s.zetax + nmaxp);
+  s.nz = s.zetax + nmaxp;
+  s.nz2 = s.nz + nmaxp;
+  s.d1m = reinterpret_cast<double*>(s.nz2 + nmaxp);
   s.d1mx = s.d1m + nmaxp;
   s.psi = s.d1mx + nmaxp;
   s.psix = s.psi + nmaxp;
+  s.nx = s.psix + nmaxp;
+  s.nx2 = s.nx + nmaxp;
   return s;
 }
 
@@ -69,10 +73,14 @@ __device__ int warp_sphere_ab(double a_p, double n_p, double k_p, double n_m,
     if (lane == 0) *nmax_out = (s.nmax >= 0 && s.nmax < (1 << 30)) ? s.nmax : 0;
     return LMB_ERR_NMAX;
   }
-  if (lane == 0) mie_d1_inside(s, w.d1in, w.d1inz);
-  if (lane == 1) mie_d1_medium(s, w.d1m, w.d1mx);
+  for (int n = 1 + lane; n <= s.nmax; n += 32)
+    mie_orders(s, n, w.nz, w.nz2, w.nx, w.nx2);
   __syncwarp();
-  if (lane == 0) mie_upward(s, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+  if (lane == 0) mie_d1_inside(s, w.nz, w.nz2, w.d1in, w.d1inz);
+  if (lane == 1) mie_d1_medium(s, w.nx, w.nx2, w.d1m, w.d1mx);
+  __syncwarp();
+  if (lane == 0)
+    mie_upward(s, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
   __syncwarp();
   for (int n = lane; n < nmaxp; n += 32) {
     if (n == 0 || n > s.nmax) {
@@ -184,6 +192,8 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     ha = sh + 5 * (L - 1) * na;
     hb = ha + na;
     w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
+    for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_medium(med, n, w.nx, w.nx2);
+    __syncwarp();
     if (lane == 0) {
       dz z1;
       z1.v = s.x[0] * s.m[0];
@@ -191,8 +201,8 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
       z1.m = (L == 1) ? mk(s.x[0], 0.) : mk(0., 0.);
       layered_d1_down(z1, s.nmax, d1c);
     } else if (lane == 1) {
-      mie_d1_medium(med, w.d1m, w.d1mx);
-      mie_upward(med, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+      mie_d1_medium(med, w.nx, w.nx2, w.d1m, w.d1mx);
+      mie_upward(med, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
     } else if (lane < 2 * L) {
       const int ii = (lane - 2) / 2 + 1, which = (lane - 2) & 1;
       const bool outer = ii == L - 1;
@@ -232,10 +242,12 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     ha = d1b + na;
     hb = ha + na;
     w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
+    for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_medium(med, n, w.nx, w.nx2);
+    __syncwarp();
     if (lane == 0) layered_core(s, d1a, ha, hb);
     if (lane == 1) {
-      mie_d1_medium(med, w.d1m, w.d1mx);
-      mie_upward(med, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+      mie_d1_medium(med, w.nx, w.nx2, w.d1m, w.d1mx);
+      mie_upward(med, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
     }
     __syncwarp();
     for (int ii = 1; ii < L; ++ii) {

@@ -440,20 +440,32 @@ LMB_HD int lm_scipy_status(int info) {
 
 // Symmetric eigen-decomposition by cyclic Jacobi rotations (n <= 6).
 // a is overwritten; w gets eigenvalues, v (row-major) eigenvectors in columns.
+// The loops run to LM_NV with the entries past n skipped, so that every
+// index is a compile-time constant once unrolled and a, v stay in registers;
+// the arithmetic and its order are those of the loops to n.
 LMB_HD void jacobi_eigh(double* a, int n, double* w, double* v) {
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j) v[i * LM_NV + j] = i == j ? 1. : 0.;
+#pragma unroll
+  for (int i = 0; i < LM_NV; ++i)
+#pragma unroll
+    for (int j = 0; j < LM_NV; ++j)
+      if (i < n && j < n) v[i * LM_NV + j] = i == j ? 1. : 0.;
   for (int sweep = 0; sweep < 30; ++sweep) {
     double off = 0., tot = 0.;
-    for (int i = 0; i < n; ++i)
-      for (int j = 0; j < n; ++j) {
+#pragma unroll
+    for (int i = 0; i < LM_NV; ++i)
+#pragma unroll
+      for (int j = 0; j < LM_NV; ++j) {
+        if (i >= n || j >= n) continue;
         const double t = a[i * LM_NV + j] * a[i * LM_NV + j];
         tot += t;
         if (i != j) off += t;
       }
     if (off <= 1e-30 * tot || off == 0.) break;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
+#pragma unroll
+    for (int p = 0; p < LM_NV - 1; ++p)
+#pragma unroll
+      for (int q = p + 1; q < LM_NV; ++q) {
+        if (q >= n) continue;
         const double apq = a[p * LM_NV + q];
         if (apq == 0.) continue;
         const double app = a[p * LM_NV + p], aqq = a[q * LM_NV + q];
@@ -461,24 +473,32 @@ LMB_HD void jacobi_eigh(double* a, int n, double* w, double* v) {
         const double t = (theta >= 0. ? 1. : -1.) /
                          (fabs(theta) + sqrt(theta * theta + 1.));
         const double c = 1. / sqrt(t * t + 1.), sn = t * c;
-        for (int k = 0; k < n; ++k) {
+#pragma unroll
+        for (int k = 0; k < LM_NV; ++k) {
+          if (k >= n) continue;
           const double akp = a[k * LM_NV + p], akq = a[k * LM_NV + q];
           a[k * LM_NV + p] = c * akp - sn * akq;
           a[k * LM_NV + q] = sn * akp + c * akq;
         }
-        for (int k = 0; k < n; ++k) {
+#pragma unroll
+        for (int k = 0; k < LM_NV; ++k) {
+          if (k >= n) continue;
           const double apk = a[p * LM_NV + k], aqk = a[q * LM_NV + k];
           a[p * LM_NV + k] = c * apk - sn * aqk;
           a[q * LM_NV + k] = sn * apk + c * aqk;
         }
-        for (int k = 0; k < n; ++k) {
+#pragma unroll
+        for (int k = 0; k < LM_NV; ++k) {
+          if (k >= n) continue;
           const double vkp = v[k * LM_NV + p], vkq = v[k * LM_NV + q];
           v[k * LM_NV + p] = c * vkp - sn * vkq;
           v[k * LM_NV + q] = sn * vkp + c * vkq;
         }
       }
   }
-  for (int i = 0; i < n; ++i) w[i] = a[i * LM_NV + i];
+#pragma unroll
+  for (int i = 0; i < LM_NV; ++i)
+    if (i < n) w[i] = a[i * LM_NV + i];
 }
 
 // redchi and uncertainties of Optimizer._statistics (analysis/Optimizer.py:
@@ -493,14 +513,20 @@ LMB_HD void lm_statistics(const LMState& s, long long npix, double* redchi,
   for (int i = 0; i < LM_NV * LM_NV; ++i) a[i] = s.jtj[i];
   jacobi_eigh(a, n, w, v);
   double wmax = 0.;
-  for (int i = 0; i < n; ++i) if (w[i] > wmax) wmax = w[i];
+#pragma unroll
+  for (int i = 0; i < LM_NV; ++i)
+    if (i < n && w[i] > wmax) wmax = w[i];
   const double big = double(npix > n ? npix : n);
   const double thr = 2.220446049250313e-16 * big;
   const double thr2 = thr * thr * wmax;
-  for (int i = 0; i < n; ++i) {
+#pragma unroll
+  for (int i = 0; i < LM_NV; ++i) {
+    if (i >= n) continue;
     double c = 0.;
-    for (int k = 0; k < n; ++k)
-      if (w[k] > thr2 && w[k] > 0.) c += v[i * LM_NV + k] * v[i * LM_NV + k] / w[k];
+#pragma unroll
+    for (int k = 0; k < LM_NV; ++k)
+      if (k < n && w[k] > thr2 && w[k] > 0.)
+        c += v[i * LM_NV + k] * v[i * LM_NV + k] / w[k];
     dp[i] = sqrt(*redchi * c);
   }
 }

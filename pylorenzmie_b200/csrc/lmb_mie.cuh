@@ -13,8 +13,11 @@
 // n_max is treated as locally constant, as the reference's JAX Jacobian does
 // (theory/jaxLorenzMie.py:354-361).
 //
-// The phases are split so that a warp can run the two downward recurrences
-// on two lanes and then compute a_n, b_n for all n in parallel.
+// The phases are split so that a warp forms the per-order quotients n/z,
+// n/z^2, n/x, n/x^2 on all lanes, runs the two downward recurrences on two
+// lanes and then computes a_n, b_n for all n in parallel.  On the
+// recurrences' dependent chains each complex reciprocal is conj(w)/|w|^2
+// with one reciprocal (recip).
 #pragma once
 
 #include "lmb_math.cuh"
@@ -60,45 +63,61 @@ LMB_HD MieScalars mie_setup(double a_p, double n_p, double k_p, double n_m,
   return s;
 }
 
-// D1(z) for z = m x, n = nmax..0, with dD1/dz; arrays of nmax+1 entries.
-LMB_HD void mie_d1_inside(const MieScalars& s, zd* d1, zd* d1z) {
+// Per-order quotients of the recurrences for order n (1 <= n <= nmax):
+// nz = n/z, nz2 = n/z^2 with z = m x (inside), nx = n/x, nx2 = n/x^2
+// (medium).  Off the recurrences' chains, so a warp forms them in parallel.
+LMB_HD void mie_orders(const MieScalars& s, int n, zd* nz, zd* nz2, double* nx,
+                       double* nx2) {
   const zd z = s.x * s.m;
   const zd z2 = z * z;
+  nz[n] = double(n) / z;
+  nz2[n] = double(n) / z2;
+  nx[n] = double(n) / s.x;
+  nx2[n] = nx[n] / s.x;
+}
+
+// The medium's quotients only (nx, nx2), for the multilayer medium.
+LMB_HD void mie_orders_medium(const MieScalars& s, int n, double* nx,
+                              double* nx2) {
+  nx[n] = double(n) / s.x;
+  nx2[n] = nx[n] / s.x;
+}
+
+// D1(z) for z = m x, n = nmax..0, with dD1/dz; arrays of nmax+1 entries.
+LMB_HD void mie_d1_inside(const MieScalars& s, const zd* nz, const zd* nz2,
+                          zd* d1, zd* d1z) {
   zd d = mk(0., 0.), dz = mk(0., 0.);
   d1[s.nmax] = d;
   d1z[s.nmax] = dz;
   for (int n = s.nmax; n > 0; --n) {
-    const zd nz = double(n) / z;
-    const zd nz2 = double(n) / z2;
-    const zd inv = 1. / (d + nz);
-    const zd dw = dz - nz2;
-    d = nz - inv;
-    dz = (inv * inv) * dw - nz2;
+    const zd inv = recip(d + nz[n]);
+    const zd dw = dz - nz2[n];
+    d = nz[n] - inv;
+    dz = (inv * inv) * dw - nz2[n];
     d1[n - 1] = d;
     d1z[n - 1] = dz;
   }
 }
 
 // D1(x) in the medium (real because x is real), with dD1/dx.
-LMB_HD void mie_d1_medium(const MieScalars& s, double* d1, double* d1x) {
-  const double x = s.x;
+LMB_HD void mie_d1_medium(const MieScalars& s, const double* nx,
+                          const double* nx2, double* d1, double* d1x) {
   double d = 0., dx = 0.;
   d1[s.nmax] = d;
   d1x[s.nmax] = dx;
   for (int n = s.nmax; n > 0; --n) {
-    const double nx = double(n) / x;
-    const double nx2 = nx / x;
-    const double inv = 1. / (d + nx);
-    const double dw = dx - nx2;
-    d = nx - inv;
-    dx = inv * inv * dw - nx2;
+    const double inv = rcp_d(d + nx[n]);
+    const double dw = dx - nx2[n];
+    d = nx[n] - inv;
+    dx = inv * inv * dw - nx2[n];
     d1[n - 1] = d;
     d1x[n - 1] = dx;
   }
 }
 
 // Upward psi (real), zeta, with d/dx; needs the medium D1.
-LMB_HD void mie_upward(const MieScalars& s, const double* d1, const double* d1x,
+LMB_HD void mie_upward(const MieScalars& s, const double* nxs,
+                       const double* nx2s, const double* d1, const double* d1x,
                        double* psi, double* psix, zd* zeta, zd* zetax) {
   const double x = s.x;
   double sx, cx;
@@ -120,8 +139,8 @@ LMB_HD void mie_upward(const MieScalars& s, const double* d1, const double* d1x,
   zeta[0] = zt;
   zetax[0] = ztx;
   for (int n = 1; n <= s.nmax; ++n) {
-    const double nx = double(n) / x;
-    const double nx2 = nx / x;
+    const double nx = nxs[n];
+    const double nx2 = nx2s[n];
     const double t1 = nx - d1[n - 1];
     const double t1x = -nx2 - d1x[n - 1];
     const zd t3 = nx - d3;
@@ -134,7 +153,7 @@ LMB_HD void mie_upward(const MieScalars& s, const double* d1, const double* d1x,
     const zd t13x = t1x * t3 + t1 * t3x;
     const zd pzn = pz * t13;
     const zd pznx = pzx * t13 + pz * t13x;
-    const zd ipz = 1. / pzn;
+    const zd ipz = recip(pzn);
     d3 = d1[n] + mul_i(ipz);
     d3x = d1x[n] - mul_i(pznx * (ipz * ipz));
     p = pn;
@@ -170,16 +189,18 @@ LMB_HD void mie_coefficient(const MieScalars& s, int n, const zd* d1in,
   const zd zex = zetax[n], ze1x = zetax[n - 1];
 
   // a_n, Eq. (5): fac = Ha/m + n/x
-  const zd im = 1. / m;
+  const zd im = recip(m);
   const zd fa = ha * im + nx;
   const zd numa = fa * ps - ps1;
   const zd dena = fa * ze - ze1;
-  const zd a = numa / dena;
+  const zd ida = recip(dena);
+  const zd a = numa * ida;
   // b_n, Eq. (6): fac = Hb m + n/x
   const zd fb = ha * m + nx;
   const zd numb = fb * ps - ps1;
   const zd denb = fb * ze - ze1;
-  const zd b = numb / denb;
+  const zd idb = recip(denb);
+  const zd b = numb * idb;
   out[0] = a;
   out[1] = b;
   if (dout == 0) return;
@@ -188,8 +209,6 @@ LMB_HD void mie_coefficient(const MieScalars& s, int n, const zd* d1in,
   const zd fa_m = ha_m * im - ha * (im * im);
   const zd fb_x = ha_x * m - nx2;
   const zd fb_m = ha_m * m + ha;
-  const zd ida = 1. / dena;
-  const zd idb = 1. / denb;
   const zd a_x = ((fa_x * ps + fa * psx - ps1x) - a * (fa_x * ze + fa * zex - ze1x)) * ida;
   const zd a_m = (fa_m * ps - a * (fa_m * ze)) * ida;
   const zd b_x = ((fb_x * ps + fb * psx - ps1x) - b * (fb_x * ze + fb * zex - ze1x)) * idb;

@@ -30,10 +30,14 @@ API int h_sphere_ab(double a_p, double n_p, double k_p, double n_m, double lam,
       zetax(s.nmax + 1);
   std::vector<double> d1m(s.nmax + 1), d1mx(s.nmax + 1), psi(s.nmax + 1),
       psix(s.nmax + 1);
-  mie_d1_inside(s, d1in.data(), d1inz.data());
-  mie_d1_medium(s, d1m.data(), d1mx.data());
-  mie_upward(s, d1m.data(), d1mx.data(), psi.data(), psix.data(), zeta.data(),
-             zetax.data());
+  std::vector<zd> nz(s.nmax + 1), nz2(s.nmax + 1);
+  std::vector<double> nx(s.nmax + 1), nx2(s.nmax + 1);
+  for (int n = 1; n <= s.nmax; ++n)
+    mie_orders(s, n, nz.data(), nz2.data(), nx.data(), nx2.data());
+  mie_d1_inside(s, nz.data(), nz2.data(), d1in.data(), d1inz.data());
+  mie_d1_medium(s, nx.data(), nx2.data(), d1m.data(), d1mx.data());
+  mie_upward(s, nx.data(), nx2.data(), d1m.data(), d1mx.data(), psi.data(),
+             psix.data(), zeta.data(), zetax.data());
   memset(ab, 0, sizeof(double) * 4 * (cap + 1));
   if (dab) memset(dab, 0, sizeof(double) * 8 * (cap + 1));
   for (int n = 1; n <= s.nmax; ++n) {
@@ -113,9 +117,11 @@ static int layered_ab_impl(const double* radii, const double* idx, int L,
   med.nmax = nm;
   std::vector<double> d1m(nm + 1), d1mx(nm + 1), psi(nm + 1), psix(nm + 1);
   std::vector<zd> zeta(nm + 1), zetax(nm + 1);
-  mie_d1_medium(med, d1m.data(), d1mx.data());
-  mie_upward(med, d1m.data(), d1mx.data(), psi.data(), psix.data(), zeta.data(),
-             zetax.data());
+  std::vector<double> nx(nm + 1), nx2(nm + 1);
+  for (int n = 1; n <= nm; ++n) mie_orders_medium(med, n, nx.data(), nx2.data());
+  mie_d1_medium(med, nx.data(), nx2.data(), d1m.data(), d1mx.data());
+  mie_upward(med, nx.data(), nx2.data(), d1m.data(), d1mx.data(), psi.data(),
+             psix.data(), zeta.data(), zetax.data());
   memset(ab, 0, sizeof(double) * 4 * (cap + 1));
   if (dab) memset(dab, 0, sizeof(double) * 8 * (cap + 1));
   for (int n = 1; n <= nm; ++n) {
