@@ -194,24 +194,29 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
     for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_medium(med, n, w.nx, w.nx2);
     __syncwarp();
-    if (lane == 0) {
-      dz z1;
-      z1.v = s.x[0] * s.m[0];
-      z1.s = z1.v;
-      z1.m = (L == 1) ? mk(s.x[0], 0.) : mk(0., 0.);
-      layered_d1_down(z1, s.nmax, d1c);
-    } else if (lane == 1) {
+    if (lane == 1) {
       mie_d1_medium(med, w.nx, w.nx2, w.d1m, w.d1mx);
       mie_upward(med, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
     } else if (lane < 2 * L) {
-      const int ii = (lane - 2) / 2 + 1, which = (lane - 2) & 1;
-      const bool outer = ii == L - 1;
+      // the core (lane 0) and each shell's two arguments (lanes 2..2L-1):
+      // one code path, so these recurrences run in step across the lanes
       dz z;
-      const double xx = which == 0 ? s.x[ii] : s.x[ii - 1];
-      z.v = xx * s.m[ii];
-      z.s = z.v;
-      z.m = outer ? mk(xx, 0.) : mk(0., 0.);
-      layered_d1_down(z, s.nmax, sh + (5 * (ii - 1) + which) * na);
+      dz* out;
+      if (lane == 0) {
+        z.v = s.x[0] * s.m[0];
+        z.s = z.v;
+        z.m = (L == 1) ? mk(s.x[0], 0.) : mk(0., 0.);
+        out = d1c;
+      } else {
+        const int ii = (lane - 2) / 2 + 1, which = (lane - 2) & 1;
+        const bool outer = ii == L - 1;
+        const double xx = which == 0 ? s.x[ii] : s.x[ii - 1];
+        z.v = xx * s.m[ii];
+        z.s = z.v;
+        z.m = outer ? mk(xx, 0.) : mk(0., 0.);
+        out = sh + (5 * (ii - 1) + which) * na;
+      }
+      layered_d1_down(z, s.nmax, out);
     }
     __syncwarp();
     if (lane >= 1 && lane < L) {

@@ -44,7 +44,7 @@ LMB_HD dz operator*(zd c, dz a) { return dz{c * a.v, c * a.s, c * a.m}; }
 LMB_HD dz operator*(double c, dz a) { return dz{c * a.v, c * a.s, c * a.m}; }
 LMB_HD dz operator+(dz a, double c) { return dz{a.v + c, a.s, a.m}; }
 LMB_HD dz dinv(dz a) {
-  const zd i = 1. / a.v;
+  const zd i = recip(a.v);
   const zd i2 = -(i * i);
   return dz{i, i2 * a.s, i2 * a.m};
 }
@@ -106,8 +106,9 @@ LMB_HD LayeredScalars layered_setup(const double* radii, const double* idx,
 // zero-start downward D1 at z from n_max+1 into d[0..nmax] (dual)
 LMB_HD void layered_d1_down(dz z, int nmax, dz* d) {
   dz cur = dconst(mk(0., 0.));
+  const dz iz = dinv(z);  // n / z = n * (1/z), the loop's invariant
   for (int n = nmax + 1; n > 0; --n) {
-    const dz nz = double(n) / z;
+    const dz nz = double(n) * iz;
     cur = nz - dinv(cur + nz);
     if (n - 1 <= nmax) d[n - 1] = cur;
   }
@@ -168,9 +169,10 @@ LMB_HD void layered_shell_rec(const LayeredScalars& s, const ShellSetup& h,
   dz pzb = 0.5 * (1. - dexpi(2., h.z2));
   dz d3a = dconst(ii1), d3b = dconst(ii1);
   dz q = (dexpi(-2., h.z2) + (-1.)) / (dexpi(-2., h.z1) + (-1.));
+  const dz iz1 = dinv(h.z1), iz2 = dinv(h.z2);
   for (int n = 1; n <= s.nmax; ++n) {
     const double fn = double(n);
-    const dz nz1 = fn / h.z1, nz2 = fn / h.z2;
+    const dz nz1 = fn * iz1, nz2 = fn * iz2;
     const dz d3a_prev = d3a, d3b_prev = d3b;
     pza = pza * ((nz1 - d1a[n - 1]) * (nz1 - d3a_prev));
     pzb = pzb * ((nz2 - d1b[n - 1]) * (nz2 - d3b_prev));
@@ -219,9 +221,10 @@ LMB_HD void layered_shell_up(const LayeredScalars& s, int ii, const dz* d1a,
   dz q = (dexpi(-2., h.z2) + (-1.)) / (dexpi(-2., h.z1) + (-1.));
   ha[0] = dconst(mk(0., 0.));
   hb[0] = dconst(mk(0., 0.));
+  const dz iz1 = dinv(h.z1), iz2 = dinv(h.z2);
   for (int n = 1; n <= s.nmax; ++n) {
     const double fn = double(n);
-    const dz nz1 = fn / h.z1, nz2 = fn / h.z2;
+    const dz nz1 = fn * iz1, nz2 = fn * iz2;
     const dz d3a_prev = d3a, d3b_prev = d3b;
     pza = pza * ((nz1 - d1a[n - 1]) * (nz1 - d3a_prev));
     pzb = pzb * ((nz2 - d1b[n - 1]) * (nz2 - d3b_prev));

@@ -87,13 +87,18 @@ LMB_HD double rcp_d(double x) {
 #endif
 }
 
-// 1/b = conj(b) / |b|^2 with one reciprocal: for the denominators of the
-// recurrences, whose magnitudes stay far inside 1e-150..1e150, where
-// |b|^2 neither overflows nor underflows (Smith's scaling, above, is for
-// arbitrary operands and costs two dependent divisions).
+// 1/b.  Where |re| + |im| lies in 1e-150..1e150, so that |b|^2 neither
+// overflows nor underflows, as conj(b) / |b|^2 with one reciprocal; else
+// (and for NaN or infinite b) by Smith's scaled division, above, which costs
+// two dependent divisions.  The recurrences' denominators are almost always
+// in the fast range.
 LMB_HD cplx<double> recip(cplx<double> b) {
-  const double r = rcp_d(b.re * b.re + b.im * b.im);
-  return mk(b.re * r, -b.im * r);
+  const double a = fabs(b.re) + fabs(b.im);
+  if (a > 1e-150 && a < 1e150) {
+    const double r = rcp_d(b.re * b.re + b.im * b.im);
+    return mk(b.re * r, -b.im * r);
+  }
+  return mk(1., 0.) / b;
 }
 template <typename T>
 LMB_HD cplx<T> operator/(cplx<T> a, T s) { return mk(a.re / s, a.im / s); }
