@@ -267,11 +267,15 @@ typedef struct lmb_fit_result {
 /*
  * Optional measurements of one lmb_fit_batch call (host struct).  When
  * requested, the call records CUDA events around each evaluation launch on
- * its stream and counts the work done on the device.
+ * its stream and counts the work done on the device.  Evaluation launches
+ * queued after the last productive round (they find no work) are not
+ * counted in eval_launches and eval_ms.
  */
 typedef struct lmb_fit_stats {
   double eval_ms;        /* summed device time of the evaluation launches */
-  double total_ms;       /* device time from the first to the last launch */
+  double total_ms;       /* device time from the first launch to the end of
+                            the last evaluation that found work (to the last
+                            launch with streamed admission) */
   double pixels;         /* pixels evaluated, summed over launches */
   double pixel_orders;   /* pixels x partial-wave orders evaluated */
   int eval_launches;     /* evaluation kernel launches */

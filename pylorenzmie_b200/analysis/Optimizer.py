@@ -330,8 +330,9 @@ class Optimizer(LMObject):
                   list of Sphere or LayeredSphere start values
         autotune: time the evaluation kernel's launch shapes on the first
                   batch (default: when it has 64 features or more)
-        depth   : batches in flight (pinned buffers); 2 overlaps the host
-                  work of one batch with the fit of the previous
+        depth   : fits running at once (default 2, which keeps the GPU
+                  busy); the next batch is converted and copied while they
+                  run
         '''
         if not self._device_fit_ok() and not (
                 set(self.variables) <= set(PARAM_KEYS)):

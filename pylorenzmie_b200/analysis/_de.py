@@ -83,138 +83,209 @@ def _integers(rng, high, size):
     return rng.randint(high, size=size, dtype='int64')
 
 
-class Population:
-    '''One search's state: population (N, P) in [0, 1], energies (N,).
+class Populations:
+    '''Searches with the same population shape (N candidates, P
+    parameters), stepped together: population (S, N, P) in [0, 1],
+    energies (S, N).  Each search draws from its own generator in scipy's
+    order; the arithmetic runs once for all of them (elementwise the same
+    operations, so every value is the one a lone search computes).
 
-    request() gives the parameters (N, P) the search needs evaluated next;
-    receive(energies) takes their values and advances it.  ``done`` is set
-    with ``result`` when it has converged or reached maxiter.'''
+    request(live) gives {search: parameters (N, P)} for the searches in
+    ``live``; receive({search: energies (N,)}) advances them.  ``done[s]``
+    is set, with ``results[s]``, when search s has converged or reached
+    maxiter.'''
 
-    def __init__(self, bounds, popsize=15, seed=None, settings=None):
-        s = dict(_DEFAULTS)
-        s.update(settings or {})
-        limits = np.array(bounds, dtype=float).T
-        if limits.shape[0] != 2 or not np.all(np.isfinite(limits)):
-            raise ValueError('bounds should be a sequence containing finite '
-                             'real valued (min, max) pairs for each value '
-                             'in x')
-        self.tol, self.atol = s['tol'], s['atol']
-        self.maxiter = 1000 if s['maxiter'] is None else int(s['maxiter'])
-        mutation = s['mutation']
-        self.scale = mutation
-        self.dither = None
-        if hasattr(mutation, '__iter__') and len(mutation) > 1:
-            self.dither = sorted([mutation[0], mutation[1]])
-        self.cr = s['recombination']
-        self.limits = limits
-        self._mid = 0.5 * (limits[0] + limits[1])
-        self._span = np.fabs(limits[0] - limits[1])
-        self.nparam = limits.shape[1]
-        self.rng = _generator(seed)
-        fixed = np.count_nonzero(limits[0] == limits[1])
-        self.N = max(5, popsize * max(1, self.nparam - fixed))
-        # latin hypercube: one draw per cell, one permutation per column
-        rng = self.rng
-        seg = 1.0 / self.N
-        samples = (seg * rng.uniform(size=(self.N, self.nparam)) +
-                   np.linspace(0., 1., self.N, endpoint=False)[:, None])
-        self.population = np.zeros_like(samples)
-        for j in range(self.nparam):
-            order = rng.permutation(range(self.N))
-            self.population[:, j] = samples[order, j]
-        self.energies = np.full(self.N, np.inf)
-        self._index = np.arange(self.N)
-        self._first = np.empty((self.N, 3), dtype=self._index.dtype)
-        self._trial = None
-        self.nfev = 0
-        self.nit = 0
-        self.done = False
-        self.result = None
+    def __init__(self, problems):
+        S = len(problems)
+        self.rngs, dither, scale, cr, tol, atol, maxiter = [], [], [], [], [], [], []
+        mids, spans, pops = [], [], []
+        for pr in problems:
+            s = dict(_DEFAULTS)
+            s.update(pr['settings'] or {})
+            limits = np.array(pr['bounds'], dtype=float).T
+            if limits.shape[0] != 2 or not np.all(np.isfinite(limits)):
+                raise ValueError('bounds should be a sequence containing '
+                                 'finite real valued (min, max) pairs for '
+                                 'each value in x')
+            mutation = s['mutation']
+            d = None
+            if hasattr(mutation, '__iter__') and len(mutation) > 1:
+                d = sorted([mutation[0], mutation[1]])
+            dither.append(d)
+            scale.append(np.nan if d is not None else float(mutation))
+            cr.append(s['recombination'])
+            tol.append(s['tol'])
+            atol.append(s['atol'])
+            maxiter.append(1000 if s['maxiter'] is None else int(s['maxiter']))
+            mids.append(0.5 * (limits[0] + limits[1]))
+            spans.append(np.fabs(limits[0] - limits[1]))
+            nparam = limits.shape[1]
+            fixed = np.count_nonzero(limits[0] == limits[1])
+            N = max(5, pr['popsize'] * max(1, nparam - fixed))
+            rng = _generator(pr['seed'])
+            self.rngs.append(rng)
+            # latin hypercube: one draw per cell, one permutation per column
+            seg = 1.0 / N
+            samples = (seg * rng.uniform(size=(N, nparam)) +
+                       np.linspace(0., 1., N, endpoint=False)[:, None])
+            pop = np.zeros_like(samples)
+            for j in range(nparam):
+                order = rng.permutation(range(N))
+                pop[:, j] = samples[order, j]
+            pops.append(pop)
+        self.S, self.N, self.P = S, pops[0].shape[0], pops[0].shape[1]
+        self.dither = dither
+        self.scale = np.array(scale, dtype=float)
+        self.cr = np.array(cr, dtype=float)
+        self.tol = np.array(tol, dtype=float)
+        self.atol = np.array(atol, dtype=float)
+        self.maxiter = np.array(maxiter)
+        self.mid = np.array(mids)[:, None, :]
+        self.span = np.array(spans)[:, None, :]
+        self.pop = np.array(pops)
+        self.energies = np.full((S, self.N), np.inf)
+        self.trial = np.zeros_like(self.pop)
+        self.index = [np.arange(self.N) for _ in range(S)]
+        self.trialed = np.zeros(S, dtype=bool)   # last request was a trial
+        self.nfev = np.zeros(S, dtype=int)
+        self.nit = np.zeros(S, dtype=int)
+        self.done = np.zeros(S, dtype=bool)
+        self.results = [None] * S
 
-    def parameters(self, unit):
-        return self._mid + (unit - 0.5) * self._span
+    def parameters(self, s, unit):
+        return self.mid[s, 0] + (unit - 0.5) * self.span[s, 0]
 
-    def request(self):
-        if np.all(np.isinf(self.energies)):
-            self._trial = None           # (re)evaluate the population
-            return self.parameters(self.population)
-        rng = self.rng
-        if self.dither is not None:
-            self.scale = rng.uniform(self.dither[0], self.dither[1])
-        # mutation, best1: for each candidate the first two of a fresh
-        # shuffle of the kept permutation other than the candidate itself
-        shuffle, index, first = rng.shuffle, self._index, self._first
-        for c in range(self.N):
-            shuffle(index)
-            first[c] = index[:3]
-        c = np.arange(self.N)
-        f0, f1, f2 = first[:, 0], first[:, 1], first[:, 2]
+    def request(self, live):
+        live = np.asarray(live)
+        inf_all = np.all(np.isinf(self.energies[live]), axis=1)
+        out = {}
+        for s in live[inf_all]:               # (re)evaluate the population
+            self.trialed[s] = False
+            out[s] = self.parameters(s, self.pop[s])
+        T = live[~inf_all]
+        if not len(T):
+            return out
+        N, P = self.N, self.P
+        first = np.empty((len(T), N, 3), dtype=self.index[0].dtype)
+        fill = np.empty((len(T), N), dtype='int64')
+        cross = np.empty((len(T), N, P), dtype=bool)
+        for i, s in enumerate(T):
+            rng = self.rngs[s]
+            if self.dither[s] is not None:
+                self.scale[s] = rng.uniform(self.dither[s][0],
+                                            self.dither[s][1])
+            # mutation, best1: for each candidate the first two of a fresh
+            # shuffle of the kept permutation other than the candidate
+            shuffle, index, fs = rng.shuffle, self.index[s], first[i]
+            for c in range(N):
+                shuffle(index)
+                fs[c] = index[:3]
+            fill[i] = _integers(rng, P, N)
+            cross[i] = rng.uniform(size=(N, P)) < self.cr[s]
+        c = np.arange(N)
+        f0, f1, f2 = first[..., 0], first[..., 1], first[..., 2]
         r0 = np.where(f0 == c, f1, f0)
         r1 = np.where((f0 == c) | (f1 == c), f2, f1)
-        pop = self.population
-        bprime = pop[0] + self.scale * (pop[r0] - pop[r1])
-        fill = _integers(rng, self.nparam, self.N)
-        cross = rng.uniform(size=(self.N, self.nparam)) < self.cr
-        cross[c, fill] = True
+        pop = self.pop[T]
+        b0 = np.take_along_axis(pop, r0[..., None], axis=1)
+        b1 = np.take_along_axis(pop, r1[..., None], axis=1)
+        bprime = pop[:, :1, :] + self.scale[T][:, None, None] * (b0 - b1)
+        cross[np.arange(len(T))[:, None], c[None, :], fill] = True
         trial = np.where(cross, bprime, pop)
-        out = (trial > 1) | (trial < 0)
-        n = np.count_nonzero(out)
-        if n:
-            trial[out] = rng.uniform(size=n)
-        self._trial = trial
-        return self.parameters(trial)
+        outside = (trial > 1) | (trial < 0)
+        for i, s in enumerate(T):
+            n = np.count_nonzero(outside[i])
+            if n:
+                trial[i][outside[i]] = self.rngs[s].uniform(size=n)
+        self.trial[T] = trial
+        self.trialed[T] = True
+        params = self.mid[T] + (trial - 0.5) * self.span[T]
+        for i, s in enumerate(T):
+            out[s] = params[i]
+        return out
 
-    def receive(self, energies):
-        energies = np.asarray(energies, dtype=float).reshape(-1)
-        self.nfev += 1
-        if self._trial is None:
-            self.energies = energies.copy()
-            self._promote()
+    def receive(self, values):
+        keys = np.array(sorted(values))
+        E = np.array([np.asarray(values[s], dtype=float).reshape(-1)
+                      for s in keys])
+        self.nfev[keys] += 1
+        fresh = ~self.trialed[keys]
+        R = keys[fresh]                      # population (re)evaluated
+        if len(R):
+            self.energies[R] = E[fresh]
+            self._promote(R)
+        T = keys[~fresh]
+        if not len(T):
             return
-        keep = energies <= self.energies
-        self.population = np.where(keep[:, None], self._trial,
-                                   self.population)
-        self.energies = np.where(keep, energies, self.energies)
-        self._promote()
-        self._trial = None
-        self.nit += 1
-        if self._converged():
-            self._finish(_SUCCESS, True)
-        elif self.nit >= self.maxiter:
-            self._finish(_MAXITER, False)
+        Et = E[~fresh]
+        keep = Et <= self.energies[T]
+        self.pop[T] = np.where(keep[..., None], self.trial[T], self.pop[T])
+        self.energies[T] = np.where(keep, Et, self.energies[T])
+        self._promote(T)
+        self.trialed[T] = False
+        self.nit[T] += 1
+        e = self.energies[T]
+        conv = ~np.any(np.isinf(e), axis=1) & (
+            np.std(e, axis=1) <= self.atol[T] + self.tol[T] * np.abs(
+                np.mean(e, axis=1)))
+        for i, s in enumerate(T):
+            if conv[i]:
+                self._finish(s, _SUCCESS, True)
+            elif self.nit[s] >= self.maxiter[s]:
+                self._finish(s, _MAXITER, False)
 
-    def _promote(self):
-        best = int(np.argmin(self.energies))
-        self.energies[[0, best]] = self.energies[[best, 0]]
-        self.population[[0, best], :] = self.population[[best, 0], :]
+    def _promote(self, rows):
+        best = np.argmin(self.energies[rows], axis=1)
+        e0 = self.energies[rows, 0].copy()
+        self.energies[rows, 0] = self.energies[rows, best]
+        self.energies[rows, best] = e0
+        p0 = self.pop[rows, 0, :].copy()
+        self.pop[rows, 0, :] = self.pop[rows, best, :]
+        self.pop[rows, best, :] = p0
 
-    def _converged(self):
-        e = self.energies
-        if np.any(np.isinf(e)):
-            return False
-        return np.std(e) <= self.atol + self.tol * np.abs(np.mean(e))
+    def _finish(self, s, message, success):
+        self.done[s] = True
+        self.results[s] = OptimizeResult(
+            x=self.parameters(s, self.pop[s, 0]), fun=self.energies[s, 0],
+            nfev=int(self.nfev[s]), nit=int(self.nit[s]), message=message,
+            success=success, population=self.parameters(s, self.pop[s]),
+            population_energies=self.energies[s].copy())
 
-    def _finish(self, message, success):
-        self.done = True
-        self.result = OptimizeResult(
-            x=self.parameters(self.population[0]), fun=self.energies[0],
-            nfev=self.nfev, nit=self.nit, message=message, success=success,
-            population=self.parameters(self.population),
-            population_energies=self.energies)
+
+def _shape(problem):
+    limits = np.array(problem['bounds'], dtype=float).T
+    nparam = limits.shape[1] if limits.ndim == 2 else 0
+    fixed = np.count_nonzero(limits[0] == limits[1]) if nparam else 0
+    return max(5, problem['popsize'] * max(1, nparam - fixed)), nparam
 
 
 def run_populations(problems, evaluate):
     '''Every problem (dict with bounds, popsize, seed, settings) searched
     with the others: each round, the parameters every unfinished search
     needs go to ``evaluate({index: x})`` at once (x as a vectorized scipy
-    objective receives it, (P, N)); returns the OptimizeResults in order.'''
-    searches = [Population(p['bounds'], p['popsize'], p['seed'],
-                           p['settings']) for p in problems]
-    live = list(range(len(searches)))
-    while live:
-        batch = {i: searches[i].request().T for i in live}
+    objective receives it, (P, N)); returns the OptimizeResults in order.
+    Searches of the same population shape share arrays (Populations).'''
+    groups = {}
+    for i, p in enumerate(problems):
+        groups.setdefault(_shape(p), []).append(i)
+    parts = [(idx, Populations([problems[i] for i in idx]))
+             for idx in groups.values()]
+    while True:
+        batch, owners = {}, []
+        for idx, g in parts:
+            live = np.flatnonzero(~g.done)
+            if len(live):
+                req = g.request(live)
+                for s, x in req.items():
+                    batch[idx[s]] = x.T
+                owners.append((idx, g, list(req)))
+        if not batch:
+            break
         values = evaluate(batch)
-        for i in live:
-            searches[i].receive(values[i])
-        live = [i for i in live if not searches[i].done]
-    return [s.result for s in searches]
+        for idx, g, members in owners:
+            g.receive({s: values[idx[s]] for s in members})
+    results = [None] * len(problems)
+    for idx, g in parts:
+        for s, i in enumerate(idx):
+            results[i] = g.results[s]
+    return results

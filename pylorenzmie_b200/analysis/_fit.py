@@ -570,19 +570,21 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
     (B, 6), results record array, npix (B,)) per batch.
 
     ``batches`` yields (items, starts, layers): items as for fit_items.
-    While the device fits batch k (driven by a worker thread, on the fit
-    stream), the caller's thread converts batch k+1 into the next of
-    ``depth`` pinned buffers and copies it on the copy stream; the fit of
-    k+1 waits for that copy on the device, not on the host, and runs on a
-    stream of its own (consecutive fits may overlap on the GPU).  A pinned
-    buffer is rewritten only after its previous copy has completed.'''
+    Up to ``depth`` fits run at once, each driven by a worker thread on a
+    stream of its own (consecutive fits overlap on the GPU).  The caller's
+    thread converts the next batch into one of depth + 1 pinned buffers and
+    copies it on the copy stream before it waits for the oldest fit, so
+    that batch's data is on the device when a fit slot frees; its fit waits
+    for that copy on the device, not on the host.  A pinned buffer is
+    rewritten only after its previous copy has completed.'''
     from collections import deque
     dev = get_device(device)
     _, s_copy = _fit_streams(dev)
-    while len(_stream_staging) < depth:
+    nstage = depth + 1
+    while len(_stream_staging) < nstage:
         _stream_staging.append(_Staging())
     pending = deque()          # (future, copy-done event)
-    done_events = [None] * depth
+    done_events = [None] * nstage
     tile_config = None
     k = 0
     try:
@@ -606,8 +608,8 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
                     tile_config = _tuner.tune(packed, starts, instrument,
                                               variables, nmax_cap, layers,
                                               dev)
-            slot = k % depth
-            s_fit = _stream_fit_stream(dev, slot)
+            slot = k % nstage
+            s_fit = _stream_fit_stream(dev, k % depth)
             if done_events[slot] is not None:
                 done_events[slot].synchronize()  # its last copy has landed
             buf, offs, nbytes = stage(packed, starts, _stream_staging[slot])
@@ -619,13 +621,14 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
             for v in views:
                 if v is not None:
                     v.record_stream(s_fit)
+            # this batch's data is on its way: now wait for a fit slot
+            while len(pending) >= depth:
+                yield _collect(pending.popleft())
             pending.append((_stream_worker(depth).submit(
                 _fit_after, s_fit, ev, views, B, packed.total, instrument,
                 variables, settings, nmax_cap, starts, tile_config, layers),
                 npix))
             k += 1
-            while len(pending) >= depth:
-                yield _collect(pending.popleft())
         while pending:
             yield _collect(pending.popleft())
     finally:

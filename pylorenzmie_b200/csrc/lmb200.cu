@@ -791,18 +791,21 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
         cudaStreamSynchronize(st) != cudaSuccess)
       status = LMB_ERR_CUDA;
   }
-  // the event timings need the last of them complete
-  if (stats && status == LMB_OK && pipelined && !ev.empty() &&
-      cudaEventSynchronize(ev.back()) != cudaSuccess)
-    status = LMB_ERR_CUDA;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
+    // events: [span start] then pairs around each evaluation, then end.
+    // The pipelined loop's productive evaluations ended before the last
+    // counter read, so their events are complete and the call need not
+    // wait for the rounds queued after them or for k_fit_finalize: its
+    // span ends with the last productive evaluation.
+    const int useful = counted_evals >= 0 ? counted_evals : evals;
     if (status == LMB_OK && ev.size() >= 2) {
       float ms = 0.f;
-      cudaEventElapsedTime(&ms, ev.front(), ev.back());
+      if (!pipelined)
+        cudaEventElapsedTime(&ms, ev.front(), ev.back());
+      else if (useful > 0)
+        cudaEventElapsedTime(&ms, ev.front(), ev[size_t(2 * useful)]);
       stats->total_ms = ms;
-      // events: [span start] then pairs around each evaluation, then end
-      const int useful = counted_evals >= 0 ? counted_evals : evals;
       for (size_t q = 1; q + 1 < ev.size() && int(q / 2) < useful; q += 2) {
         float e = 0.f;
         cudaEventElapsedTime(&e, ev[q], ev[q + 1]);

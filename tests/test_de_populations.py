@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 from scipy.optimize import differential_evolution
 
-from pylorenzmie_b200.analysis._de import Population, run_populations, supported
+from pylorenzmie_b200.analysis._de import Populations, run_populations, supported
 from pylorenzmie_b200.analysis._population import de_settings
 
 
@@ -145,4 +145,53 @@ def test_other_settings_go_to_scipy(extra):
 
 def test_bad_bounds_raise():
     with pytest.raises(ValueError):
-        Population([(0., np.inf)], popsize=5, seed=1)
+        Populations([dict(bounds=[(0., np.inf)], popsize=5, seed=1,
+                          settings={})])
+
+
+def test_one_shape_group_matches_scipy():
+    '''Twelve searches of one population shape share arrays: different
+    objectives, generators, tolerances, mutation settings and maxiter
+    exits, a NaN band, and a search whose first population is all
+    infinite; each still ends where scipy ends alone.'''
+    base = {'tol': 0.01, 'polish': False, 'updating': 'deferred',
+            'workers': -1}
+    rng = np.random.default_rng(17)
+    cases = []
+    for i in range(12):
+        c = list(rng.uniform(-1., 1., 3))
+        kw = {}
+        if i == 4:
+            kw['nan_band'] = (-0.3, 0.1)
+        if i == 7:
+            kw['inf_calls'] = 1
+        settings = dict(base, tol=[0.01, 1e-3, 0.05][i % 3])
+        if i % 4 == 1:
+            settings['mutation'] = 0.7
+        if i % 5 == 2:
+            settings['maxiter'] = 6
+        if i % 6 == 3:
+            settings['recombination'] = 0.4
+        seed = (100 + i if i % 3 == 0 else
+                np.random.RandomState(200 + i) if i % 3 == 1 else
+                np.random.default_rng(300 + i))
+        cases.append((dict(bounds=[(-2., 2.)] * 3, popsize=10,
+                           settings=settings), c, kw, i))
+
+    def fresh(i):
+        return (100 + i if i % 3 == 0 else
+                np.random.RandomState(200 + i) if i % 3 == 1 else
+                np.random.default_rng(300 + i))
+    fs = [_objective(c, [1., 0.5, 0.3], **kw) for _, c, kw, _ in cases]
+    problems = [dict(p, seed=fresh(i)) for p, _, _, i in cases]
+    with np.errstate(invalid='ignore'):
+        got = run_populations(problems, lambda b: {k: fs[k](x)
+                                                   for k, x in b.items()})
+    for (p, c, kw, i), r in zip(cases, got):
+        f = _objective(c, [1., 0.5, 0.3], **kw)
+        with np.errstate(invalid='ignore'):
+            ref = differential_evolution(f, p['bounds'], popsize=10,
+                                         seed=fresh(i),
+                                         **de_settings(p['settings']))
+        _assert_same(r, ref)
+    assert len({r.nit for r in got}) > 3      # they finished apart
