@@ -319,6 +319,32 @@ int lmb_fit_batch(const lmb_feature *features, int nfeatures,
                   size_t workspace_bytes, lmb_fit_stats *stats, void *stream);
 
 /*
+ * lmb_fit_batch for an instrument with spherical aberration: the model
+ * hologram of each feature is |E e^{i Phi} + x|^2 with the phase of
+ * AberratedLorenzMie._aberration (theory/Aberrated.py:62-79),
+ * Phi = c r^4 / (r^2 + z_p^2)^2, r the in-plane distance of the pixel from
+ * the particle and c = aberration = 4 n_m^3 s / k (k = Instrument.wavenumber,
+ * s = spherical, the same coefficient lmb_field_aberrated takes); its
+ * derivatives enter the x_p, y_p, z_p columns of the Jacobian.  Replaces
+ * the reference's Optimizer.optimize of an AberratedLorenzMie model
+ * (analysis/Optimizer.py:196-278 with a forward-difference Jacobian).
+ * Multilayer spheres as lmb_fit_batch_layered (nlayers 1: homogeneous).
+ * aberration 0 gives lmb_fit_batch's (or lmb_fit_batch_layered's) results
+ * exactly; a non-finite value returns LMB_ERR_ARG.
+ */
+int lmb_fit_batch_aberrated(const lmb_feature *features, int nfeatures,
+                            long long total_pixels, const float *data,
+                            const float *coords, lmb_sphere *params,
+                            int nlayers, const double *layer_fractions,
+                            const double *layer_indices, double n_m,
+                            double wavelength, double magnification,
+                            double noise, int nmax_cap, double aberration,
+                            const lmb_fit_settings *settings,
+                            lmb_fit_result *results, void *workspace,
+                            size_t workspace_bytes, lmb_fit_stats *stats,
+                            void *stream);
+
+/*
  * lmb_fit_batch for multilayer (core-shell) spheres: the free parameters
  * are the outer radius a_p and the outer layer's index n_p + i k_p (with
  * the position); every inner radius keeps its fraction of a_p.  Layered

@@ -13,7 +13,7 @@ Test infrastructure only: see ``oracle/__init__.py``.
 import numpy as np
 from scipy.optimize import least_squares
 from scipy.linalg import svd
-from .field import hologram
+from .field import hologram, aberrated_hologram
 
 PARTICLE_KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
 DEFAULT_VARIABLES = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')
@@ -35,7 +35,7 @@ def statistics(res, npix):
 
 
 def fit(data, coordinates, particle, instrument, variables=DEFAULT_VARIABLES,
-        settings=None, jac=None):
+        settings=None, jac=None, spherical=0.):
     '''One LM fit; returns a dict shaped like ``Optimizer.result``.
 
     ``data``: (npts,) normalized intensities; ``coordinates``: (2|3, npts);
@@ -46,6 +46,9 @@ def fit(data, coordinates, particle, instrument, variables=DEFAULT_VARIABLES,
     ``jac``: optional callable p -> (npts, nvar) dH/dp (not divided by
     noise), standing in for the analytic-Jacobian slot
     (analysis/Optimizer.py:218-220, 251-255).
+    ``spherical``: the model is AberratedLorenzMie with this coefficient
+    (theory/Aberrated.py:41-85), as when the reference's Optimizer is given
+    that model.
     '''
     settings = dict(DEFAULT_SETTINGS if settings is None else settings)
     variables = list(variables)
@@ -63,8 +66,12 @@ def fit(data, coordinates, particle, instrument, variables=DEFAULT_VARIABLES,
         return p
 
     def residuals(values):
-        return (hologram(coordinates, [params(values)], instrument) -
-                data) / noise
+        if spherical:
+            h = aberrated_hologram(coordinates, [params(values)], instrument,
+                                   spherical)
+        else:
+            h = hologram(coordinates, [params(values)], instrument)
+        return (h - data) / noise
 
     if jac is not None:
         settings['jac'] = lambda values: jac(params(values)) / noise

@@ -98,6 +98,10 @@ _SIGNATURES = {
                                    _d, _d, _d, _d, _i,
                                    ctypes.POINTER(FitSettings), _vp, _vp, _sz,
                                    ctypes.POINTER(FitStats), _vp]),
+    'lmb_fit_batch_aberrated': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _i, _vp,
+                                     _vp, _d, _d, _d, _d, _i, _d,
+                                     ctypes.POINTER(FitSettings), _vp, _vp,
+                                     _sz, ctypes.POINTER(FitStats), _vp]),
     'lmb_fit_batch_streamed': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _i, _vp,
                                     _vp, _d, _d, _d, _d, _i,
                                     ctypes.POINTER(FitSettings), _vp, _d,

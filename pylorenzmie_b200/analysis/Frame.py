@@ -149,7 +149,7 @@ class Frame(Hologram):
                    tuple(sorted((k, repr(v)) for k, v in opt.settings.items())),
                    tuple(sorted(inst.properties.items())),
                    None if layers is None else layers[0],
-                   str(f.model.device))
+                   str(f.model.device), opt._aberration())
             groups.setdefault(key, []).append(i)
         done = set()
         for key, idx in groups.items():
@@ -161,7 +161,7 @@ class Frame(Hologram):
             params, res, _ = _fit.fit_items(
                 items, starts, members[0].model.instrument, opt0.variables,
                 opt0.settings, device=members[0].model.device, layers=layers,
-                autotune=len(members) >= 64)
+                autotune=len(members) >= 64, aberration=opt0._aberration())
             for j, f in enumerate(members):
                 f.optimizer._data = np.asarray(items[j][0])
                 f.optimizer.model.coordinates = items[j][2] if \

@@ -157,8 +157,6 @@ class Optimizer(LMObject):
             return False
         if not set(self.variables) <= set(PARAM_KEYS) or not self.variables:
             return False
-        if getattr(self.model, '_aberration', lambda: 0.)() != 0.:
-            return False  # the device fit models ideal optics
         p = self.model.particle
         return len(p) == 1 and hasattr(p, 'a_p')
 
@@ -194,6 +192,12 @@ class Optimizer(LMObject):
         return np.array([[r[0], r[1], r[2], part.a_p, part.n_p,
                           getattr(part, 'k_p', 0.)]])
 
+    def _aberration(self):
+        '''Spherical-aberration coefficient c of the model (0: ideal
+        optics; AberratedLorenzMie models carry the phase of
+        theory/Aberrated.py into the device fit).'''
+        return float(getattr(self.model, '_aberration', lambda: 0.)())
+
     def _optimize_device(self, data, grid, coords):
         packed = _fit.PackedFeatures([(data, grid, coords)])
         part = self.model.particle[0] if len(self.model.particle) else None
@@ -201,7 +205,8 @@ class Optimizer(LMObject):
                                       self.model.instrument,
                                       self.variables, self.settings,
                                       device=self.model.device,
-                                      layers=_fit.layers_of([part]))
+                                      layers=_fit.layers_of([part]),
+                                      aberration=self._aberration())
         status = int(res['status'][0])
         if status == -1:
             raise ValueError("Method 'lm' doesn't work when the number of "
@@ -298,9 +303,6 @@ class Optimizer(LMObject):
         if not self._device_fit_ok() and not (
                 set(self.variables) <= set(PARAM_KEYS)):
             raise ValueError('optimize_batch fits sphere parameters only')
-        if getattr(self.model, '_aberration', lambda: 0.)() != 0.:
-            raise ValueError('optimize_batch models ideal optics; fit an '
-                             'aberrated model with optimize()')
         layers = None
         if particles is not None:
             layers = _fit.layers_of(list(particles))
@@ -316,7 +318,7 @@ class Optimizer(LMObject):
         params, res, npix = _fit.fit_items(
             items, starts, self.model.instrument, self.variables,
             self.settings, device=self.model.device, layers=layers,
-            autotune=autotune, chunks=chunks)
+            autotune=autotune, chunks=chunks, aberration=self._aberration())
         return batch_frame(params, res, npix, self.variables)
 
 
@@ -337,8 +339,6 @@ class Optimizer(LMObject):
         if not self._device_fit_ok() and not (
                 set(self.variables) <= set(PARAM_KEYS)):
             raise ValueError('optimize_stream fits sphere parameters only')
-        if getattr(self.model, '_aberration', lambda: 0.)() != 0.:
-            raise ValueError('optimize_stream models ideal optics')
         variables = list(self.variables)
         first = [True]
 
@@ -374,7 +374,7 @@ class Optimizer(LMObject):
         for params, res, npix in _fit.fit_stream(
                 chain(), self.model.instrument, variables, self.settings,
                 device=self.model.device, autotune=self._stream_tune,
-                depth=depth):
+                depth=depth, aberration=self._aberration()):
             yield batch_frame(params, res, npix, variables)
 
 

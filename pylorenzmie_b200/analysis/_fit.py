@@ -279,12 +279,14 @@ def upload(packed, starts, device=None):
 def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
                instrument, variables, settings=None, nmax_cap=None,
                starts_host=None, stats=False, tile_config=0, layers=None,
-               ready=None, wait_seconds=60.):
+               ready=None, wait_seconds=60., aberration=0.):
     '''Run lmb_fit_batch on device-resident inputs.  d_params is updated in
     place with the fitted values; returns (results tensor (B*80 uint8),
     FitStats or None).  With ``ready`` (a device int32 tensor) the fit is
     streamed (lmb_fit_batch_streamed): features are admitted as the caller
-    advances it.'''
+    advances it.  A nonzero ``aberration`` (the coefficient c of the
+    spherical-aberration phase, AberratedLorenzMie._aberration) fits the
+    aberrated model (lmb_fit_batch_aberrated; not streamed).'''
     dev = d_data.device
     lib = _native.load()
     settings = dict(DEFAULT_SETTINGS if settings is None else settings)
@@ -309,6 +311,20 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
     st.max_iterations = st.max_nfev
     st.tile_config = int(tile_config)
     fs = _native.FitStats() if stats else None
+    if aberration:
+        if ready is not None:
+            raise ValueError('streamed admission fits ideal optics only')
+        if layers is None:
+            L, d_frac, d_ind = 1, None, None
+        else:
+            L, d_frac, d_ind = _layer_arrays(layers, nfeatures, dev)
+        _native.check(lib.lmb_fit_batch_aberrated(
+            ptr(d_feat), nfeatures, total_pixels, ptr(d_data), ptr(d_coords),
+            ptr(d_params), L, ptr(d_frac), ptr(d_ind), n_m, lam,
+            float(instrument.magnification), float(instrument.noise),
+            nmax_cap, float(aberration), st, ptr(d_res), ptr(ws), nbytes, fs,
+            stream_handle(dev)), 'lmb_fit_batch_aberrated')
+        return d_res, fs
     if ready is not None:
         if layers is None:
             L, d_frac, d_ind = 1, None, None
@@ -352,10 +368,10 @@ def _layer_arrays(layers, nfeatures, dev):
 
 def fit_packed(packed, starts, instrument, variables, settings=None,
                device=None, nmax_cap=None, stats=False, layers=None,
-               autotune=False):
+               autotune=False, aberration=0.):
     '''Fit every packed feature; returns (params (B, 6), results record
     array with dparams, redchi, cost, status, success, nfev, njev) and,
-    when stats, the FitStats of the call.'''
+    when stats, the FitStats of the call.  ``aberration``: see fit_device.'''
     starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
     B = starts.shape[0]
     if B == 0:
@@ -366,14 +382,14 @@ def fit_packed(packed, starts, instrument, variables, settings=None,
         nmax_cap = fit_capacity(starts, float(instrument.n_m),
                                 float(instrument.wavelength), layers)
     tile_config = 0
-    if autotune:
+    if autotune and not aberration:   # the aberrated fit has one shape
         from .. import autotune as _tuner
         tile_config = _tuner.tune(packed, starts, instrument, variables,
                                   nmax_cap, layers, d_data.device)
     d_res, fs = fit_device(d_feat, d_data, d_coords, d_params, B,
                            packed.total, instrument, variables, settings,
                            nmax_cap, starts, stats, tile_config=tile_config,
-                           layers=layers)
+                           layers=layers, aberration=aberration)
     params = d_params.view(torch.float64).reshape(B, 6).cpu().numpy()
     res = d_res[:B * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
         _native.RESULT_DTYPE).copy()
@@ -425,15 +441,16 @@ def split_by_pixels(npix, chunks):
 
 def fit_items(items, starts, instrument, variables, settings=None,
               device=None, layers=None, autotune=False, chunks=None,
-              wait_seconds=60.):
+              wait_seconds=60., aberration=0.):
     '''Fit crops given as (data, grid, coords) items.  Large batches are
     streamed: the feature records and starts go to the device first and the
     fit starts (lmb_fit_batch_streamed, driven by a worker thread); the host
     then converts the pixel data portion by portion into pinned memory and
     copies each on a second stream, advancing the device's admission count
     after each copy, so that conversion and transfer overlap the fitting of
-    the features already admitted.  Returns (params (B, 6), results record
-    array, npix (B,)).'''
+    the features already admitted.  An aberrated fit (``aberration``, see
+    fit_device) is one call.  Returns (params (B, 6), results record array,
+    npix (B,)).'''
     global _flags
     starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
     B = starts.shape[0]
@@ -443,10 +460,10 @@ def fit_items(items, starts, instrument, variables, settings=None,
     npix = packed.features['npix'].astype(np.int64)
     if chunks is None:
         chunks = default_chunks(npix)
-    if B == 0 or chunks <= 1:
+    if B == 0 or chunks <= 1 or aberration:
         params, res = fit_packed(packed, starts, instrument, variables,
                                  settings, device, layers=layers,
-                                 autotune=autotune)
+                                 autotune=autotune, aberration=aberration)
         return params, res, npix
     dev = get_device(device)
     nmax_cap = fit_capacity(starts, float(instrument.n_m),
@@ -565,7 +582,7 @@ def _stream_fit_stream(dev, slot):
 
 
 def fit_stream(batches, instrument, variables, settings=None, device=None,
-               autotune=False, depth=2):
+               autotune=False, depth=2, aberration=0.):
     '''Fit a sequence of batches, pipelined; yields, in order, (params
     (B, 6), results record array, npix (B,)) per batch.
 
@@ -603,7 +620,7 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
                                     float(instrument.wavelength), layers)
             if tile_config is None:
                 tile_config = 0
-                if autotune:
+                if autotune and not aberration:
                     from .. import autotune as _tuner
                     tile_config = _tuner.tune(packed, starts, instrument,
                                               variables, nmax_cap, layers,
@@ -626,8 +643,8 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
                 yield _collect(pending.popleft())
             pending.append((_stream_worker(depth).submit(
                 _fit_after, s_fit, ev, views, B, packed.total, instrument,
-                variables, settings, nmax_cap, starts, tile_config, layers),
-                npix))
+                variables, settings, nmax_cap, starts, tile_config, layers,
+                aberration), npix))
             k += 1
         while pending:
             yield _collect(pending.popleft())
@@ -647,14 +664,14 @@ def _collect(entry):
 
 
 def _fit_after(stream, event, views, n, total, instrument, variables,
-               settings, nmax_cap, starts, tile_config, layers):
+               settings, nmax_cap, starts, tile_config, layers, aberration=0.):
     d_feat, d_data, d_coords, d_params = views
     stream.wait_event(event)
     with torch.cuda.stream(stream):
         d_res, _ = fit_device(d_feat, d_data, d_coords, d_params, n, total,
                               instrument, variables, settings, nmax_cap,
                               starts, False, tile_config=tile_config,
-                              layers=layers)
+                              layers=layers, aberration=aberration)
         params = d_params.view(torch.float64).reshape(n, 6).cpu().numpy()
         res = d_res[:n * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
             _native.RESULT_DTYPE).copy()

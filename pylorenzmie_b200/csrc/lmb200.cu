@@ -100,6 +100,13 @@ const EvalShape kEvalShapes[] = {
     {256, 16, 2, k_fit_eval_warp<8, 2>, 1},
 };
 constexpr int kNumEvalShapes = int(sizeof(kEvalShapes) / sizeof(kEvalShapes[0]));
+// The same kernels with the spherical-aberration phase in the epilogue
+// (lmb_fit_batch_aberrated): the default packed shape and the scalar
+// fallback.
+const EvalShape kAberrShapes[] = {
+    {64, 8, 6, k_fit_eval_pair<64, 8, 6, true, true>, 0, 1},
+    {128, 4, 4, k_fit_eval<128, 4, 4, true>},
+};
 constexpr int kScalarShape = 1;  // scalar loop, used when pair records do not fit
 // pair records take 256 B per order: above this they no longer fit in
 // shared memory beside the kernels' own buffers, and the scalar loop runs
@@ -537,7 +544,8 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
                    size_t workspace_bytes, lmb_fit_stats* stats, void* stream,
                    int nlayers, const double* layer_frac,
                    const double* layer_index, const int* ready = nullptr,
-                   double wait_seconds = 0., bool sync_rounds = false) {
+                   double wait_seconds = 0., bool sync_rounds = false,
+                   double aberr = 0.) {
   if (nlayers < 1 || nlayers > LMB_MAX_LAYERS) return LMB_ERR_ARG;
   if (nlayers > 1 && nfeatures > 0 && (!layer_frac || !layer_index))
     return LMB_ERR_ARG;
@@ -588,6 +596,8 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   k *= magnification;
   c.k = k;
   c.inv_noise = 1. / noise;
+  if (!isfinite(aberr)) return LMB_ERR_ARG;
+  c.aberr = aberr;
   c.set.ftol = settings->ftol;
   c.set.xtol = settings->xtol;
   c.set.gtol = settings->gtol;
@@ -602,13 +612,13 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
                                      : ab_scratch_bytes(nmax_cap + 1);
   const int shape_index = settings->tile_config;
   if (shape_index < 0 || shape_index >= kNumEvalShapes) return LMB_ERR_ARG;
-  EvalShape shape = kEvalShapes[shape_index];
+  EvalShape shape = aberr != 0. ? kAberrShapes[0] : kEvalShapes[shape_index];
   // pair records take 256 B per order: above ~800 orders they no longer fit
   // in shared memory next to the reduction buffer, so such batches use the
   // scalar loop
   if (shape.pair && sizeof(float4) * PAIR_QUADS * (size_t(nmax_cap) + 1) >
                         kPairSmemLimit)
-    shape = kEvalShapes[kScalarShape];
+    shape = aberr != 0. ? kAberrShapes[1] : kEvalShapes[kScalarShape];
   c.pair_records = shape.pair;
   const size_t coef_smem = (shape.pair ? sizeof(float4) * PAIR_QUADS
                                        : sizeof(Quad<float>) * JAC_QUADS) *
@@ -858,6 +868,24 @@ int lmb_fit_batch_streamed(const lmb_feature* features, int nfeatures,
                         stream, nlayers, layer_fractions, layer_indices, ready,
                         wait_seconds);
 }
+int lmb_fit_batch_aberrated(const lmb_feature* features, int nfeatures,
+                            long long total_pixels, const float* data,
+                            const float* coords, lmb_sphere* params,
+                            int nlayers, const double* layer_fractions,
+                            const double* layer_indices, double n_m,
+                            double wavelength, double magnification,
+                            double noise, int nmax_cap, double aberration,
+                            const lmb_fit_settings* settings,
+                            lmb_fit_result* results, void* workspace,
+                            size_t workspace_bytes, lmb_fit_stats* stats,
+                            void* stream) {
+  return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
+                        n_m, wavelength, magnification, noise, nmax_cap,
+                        settings, results, workspace, workspace_bytes, stats,
+                        stream, nlayers, layer_fractions, layer_indices, nullptr,
+                        0., false, aberration);
+}
+
 int lmb_fit_batch_layered(const lmb_feature* features, int nfeatures,
                           long long total_pixels, const float* data,
                           const float* coords, lmb_sphere* params, int nlayers,

@@ -623,11 +623,24 @@ __global__ void k_chi2_reduce(const double* partial, const int* partial_bad,
 // ---------------------------------------------------------------------------
 // Hologram + 6-column Jacobian, single sphere per item.
 
+// With kAberr (fits with spherical aberration c = aberr): the phase and
+// its gradient at pixel offset (dx, dy) from a particle at height zp enter
+// the epilogue and the x_p, y_p, z_p columns.
+template <bool kAberr = false>
 __device__ inline void holo_jac_pixel(const Geometry<float>& g,
                                       const Quad<float>* coef, int nm, float kf,
-                                      float* H, float* dH) {
+                                      float* H, float* dH, double aberr = 0.,
+                                      double dx = 0., double dy = 0.,
+                                      double zp = 0.) {
   const JacSums<float> A = order_sum_jac<float>(g, coef, nm);
-  holo_jac_reverse<float>(g, A, kf, H, dH);
+  if constexpr (kAberr) {
+    float dphi[3], hphi;
+    const cplx<float> w = aberration_wave<float>(aberr, dx, dy, zp, dphi);
+    holo_jac_reverse<float, true>(g, A, kf, H, dH, w, &hphi);
+    for (int j = 0; j < 3; ++j) dH[j] += hphi * dphi[j];
+  } else {
+    holo_jac_reverse<float>(g, A, kf, H, dH);
+  }
 }
 
 __global__ void __launch_bounds__(128)
@@ -842,6 +855,7 @@ struct FitCtx {
   const double* layer_frac;   // [nf][nlayers-1] inner radii / outer radius
   const double* layer_index;  // [nf][nlayers-1][2] inner layer indices
   double n_m, wavelength, k, inv_noise;
+  double aberr;  // spherical-aberration coefficient c (0: ideal optics)
   LMSettings set;
   int variables, flags, max_iterations;
   int pair_records;    // the evaluation kernel reads stage_pair records
@@ -931,7 +945,7 @@ __global__ void k_fit_setup(FitCtx c) {
 }
 
 // Evaluation: persistent CTAs pull tiles from an atomic queue.
-template <int TPB, int PPT, int MINB>
+template <int TPB, int PPT, int MINB, bool kAberr = false>
 __global__ void __launch_bounds__(TPB, MINB)
 k_fit_eval(FitCtx c) {
   extern __shared__ __align__(16) char smem[];
@@ -985,7 +999,8 @@ k_fit_eval(FitCtx c) {
       const Geometry<float> g = geometry<float>(c.k, x - ep.p[0], y - ep.p[1],
                                                 -ep.p[2], 0., ep.p[2], bohren);
       float H, dH[6];
-      holo_jac_pixel(g, coef, nm, kf, &H, dH);
+      holo_jac_pixel<kAberr>(g, coef, nm, kf, &H, dH, c.aberr, x - ep.p[0],
+                             y - ep.p[1], ep.p[2]);
       const float r = (H - d) * inv_noise;
       float J[6];
 #pragma unroll
@@ -1017,11 +1032,12 @@ k_fit_eval(FitCtx c) {
 // With kRecompute the pixel geometry is formed again after the order loop
 // instead of being held in registers across it (the empty asm statements
 // keep the compiler from merging the two computations).
-template <bool kRecompute>
+template <bool kRecompute, bool kAberr = false>
 __device__ inline void holo_jac_pair(double k, const double* dx,
                                      const double* dy, double dz, double zp,
                                      bool bohren, const float4* rec, int nm,
-                                     float kf, float* H, float (*dH)[6]) {
+                                     float kf, float* H, float (*dH)[6],
+                                     double aberr = 0.) {
   Geometry<float> g[2];
   for (int l = 0; l < 2; ++l)
     g[l] = geometry<float>(k, dx[l], dy[l], dz, 0., zp, bohren);
@@ -1038,7 +1054,14 @@ __device__ inline void holo_jac_pair(double k, const double* dx,
   for (int lane = 0; lane < 2; ++lane) {
     const Geometry<float>& gl = g[lane];
     const JacSums<float> A = pair_lane(P, lane, gl.smu);
-    holo_jac_reverse<float>(gl, A, kf, &H[lane], dH[lane]);
+    if constexpr (kAberr) {
+      float dphi[3], hphi;
+      const cplx<float> w = aberration_wave<float>(aberr, dx[lane], dy[lane], zp, dphi);
+      holo_jac_reverse<float, true>(gl, A, kf, &H[lane], dH[lane], w, &hphi);
+      for (int j = 0; j < 3; ++j) dH[lane][j] += hphi * dphi[j];
+    } else {
+      holo_jac_reverse<float>(gl, A, kf, &H[lane], dH[lane]);
+    }
   }
 }
 
@@ -1058,7 +1081,7 @@ __device__ inline void fit_pixel_xy(const lmb_feature& ft, const float* coords,
 // Evaluation with the packed two-pixel loop: as k_fit_eval, each thread
 // takes pixel pairs (i, i + TPB) of its tile; PPT is even.  The records in
 // coef32 are in the pair layout (stage_pair).
-template <int TPB, int PPT, int MINB, bool kRecompute>
+template <int TPB, int PPT, int MINB, bool kRecompute, bool kAberr = false>
 __global__ void __launch_bounds__(TPB, MINB)
 k_fit_eval_pair(FitCtx c) {
   static_assert(PPT % 2 == 0, "pixel pairs");
@@ -1111,8 +1134,8 @@ k_fit_eval_pair(FitCtx c) {
       const double dx[2] = {x0 - ep.p[0], x1 - ep.p[0]};
       const double dy[2] = {y0 - ep.p[1], y1 - ep.p[1]};
       float H[2], dH[2][6];
-      holo_jac_pair<kRecompute>(c.k, dx, dy, -ep.p[2], ep.p[2], bohren, rec, nm,
-                                kf, H, dH);
+      holo_jac_pair<kRecompute, kAberr>(c.k, dx, dy, -ep.p[2], ep.p[2], bohren,
+                                        rec, nm, kf, H, dH, c.aberr);
 #pragma unroll
       for (int lane = 0; lane < 2; ++lane) {
         if (lane == 1 && !v1) break;
@@ -1146,7 +1169,7 @@ k_fit_eval_pair(FitCtx c) {
 // queue (16 pixels per lane), keeps its own copy of the coefficients of the
 // feature it is on, and reduces its 28 sums with shuffles -- no block-wide
 // barrier anywhere.  WPB warps per CTA, MINB CTAs per SM at least.
-template <int WPB, int MINB>
+template <int WPB, int MINB, bool kAberr = false>
 __global__ void __launch_bounds__(WPB * 32, MINB)
 k_fit_eval_warp(FitCtx c) {
   extern __shared__ __align__(16) char smem[];
@@ -1201,7 +1224,8 @@ k_fit_eval_warp(FitCtx c) {
       const Geometry<float> g = geometry<float>(c.k, x - ep.p[0], y - ep.p[1],
                                                 -ep.p[2], 0., ep.p[2], bohren);
       float H, dH[6];
-      holo_jac_pixel(g, coef, nm, kf, &H, dH);
+      holo_jac_pixel<kAberr>(g, coef, nm, kf, &H, dH, c.aberr, x - ep.p[0],
+                             y - ep.p[1], ep.p[2]);
       const float r = (H - d) * inv_noise;
       float J[6];
 #pragma unroll

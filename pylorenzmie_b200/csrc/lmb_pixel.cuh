@@ -707,9 +707,14 @@ LMB_HD void epilogue_jac(const Geometry<R>& g, const JacSums<R>& A, R k,
 // where S_k does) and of the real geometric variables, which the chain rule
 // then maps onto (kx, ky, kz).  The phase's kz rate and the on-axis branch
 // are those of epilogue_jac.  For a complex z, zbar = dH/dRe z + i dH/dIm z.
-template <typename R>
+// With kAberr the particle's field carries a phase e^{i Phi} (spherical
+// aberration, theory/Aberrated.py:62-85): |E e^{i Phi} + x|^2 = |E + w x|^2
+// with w = e^{-i Phi}, so w replaces the unit reference wave, and
+// *hphi = dH/dPhi = 2 Im(conj(E_x + w) w) for the caller's chain rule.
+template <typename R, bool kAberr = false>
 LMB_HD void holo_jac_reverse(const Geometry<R>& g, const JacSums<R>& A, R k,
-                             R* H, R* dH) {
+                             R* H, R* dH, cplx<R> w = mk(R(1), R(0)),
+                             R* hphi = nullptr) {
   const R ikr = g.ikr, mu = g.mu, st = g.sint, cp = g.cosp, sp = g.sinp;
   const R ikr2 = ikr * ikr;
   // forward
@@ -723,7 +728,12 @@ LMB_HD void holo_jac_reverse(const Geometry<R>& g, const JacSums<R>& A, R k,
   c[2] = mu * es[0] - st * es[1];
   cplx<R> et[3];
   for (int j = 0; j < 3; ++j) et[j] = g.phase * c[j];
-  et[0].re += R(1);
+  if constexpr (kAberr) {
+    et[0] = et[0] + w;
+    *hphi = R(2) * (conj(et[0]) * w).im;
+  } else {
+    et[0].re += R(1);
+  }
   *H = norm2(et[0]) + norm2(et[1]) + norm2(et[2]);
   // reverse: E = phase c
   cplx<R> cb[3], phb = mk(R(0), R(0));
@@ -792,6 +802,32 @@ LMB_HD void holo_jac_reverse(const Geometry<R>& g, const JacSums<R>& A, R k,
   dH[3] = da;
   dH[4] = dn;
   dH[5] = dk;
+}
+
+// Spherical aberration in the fits (theory/Aberrated.py:62-79): the phase
+// Phi = c r^4 / (r^2 + z_p^2)^2 of a particle's field at a pixel, returned
+// as w = e^{-i Phi} (the reference wave as the aberrated field sees it),
+// with dPhi/d(x_p, y_p, z_p) in dphi; (dx, dy) is the pixel minus the
+// particle, zp the particle's height:
+//   dPhi/dx_p = -4 c r^2 z_p^2 dx / (r^2 + z_p^2)^3 (and y alike),
+//   dPhi/dz_p = -4 c r^4 z_p / (r^2 + z_p^2)^3.
+template <typename R>
+LMB_HD cplx<R> aberration_wave(double c, double dx, double dy, double zp,
+                               R* dphi) {
+  const double rsq = dx * dx + dy * dy;
+  const double z2 = zp * zp;
+  const double den = rsq + z2;
+  if (!(den > 0.)) {
+    dphi[0] = dphi[1] = dphi[2] = R(0);
+    return mk(R(1), R(0));
+  }
+  const double q = rsq / den;
+  const double phi = c * q * q;
+  const double t = 4. * c * q / (den * den);  // 4 c r^2 / (r^2 + z_p^2)^3
+  dphi[0] = R(-t * z2 * dx);
+  dphi[1] = R(-t * z2 * dy);
+  dphi[2] = R(-t * rsq * zp);
+  return conj(cis(R(reduce_2pi(phi))));
 }
 
 // Hologram from the total scattered field: |E + x|^2 = |E|^2 + 2 Re(E_x) + 1

@@ -8,9 +8,10 @@ in-medium wave number (rad/pixel), r the in-plane distance from each
 particle and z_p its axial position, both in pixels.  Here the phase is
 applied inside the field kernel (lmb_field_aberrated /
 lmb_hologram_aberrated), per particle and pixel, before the superposition.
-The device fit and the analytic Jacobian do not include the aberration:
-with spherical != 0, Optimizer fits through its host loop on this model's
-holograms, and ``jac_params`` is empty.
+The device fits include it (lmb_fit_batch_aberrated: the phase enters the
+hologram and the x_p, y_p, z_p columns of the Jacobian), so Optimizer's
+optimize, optimize_batch and optimize_stream fit this model on the GPU;
+``jac()`` does not, and ``jac_params`` is empty when spherical != 0.
 '''
 from .LorenzMie import LorenzMie
 

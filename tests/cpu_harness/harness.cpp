@@ -294,10 +294,12 @@ API void h_jacobian_pair(const double* coords, long long npts, const double* p,
 
 // Hologram and Jacobian of one sphere with the reverse-mode epilogue
 // (holo_jac_reverse) after the scalar order loop.
+// aberr != 0: the spherical-aberration phase of the device fits
+// (aberration_wave) in the epilogue and the x_p, y_p, z_p columns.
 template <typename R>
 static void jac_rev_one(const double* coords, long long npts, const double* p,
                         const double* ab, const double* dab, int nmax, double k,
-                        int flags, double* holo, double* jac) {
+                        int flags, double* holo, double* jac, double aberr = 0.) {
   std::vector<Quad<R>> q(JAC_QUADS * (nmax + 1));
   stage<R>(ab, dab, nmax, q.data(), JAC_QUADS);
   for (long long i = 0; i < npts; ++i) {
@@ -305,10 +307,28 @@ static void jac_rev_one(const double* coords, long long npts, const double* p,
     Geometry<R> g = geometry<R>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
     JacSums<R> A = order_sum_jac<R>(g, q.data(), nmax);
     R H, dH[6];
-    holo_jac_reverse<R>(g, A, R(k), &H, dH);
+    if (aberr != 0.) {
+      R dphi[3], hphi;
+      const cplx<R> w = aberration_wave<R>(aberr, x - p[0], y - p[1], p[2], dphi);
+      holo_jac_reverse<R, true>(g, A, R(k), &H, dH, w, &hphi);
+      for (int j = 0; j < 3; ++j) dH[j] += hphi * dphi[j];
+    } else {
+      holo_jac_reverse<R>(g, A, R(k), &H, dH);
+    }
     holo[i] = H;
     for (int j = 0; j < 6; ++j) jac[j * npts + i] = dH[j];
   }
+}
+
+API void h_jacobian_aberrated(const double* coords, long long npts,
+                              const double* p, const double* ab,
+                              const double* dab, int nmax, double k, int flags,
+                              int fp64, double aberr, double* holo,
+                              double* jac) {
+  if (fp64)
+    jac_rev_one<double>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac, aberr);
+  else
+    jac_rev_one<float>(coords, npts, p, ab, dab, nmax, k, flags, holo, jac, aberr);
 }
 
 API void h_jacobian_rev(const double* coords, long long npts, const double* p,

@@ -48,6 +48,10 @@ def load():
     lib.h_jacobian_rev.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
                                    ctypes.c_int, ctypes.c_double,
                                    ctypes.c_int, ctypes.c_int, _dp, _dp]
+    lib.h_jacobian_aberrated.argtypes = [_dp, ctypes.c_longlong, _dp, _dp,
+                                         _dp, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, _dp, _dp]
     lib.h_field_pair.argtypes = [_dp, ctypes.c_longlong, _dp, _dp,
                                  ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                  _dp]
@@ -171,6 +175,21 @@ class Harness:
                               (1 if cartesian else 0) | (2 if bohren else 0),
                               ptr(out))
         return out[..., 0] + 1j * out[..., 1]
+
+    def jacobian_aberrated(self, coords, p, ab, dab, k, aberration,
+                           bohren=True, fp64=False):
+        '''Hologram and Jacobian of the aberrated model of the device fits
+        (spherical-aberration coefficient c = aberration).'''
+        c = np.ascontiguousarray(coords, dtype=float)
+        npts = c.shape[1]
+        n, a, d = self._pack_ab(ab, dab)
+        holo = np.zeros(npts)
+        jac = np.zeros((6, npts))
+        pv = np.asarray(p, dtype=float)
+        self.lib.h_jacobian_aberrated(ptr(c), npts, ptr(pv), ptr(a), ptr(d), n,
+                                      k, 1 | (2 if bohren else 0), int(fp64),
+                                      float(aberration), ptr(holo), ptr(jac))
+        return holo, jac
 
     def jacobian_rev(self, coords, p, ab, dab, k, bohren=True, fp64=False):
         '''As jacobian, with the reverse-mode epilogue.'''

@@ -152,6 +152,44 @@ def test_lm_state_machine_matches_scipy(h, golden_fit, variables):
     np.testing.assert_allclose(dp, sdp, rtol=1e-6)
 
 
+@pytest.mark.parametrize('spherical', [0.9, -2.5])
+def test_aberrated_jacobian(h, spherical):
+    '''The aberrated epilogue of the device fits: the hologram equals the
+    oracle's AberratedLorenzMie hologram, and the six columns equal central
+    differences of it (FP64 sums; FP32 sums within FP32 accuracy).'''
+    inst = field.DEFAULT_INSTRUMENT
+    c = field.coordinates3(field.meshgrid((41, 53)))
+    p = np.array([20.3, 25.1, 120., 0.8, 1.45, 0.002])
+    caber = 4. * inst['n_m'] ** 3 / K * spherical
+    ab, dab = h.sphere_ab(p[3], p[4], p[5], 1.34, 0.447, deriv=True)
+    H, J = h.jacobian_aberrated(c, p[:3], ab, dab, K, caber, fp64=True)
+
+    def holo(q):
+        return field.aberrated_hologram(c, [dict(zip(KEYS, q))], inst,
+                                        spherical)
+    ref = holo(p)
+    np.testing.assert_allclose(H, ref, rtol=1e-10, atol=1e-12)
+    steps = [1e-4, 1e-4, 1e-3, 1e-6, 1e-6, 1e-6]
+    for j, dj in enumerate(steps):
+        qp, qm = p.copy(), p.copy()
+        qp[j] += dj
+        qm[j] -= dj
+        fd = (holo(qp) - holo(qm)) / (2 * dj)
+        scale = np.abs(fd).max()
+        assert np.abs(J[j] - fd).max() <= 2e-5 * scale, \
+            (KEYS[j], np.abs(J[j] - fd).max() / scale)
+    H32, J32 = h.jacobian_aberrated(c, p[:3], ab, dab, K, caber, fp64=False)
+    assert np.all(np.abs(H32 - H) <= 2e-5 * (1 + np.abs(H)))
+    for j in range(6):
+        scale = np.abs(J[j]).max()
+        assert np.abs(J32[j] - J[j]).max() <= 2e-4 * scale, KEYS[j]
+    # no aberration: the ideal epilogue exactly
+    H0, J0 = h.jacobian_aberrated(c, p[:3], ab, dab, K, 0., fp64=True)
+    H1, J1 = h.jacobian_rev(c, p[:3], ab, dab, K, fp64=True)
+    np.testing.assert_array_equal(H0, H1)
+    np.testing.assert_array_equal(J0, J1)
+
+
 @pytest.mark.parametrize('radii,idx', [
     ([0.3, 0.75], [1.6, 1.45 + 0.002j]),
     ([0.4, 0.8, 1.2], [1.8 + 0.01j, 1.33, 1.5]),
