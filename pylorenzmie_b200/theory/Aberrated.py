@@ -9,9 +9,13 @@ particle and z_p its axial position, both in pixels.  Here the phase is
 applied inside the field kernel (lmb_field_aberrated /
 lmb_hologram_aberrated), per particle and pixel, before the superposition.
 The device fits include it (lmb_fit_batch_aberrated: the phase enters the
-hologram and the x_p, y_p, z_p columns of the Jacobian), so Optimizer's
-optimize, optimize_batch and optimize_stream fit this model on the GPU;
-``jac()`` does not, and ``jac_params`` is empty when spherical != 0.
+hologram and the x_p, y_p, z_p columns of the Jacobian): with ``spherical``
+among an Optimizer's fixed parameters (a calibrated instrument), optimize,
+optimize_batch and optimize_stream fit this model on the GPU.  With it free
+-- the reference's default, whose fixed list does not name it -- the fit
+runs through scipy's host loop on this model's holograms, as the
+reference's does.  ``jac()`` does not include the aberration, and
+``jac_params`` is empty when spherical != 0.
 '''
 from .LorenzMie import LorenzMie
 

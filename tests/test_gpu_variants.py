@@ -70,8 +70,8 @@ def test_dimer_hologram_matches_reference(golden_variants, fp64):
 
 
 def test_aberrated_device_fit():
-    '''With spherical != 0 the device fit (lmb_fit_batch_aberrated) fits the
-    aberrated model: against the oracle's fit of the same hologram (scipy
+    '''With spherical != 0 and fixed (a calibrated instrument), the device
+    fit (lmb_fit_batch_aberrated) fits the aberrated model: against the oracle's fit of the same hologram (scipy
     lm on a forward-difference Jacobian of the FP64 aberrated model, as the
     reference's Optimizer does on an AberratedLorenzMie) the parameters
     agree to the fit targets or a third of their uncertainty, it recovers
@@ -95,6 +95,11 @@ def test_aberrated_device_fit():
                                particle=s, instrument=_inst(),
                                spherical=spherical)
         opt = Optimizer(model=m)
+        # by default 'spherical' is free too (the reference's default
+        # fixed list does not name it): scipy's host loop fits it
+        assert 'spherical' in opt.variables and not opt._device_fit_ok()
+        # a calibrated instrument: 'spherical' fixed, the device fit
+        opt.fixed = opt.fixed + ['spherical']
         assert opt._device_fit_ok()
         holo = Hologram(data.reshape(shape))
         r = opt.optimize(holo)
