@@ -176,8 +176,11 @@ int lmb_chi2_batch(const double *coords, long long npts, const double *data,
  *   max_crop_npts  the largest crop (sets the grid; a crop larger than it,
  *              or a range outside [0, npts), gives that item NaN)
  *   workspace  of lmb_chi2_workspace_bytes(max_crop_npts, nitems) bytes
- * Every other argument as lmb_chi2_batch; each item's chi2 is bit-identical
- * to lmb_chi2_batch over its crop alone.
+ *   aberration the spherical-aberration coefficient c of
+ *              lmb_field_aberrated (0: ideal optics), for the searches of
+ *              AberratedLorenzMie models
+ * Every other argument as lmb_chi2_batch; with aberration 0 each item's
+ * chi2 is bit-identical to lmb_chi2_batch over its crop alone.
  */
 int lmb_chi2_crops(const double *coords, long long npts, const double *data,
                    double noise, const long long *crop_start, int ncrops,
@@ -185,7 +188,7 @@ int lmb_chi2_crops(const double *coords, long long npts, const double *data,
                    const lmb_sphere *spheres, const int *item_start, int nitems,
                    const double *ab, const int *nmax, int nmax_cap, double k,
                    int flags, double *chi2, int *nonfinite, void *workspace,
-                   size_t workspace_bytes, void *stream);
+                   size_t workspace_bytes, void *stream, double aberration);
 
 /*
  * Hologram and its Jacobian for nitems single-sphere items, FP32 sums,

@@ -93,7 +93,7 @@ _SIGNATURES = {
                             _d, _i, _vp, _vp, _vp, _sz, _vp]),
     'lmb_chi2_crops': (_i, [_vp, _ll, _vp, _d, _vp, _i, _vp, _ll, _vp, _vp,
                             _i, _vp, _vp, _i, _d, _i, _vp, _vp, _vp, _sz,
-                            _vp]),
+                            _vp, _d]),
     'lmb_fit_batch_layered': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _i, _vp, _vp,
                                    _d, _d, _d, _d, _i,
                                    ctypes.POINTER(FitSettings), _vp, _vp, _sz,

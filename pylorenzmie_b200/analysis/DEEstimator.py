@@ -25,8 +25,8 @@ from scipy.optimize import differential_evolution
 from .BaseEstimator import BaseEstimator
 from .Mask import Mask
 from ._de import run_populations, supported
-from ._population import (CropPopulations, PopulationChi2, batchable,
-                          de_settings, lockstep_de)
+from ._population import (CropPopulations, PopulationChi2, aberration,
+                          batchable, de_settings, lockstep_de)
 
 DEFAULT_BOUNDS = {
     'z_p': (10., 600.),
@@ -100,7 +100,7 @@ def run_searches(searches, workers=256):
         inst = m.instrument
         key = (str(m.device), float(inst.n_m), float(inst.wavelength),
                float(inst.magnification), float(sr['noise']),
-               bool(getattr(m, 'double_precision', False)))
+               bool(getattr(m, 'double_precision', False)), aberration(m))
         groups.setdefault(key, []).append(i)
     for key, idx in groups.items():
         if key is None or len(idx) == 1:

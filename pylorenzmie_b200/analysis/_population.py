@@ -25,13 +25,19 @@ MAX_ITEMS = 65535          # candidates per launch (the grid's y extent)
 
 def batchable(model, variables):
     '''True when every searched variable is a parameter of a single
-    homogeneous sphere (the population then goes to the GPU in one call).'''
+    homogeneous sphere (the population then goes to the GPU in one call;
+    an aberrated model's phase is applied in the same launch).'''
     p = model.particle
     if isinstance(p, (list, tuple)) or K.is_layered(p) or not hasattr(p, 'a_p'):
         return False
-    if len(p) != 1 or getattr(model, '_aberration', lambda: 0.)() != 0.:
+    if len(p) != 1:
         return False
     return all(v in SPHERE_KEYS for v in variables)
+
+
+def aberration(model):
+    '''Spherical-aberration coefficient c of a model (0: ideal optics).'''
+    return float(getattr(model, '_aberration', lambda: 0.)())
 
 
 def de_settings(settings):
@@ -95,7 +101,24 @@ class PopulationChi2:
         self.k = inst.wavenumber()
         self.noise = float(noise)
         self.fp64 = bool(getattr(model, 'double_precision', False))
+        self.aberr = aberration(model)
         self.evaluations = 0
+
+    def _chi2(self, sp, ab, nmax, cap, fp64):
+        '''(chi2, nonfinite) of candidates sp; aberrated models through
+        lmb_chi2_crops with the whole pixel set as the one crop.'''
+        dev = self.coords.device
+        S = sp.shape[0]
+        item_start = torch.arange(S + 1, dtype=torch.int32, device=dev)
+        if not self.aberr:
+            return K.chi2(self.coords, self.data, self.noise, sp, item_start,
+                          ab, nmax, cap, self.k, fp64=fp64, nonfinite=True)
+        n = self.coords.shape[1]
+        crop_start = torch.tensor([0, n], dtype=torch.int64, device=dev)
+        item_crop = torch.zeros(S, dtype=torch.int32, device=dev)
+        return K.chi2_crops(self.coords, self.data, self.noise, crop_start,
+                            item_crop, n, sp, item_start, ab, nmax, cap,
+                            self.k, fp64=fp64, aberration=self.aberr)
 
     def __call__(self, x):
         x = np.asarray(x, dtype=float)
@@ -108,21 +131,15 @@ class PopulationChi2:
                              self.wavelength)
         ab, _, nmax = K.sphere_ab(sp, self.n_m, self.wavelength, cap,
                                   check=False)
-        item_start = torch.arange(S + 1, dtype=torch.int32, device=dev)
-        chi2, bad = K.chi2(self.coords, self.data, self.noise, sp, item_start,
-                           ab, nmax, cap, self.k, fp64=self.fp64,
-                           nonfinite=True)
+        chi2, bad = self._chi2(sp, ab, nmax, cap, self.fp64)
         chi2 = chi2.cpu().numpy()
         redo = np.flatnonzero(bad.cpu().numpy()) if not self.fp64 else []
         if len(redo):
             # candidates whose focal plane cuts the sphere: the partial
             # waves outgrow FP32's range there; FP64, as the reference
             sel = torch.from_numpy(redo).to(dev)
-            n = len(redo)
-            chi2[redo] = K.chi2(
-                self.coords, self.data, self.noise, sp[sel],
-                torch.arange(n + 1, dtype=torch.int32, device=dev),
-                ab[sel], nmax[sel], cap, self.k, fp64=True).cpu().numpy()
+            chi2[redo] = self._chi2(sp[sel], ab[sel], nmax[sel], cap,
+                                    True)[0].cpu().numpy()
         self.evaluations += S
         return float(chi2[0]) if single else chi2
 
@@ -133,7 +150,8 @@ class CropPopulations:
     it is given in one lmb_chi2_crops launch (per 65535 candidates).  The
     searches share the instrument, the noise and the precision.
 
-    searches : list of (model, data, coords, variables), as PopulationChi2.
+    searches : list of (model, data, coords, variables), as PopulationChi2;
+        the models share the instrument and the aberration.
     '''
 
     def __init__(self, searches, noise):
@@ -155,6 +173,7 @@ class CropPopulations:
         self.k = inst.wavenumber()
         self.noise = float(noise)
         self.fp64 = bool(getattr(model, 'double_precision', False))
+        self.aberr = aberration(model)
         self.evaluations = 0
 
     def evaluate(self, batch):
@@ -191,7 +210,7 @@ class CropPopulations:
         chi2, bad = K.chi2_crops(self.coords, self.data, self.noise,
                                  self.crop_start, item_crop, self.max_npts,
                                  sp, item_start, ab, nmax, cap, self.k,
-                                 fp64=self.fp64)
+                                 fp64=self.fp64, aberration=self.aberr)
         bad = bad.cpu().numpy()
         chi2 = chi2.cpu().numpy()
         redo = np.flatnonzero(bad) if not self.fp64 else []
@@ -203,7 +222,8 @@ class CropPopulations:
                 self.coords, self.data, self.noise, self.crop_start,
                 item_crop[sel], self.max_npts, sp[sel],
                 torch.arange(m + 1, dtype=torch.int32, device=dev), ab[sel],
-                nmax[sel], cap, self.k, fp64=True)[0].cpu().numpy()
+                nmax[sel], cap, self.k, fp64=True,
+                aberration=self.aberr)[0].cpu().numpy()
         return chi2
 
 

@@ -322,8 +322,9 @@ static int chi2_launch(const double* coords, long long npts, const double* data,
                        int nitems, const double* ab, const int* nmax,
                        int nmax_cap, double k, int flags, double* chi2,
                        int* nonfinite, void* workspace, size_t workspace_bytes,
-                       void* stream) {
+                       void* stream, double aberr = 0.) {
   if (nitems < 0 || npts < 0 || span < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
+  if (!isfinite(aberr)) return LMB_ERR_ARG;
   if (nitems == 0) return LMB_OK;
   if (!chi2 || !(noise > 0.)) return LMB_ERR_ARG;
   cudaStream_t st = as_stream(stream);
@@ -348,15 +349,15 @@ static int chi2_launch(const double* coords, long long npts, const double* data,
     LMB_CK(smem_attr((const void*)k_chi2<double>, smem));
     k_chi2<double><<<grid, tpb, smem, st>>>(
         coords, npts, crop_start, item_crop, ncrops, spheres, item_start,
-        reinterpret_cast<const zd*>(ab), nmax, nmax_cap + 1, k, flags, data,
-        1. / noise, partial, partial_bad);
+        reinterpret_cast<const zd*>(ab), nmax, nmax_cap + 1, k, flags, aberr,
+        data, 1. / noise, partial, partial_bad);
   } else {
     const size_t smem = sizeof(Quad<float>) * 2 * (size_t(nmax_cap) + 1);
     LMB_CK(smem_attr((const void*)k_chi2<float>, smem));
     k_chi2<float><<<grid, tpb, smem, st>>>(
         coords, npts, crop_start, item_crop, ncrops, spheres, item_start,
-        reinterpret_cast<const zd*>(ab), nmax, nmax_cap + 1, k, flags, data,
-        1. / noise, partial, partial_bad);
+        reinterpret_cast<const zd*>(ab), nmax, nmax_cap + 1, k, flags, aberr,
+        data, 1. / noise, partial, partial_bad);
   }
   LMB_CK(cudaGetLastError());
   k_chi2_reduce<<<(nitems + 127) / 128, 128, 0, st>>>(partial, partial_bad, nb,
@@ -382,13 +383,13 @@ int lmb_chi2_crops(const double* coords, long long npts, const double* data,
                    const lmb_sphere* spheres, const int* item_start, int nitems,
                    const double* ab, const int* nmax, int nmax_cap, double k,
                    int flags, double* chi2, int* nonfinite, void* workspace,
-                   size_t workspace_bytes, void* stream) {
+                   size_t workspace_bytes, void* stream, double aberration) {
   if (ncrops <= 0 || !crop_start || !item_crop || max_crop_npts > npts)
     return nitems == 0 ? LMB_OK : LMB_ERR_ARG;
   return chi2_launch(coords, npts, data, noise, crop_start, ncrops, item_crop,
                      max_crop_npts, spheres, item_start, nitems, ab, nmax,
                      nmax_cap, k, flags, chi2, nonfinite, workspace,
-                     workspace_bytes, stream);
+                     workspace_bytes, stream, aberration);
 }
 
 int lmb_jacobian(const double* coords, long long npts,

@@ -520,7 +520,7 @@ k_chi2(const double* __restrict__ coords, long long npts,
        int ncrops, const lmb_sphere* __restrict__ spheres,
        const int* __restrict__ item_start, const zd* __restrict__ ab,
        const int* __restrict__ nmax, int nmaxp, double k, int flags,
-       const double* __restrict__ data, double inv_noise,
+       double aberr, const double* __restrict__ data, double inv_noise,
        double* __restrict__ partial, int* __restrict__ partial_bad) {
   extern __shared__ __align__(16) char smem[];
   __shared__ double red[256 / 32];
@@ -572,6 +572,10 @@ k_chi2(const double* __restrict__ coords, long long npts,
       const Sums<R> sm = order_sum<R>(g, coef, nm);
       cplx<R> ep[3];
       epilogue<R>(g, sm, cart, ep);
+      if (aberr != 0.) {  // spherical aberration, as k_field
+        const cplx<R> ph = aberration_phase<R>(aberr, x - sp.x_p, y - sp.y_p, sp.z_p);
+        for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
+      }
       for (int c = 0; c < 3; ++c) e[c] = e[c] + ep[c];
     }
   }

@@ -156,11 +156,12 @@ def chi2(coords, data, noise, spheres, item_start, ab, nmax, cap, k,
 
 def chi2_crops(coords, data, noise, crop_start, item_crop, max_crop_npts,
                spheres, item_start, ab, nmax, cap, k, cartesian=True,
-               bohren=True, fp64=False):
+               bohren=True, fp64=False, aberration=0.):
     '''chi2 as above with item i compared with the pixels of its own crop
     item_crop[i], [crop_start[c], crop_start[c + 1]) of coords and data
     (lmb_chi2_crops): (nitems,) float64 sums and (nitems,) int32 counts of
-    NaN or infinite hologram pixels.'''
+    NaN or infinite hologram pixels.  ``aberration``: the coefficient c of
+    the spherical-aberration phase (0: ideal optics).'''
     coords, data, crop_start, item_crop, spheres, item_start, ab, nmax = \
         _contiguous(coords, data, crop_start, item_crop, spheres, item_start,
                     ab, nmax)
@@ -178,7 +179,7 @@ def chi2_crops(coords, data, noise, crop_start, item_crop, max_crop_npts,
         ptr(item_crop), int(max_crop_npts), ptr(spheres), ptr(item_start),
         nitems, ptr(ab), ptr(nmax), cap, float(k),
         _flags(cartesian, bohren, fp64), ptr(out), ptr(bad), ptr(ws), nbytes,
-        stream_handle(dev)), 'lmb_chi2_crops')
+        stream_handle(dev), float(aberration)), 'lmb_chi2_crops')
     return out[:nitems], bad[:nitems]
 
 

@@ -124,3 +124,39 @@ def test_aberrated_device_fit():
             shape), particle=s0, instrument=_inst()))
         rp = plain.optimize(holo)
         assert rp['redchi'] > r['redchi']
+
+
+@pytest.mark.parametrize('fp64', [True, False])
+def test_aberrated_population_objective(fp64):
+    '''The estimators' population objective for an AberratedLorenzMie
+    model applies the aberration phase in the same launch: against one
+    aberrated model.hologram() per candidate (the reference's objective,
+    NaN skipped) to 1e-10 in FP64 and FP32 accuracy otherwise; the
+    many-crop form equals the one-crop form exactly.'''
+    from pylorenzmie_b200 import AberratedLorenzMie, Sphere, LorenzMie
+    from pylorenzmie_b200.analysis._population import (PopulationChi2,
+                                                        CropPopulations,
+                                                        batchable)
+    from pylorenzmie_b200.analysis.DEEstimator import _HostObjective
+    rng = np.random.default_rng(12)
+    shape = (41, 47)
+    c = ofield.meshgrid(shape)
+    keep = rng.random(c.shape[1]) < 0.3
+    coords = c[:, keep]
+    truth = dict(zip(KEYS, [20.4, 23.1, 140., 0.8, 1.45, 0.]))
+    data = ofield.aberrated_hologram(coords, [truth], ofield.DEFAULT_INSTRUMENT,
+                                     2.) + rng.normal(0., 0.05, coords.shape[1])
+    s = Sphere(a_p=0.8, n_p=1.45, k_p=0.)
+    s.r_p = [20.4, 23.1, 140.]
+    m = AberratedLorenzMie(coordinates=coords, particle=s, instrument=_inst(),
+                           spherical=2., double_precision=fp64)
+    variables = ['z_p', 'a_p', 'n_p']
+    assert batchable(m, variables)
+    S = 24
+    X = np.vstack([rng.uniform(80., 300., S), rng.uniform(0.4, 2.0, S),
+                   rng.uniform(1.35, 1.9, S)])
+    got = PopulationChi2(m, data, coords, variables, 0.05)(X)
+    ref = _HostObjective(m, data, variables, 0.05)(X)
+    np.testing.assert_allclose(got, ref, rtol=1e-10 if fp64 else 2e-5)
+    pop = CropPopulations([(m, data, coords, variables)], 0.05)
+    np.testing.assert_array_equal(pop.evaluate({0: X})[0], got)
