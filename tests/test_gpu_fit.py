@@ -119,6 +119,28 @@ def test_fit_edge_cases():
     assert abs(df['a_p'][2] - 0.75) < 0.02
 
 
+def test_evaluation_cap():
+    '''max_nfev reached: every feature stops there with scipy's status 0
+    (not a success) and finite statistics, however many rounds the host
+    loop has queued ahead; the first evaluation's point is the start.'''
+    from pylorenzmie_b200 import Hologram, workloads
+    truth, start = workloads.batch_201(12, seed=17)
+    opt = make_optimizer(start[0], (201, 201))
+    holos = [Hologram(_render(40 + i, (201, 201), truth[i]).reshape(201, 201))
+             for i in range(12)]
+    full = opt.optimize_batch(holos, starts=start)
+    assert (full['nfev'] > 2).all()
+    for cap in (1, 2):
+        opt.settings = dict(opt.settings, max_nfev=cap)
+        df = opt.optimize_batch(holos, starts=start)
+        assert (df['nfev'] == cap).all() and (df['status'] == 0).all()
+        assert not df['success'].any()
+        assert np.isfinite(df['redchi']).all()
+        if cap == 1:
+            for j, k in enumerate(KEYS[:5]):
+                np.testing.assert_array_equal(df[k].to_numpy(), start[:, j])
+
+
 def test_autotuned_batch_matches_default(tmp_path, monkeypatch):
     from pylorenzmie_b200 import Hologram, workloads, autotune
     monkeypatch.setenv('LMB200_AUTOTUNE_CACHE', str(tmp_path / 'tune.json'))
