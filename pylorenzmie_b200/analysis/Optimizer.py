@@ -6,9 +6,12 @@ returns the same pandas Series (:166-186).  With the default settings
 (method 'lm', linear loss, x_scale 'jac') and free variables among the
 sphere's x_p, y_p, z_p, a_p, n_p, k_p, the whole fit -- residuals,
 analytic Jacobian, J^T J reduction, MINPACK's damped step and its
-convergence tests -- runs on the device in one call (``lmb_fit_batch``).
-Other settings (robust losses, 'trf'/'dogbox', explicit x_scale, instrument
-parameters as variables) keep the reference's host loop:
+convergence tests -- runs on the device in one call (``lmb_fit_batch``;
+``lmb_fit_batch_layered`` for LayeredSphere particles,
+``lmb_fit_batch_aberrated`` for an AberratedLorenzMie model whose
+``spherical`` is fixed).  Other settings (robust losses, 'trf'/'dogbox',
+explicit x_scale, instrument parameters or ``spherical`` as variables) keep
+the reference's host loop:
 scipy.optimize.least_squares calling this model's GPU ``hologram()`` and,
 when every variable is covered, its analytic ``jac()``.
 
