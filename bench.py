@@ -616,6 +616,52 @@ def run_extras(dev, inst, chosen_value):
         'median_abs_a_p_error_vs_truth_um': float(
             np.median(np.abs(est_side[:, 1] - P[:, 3])))}
 
+    # spherical aberration (s = 1.5 wavelengths, fixed: a calibrated
+    # instrument): 256 aberrated 201x201 crops through optimize_batch,
+    # beside the ideal model on the ideal rendering of the same spheres
+    from pylorenzmie_b200 import AberratedLorenzMie
+    truth, start = workloads.batch_201(256, seed=31)
+    grid = LorenzMie.meshgrid(SHAPE)
+    ma = AberratedLorenzMie(coordinates=grid, instrument=inst, spherical=1.5,
+                            double_precision=True, device=dev)
+    ha = ma.batch_hologram([[s] for s in workloads.spheres(truth)],
+                           device=True)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(31)
+    ha = (ha + inst.noise * torch.randn(ha.shape, generator=gen, device=dev,
+                                        dtype=ha.dtype)).cpu().numpy()
+    holo_a = [Hologram(ha[i].reshape(SHAPE)) for i in range(256)]
+    hi = workloads.render(truth, SHAPE, seed=31, device=dev).cpu().numpy()
+    holo_i = [Hologram(hi[i].astype(np.float64)) for i in range(256)]
+    opt_a = Optimizer(model=AberratedLorenzMie(
+        coordinates=np.zeros((2, 1)), instrument=inst, spherical=1.5,
+        device=dev))
+    opt_a.fixed = opt_a.fixed + ['spherical']
+    opt_i = Optimizer(model=LorenzMie(coordinates=np.zeros((2, 1)),
+                                      instrument=inst, device=dev))
+    rates = {}
+    for name, o, hs in (('aberrated', opt_a, holo_a), ('ideal', opt_i, holo_i)):
+        o.optimize_batch(hs, starts=start)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            df = o.optimize_batch(hs, starts=start)
+        torch.cuda.synchronize()
+        rates[name] = (256 * reps / (time.perf_counter() - t0), df)
+    dfa = rates['aberrated'][1]
+    out['aberrated_fit'] = {
+        'value': rates['aberrated'][0], 'unit': UNIT,
+        'api': 'Optimizer.optimize_batch, AberratedLorenzMie (spherical 1.5 '
+               'fixed), 256 x 201x201 crops',
+        'ideal_same_call_per_s': rates['ideal'][0],
+        'success_fraction': float(dfa['success'].mean()),
+        'mean_nfev': float(dfa['nfev'].mean()),
+        'median_abs_a_p_error_vs_truth_um': float(np.median(np.abs(
+            dfa['a_p'].to_numpy() - truth[:, 3]))),
+        'median_abs_z_p_error_vs_truth_px': float(np.median(np.abs(
+            dfa['z_p'].to_numpy() - truth[:, 2])))}
+
     # mixed crop sizes 51..301, 256 features per launch
     sides, truth, start = workloads.mixed_crops(256, seed=9)
     holos, raw = [], []

@@ -402,7 +402,8 @@ int lmb_pack_crops(const void *const *sources, const long long *counts,
  * batch: features not yet admitted end with status -4.  The call returns
  * LMB_ERR_TIMEOUT if no feature is running and no new feature has been
  * admitted for wait_seconds.  nlayers = 1 with null layer arrays fits
- * homogeneous spheres.
+ * homogeneous spheres; a nonzero aberration fits the aberrated model of
+ * lmb_fit_batch_aberrated (0: ideal optics).
  */
 int lmb_fit_batch_streamed(const lmb_feature *features, int nfeatures,
                            long long total_pixels, const float *data,
@@ -414,7 +415,8 @@ int lmb_fit_batch_streamed(const lmb_feature *features, int nfeatures,
                            const lmb_fit_settings *settings, const int *ready,
                            double wait_seconds, lmb_fit_result *results,
                            void *workspace, size_t workspace_bytes,
-                           lmb_fit_stats *stats, void *stream);
+                           lmb_fit_stats *stats, void *stream,
+                           double aberration);
 
 /*
  * lmb_fit_batch for callers that cannot allocate device memory.  No

@@ -106,7 +106,7 @@ _SIGNATURES = {
                                     _vp, _d, _d, _d, _d, _i,
                                     ctypes.POINTER(FitSettings), _vp, _d,
                                     _vp, _vp, _sz, ctypes.POINTER(FitStats),
-                                    _vp]),
+                                    _vp, _d]),
     'lmb_fit_tile_config': (_i, [_i, ctypes.POINTER(_i), ctypes.POINTER(_i),
                                  ctypes.POINTER(_i)]),
     'lmb_fit_batch': (_i, [_vp, _i, _ll, _vp, _vp, _vp, _d, _d, _d, _d, _i,

@@ -286,7 +286,8 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
     streamed (lmb_fit_batch_streamed): features are admitted as the caller
     advances it.  A nonzero ``aberration`` (the coefficient c of the
     spherical-aberration phase, AberratedLorenzMie._aberration) fits the
-    aberrated model (lmb_fit_batch_aberrated; not streamed).'''
+    aberrated model (lmb_fit_batch_aberrated, or lmb_fit_batch_streamed
+    with the coefficient).'''
     dev = d_data.device
     lib = _native.load()
     settings = dict(DEFAULT_SETTINGS if settings is None else settings)
@@ -311,9 +312,7 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
     st.max_iterations = st.max_nfev
     st.tile_config = int(tile_config)
     fs = _native.FitStats() if stats else None
-    if aberration:
-        if ready is not None:
-            raise ValueError('streamed admission fits ideal optics only')
+    if aberration and ready is None:
         if layers is None:
             L, d_frac, d_ind = 1, None, None
         else:
@@ -335,7 +334,8 @@ def fit_device(d_feat, d_data, d_coords, d_params, nfeatures, total_pixels,
             ptr(d_params), L, ptr(d_frac), ptr(d_ind), n_m, lam,
             float(instrument.magnification), float(instrument.noise),
             nmax_cap, st, ptr(ready), float(wait_seconds), ptr(d_res),
-            ptr(ws), nbytes, fs, stream_handle(dev)), 'lmb_fit_batch_streamed')
+            ptr(ws), nbytes, fs, stream_handle(dev), float(aberration)),
+            'lmb_fit_batch_streamed')
         return d_res, fs
     if layers is None:
         _native.check(lib.lmb_fit_batch(
@@ -448,9 +448,8 @@ def fit_items(items, starts, instrument, variables, settings=None,
     then converts the pixel data portion by portion into pinned memory and
     copies each on a second stream, advancing the device's admission count
     after each copy, so that conversion and transfer overlap the fitting of
-    the features already admitted.  An aberrated fit (``aberration``, see
-    fit_device) is one call.  Returns (params (B, 6), results record array,
-    npix (B,)).'''
+    the features already admitted.  ``aberration``: see fit_device.
+    Returns (params (B, 6), results record array, npix (B,)).'''
     global _flags
     starts = np.ascontiguousarray(starts, dtype=np.float64).reshape(-1, 6)
     B = starts.shape[0]
@@ -460,7 +459,7 @@ def fit_items(items, starts, instrument, variables, settings=None,
     npix = packed.features['npix'].astype(np.int64)
     if chunks is None:
         chunks = default_chunks(npix)
-    if B == 0 or chunks <= 1 or aberration:
+    if B == 0 or chunks <= 1:
         params, res = fit_packed(packed, starts, instrument, variables,
                                  settings, device, layers=layers,
                                  autotune=autotune, aberration=aberration)
@@ -469,7 +468,7 @@ def fit_items(items, starts, instrument, variables, settings=None,
     nmax_cap = fit_capacity(starts, float(instrument.n_m),
                             float(instrument.wavelength), layers)
     tile_config = 0
-    if autotune:
+    if autotune and not aberration:   # the aberrated fit has one shape
         from .. import autotune as _tuner
         tile_config = _tuner.tune(packed, starts, instrument, variables,
                                   nmax_cap, layers, dev)
@@ -510,7 +509,8 @@ def fit_items(items, starts, instrument, variables, settings=None,
     future = _worker().submit(_fit_streamed, s_fit, d_feat, d_data, d_coords,
                               d_params, B, packed.total, instrument,
                               variables, settings, nmax_cap, starts,
-                              tile_config, layers, d_ready, wait_seconds)
+                              tile_config, layers, d_ready, wait_seconds,
+                              aberration)
     offs = packed.features['data_offset']
     try:
         for k, (a, b) in enumerate(ranges):
@@ -543,13 +543,13 @@ def fit_items(items, starts, instrument, variables, settings=None,
 
 def _fit_streamed(stream, d_feat, d_data, d_coords, d_params, n, total,
                   instrument, variables, settings, nmax_cap, starts,
-                  tile_config, layers, d_ready, wait_seconds):
+                  tile_config, layers, d_ready, wait_seconds, aberration=0.):
     with torch.cuda.stream(stream):
         d_res, _ = fit_device(d_feat, d_data, d_coords, d_params, n, total,
                               instrument, variables, settings, nmax_cap,
                               starts, False, tile_config=tile_config,
                               layers=layers, ready=d_ready,
-                              wait_seconds=wait_seconds)
+                              wait_seconds=wait_seconds, aberration=aberration)
         params = d_params.view(torch.float64).reshape(n, 6).cpu().numpy()
         res = d_res[:n * _native.RESULT_DTYPE.itemsize].cpu().numpy().view(
             _native.RESULT_DTYPE).copy()

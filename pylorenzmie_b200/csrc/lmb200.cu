@@ -861,13 +861,14 @@ int lmb_fit_batch_streamed(const lmb_feature* features, int nfeatures,
                            const lmb_fit_settings* settings, const int* ready,
                            double wait_seconds, lmb_fit_result* results,
                            void* workspace, size_t workspace_bytes,
-                           lmb_fit_stats* stats, void* stream) {
+                           lmb_fit_stats* stats, void* stream,
+                           double aberration) {
   if (!ready || !(wait_seconds >= 0.)) return LMB_ERR_ARG;
   return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
                         n_m, wavelength, magnification, noise, nmax_cap,
                         settings, results, workspace, workspace_bytes, stats,
                         stream, nlayers, layer_fractions, layer_indices, ready,
-                        wait_seconds);
+                        wait_seconds, false, aberration);
 }
 int lmb_fit_batch_aberrated(const lmb_feature* features, int nfeatures,
                             long long total_pixels, const float* data,

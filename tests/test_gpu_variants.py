@@ -75,8 +75,8 @@ def test_aberrated_device_fit():
     lm on a forward-difference Jacobian of the FP64 aberrated model, as the
     reference's Optimizer does on an AberratedLorenzMie) the parameters
     agree to the fit targets or a third of their uncertainty, it recovers
-    the sphere, and optimize_batch / optimize_stream give optimize's
-    result exactly.'''
+    the sphere, and optimize_batch (one call or streamed admission) and
+    optimize_stream give optimize's result exactly.'''
     from oracle import fit as ofit
     from pylorenzmie_b200 import (AberratedLorenzMie, Sphere, Optimizer,
                                   Hologram, LorenzMie)
@@ -114,9 +114,13 @@ def test_aberrated_device_fit():
         starts = np.array([start, start])
         df = opt.optimize_batch([holo, holo], starts=starts)
         dfs = next(opt.optimize_stream(iter([([holo, holo], starts)])))
+        # streamed admission (the batch in three portions) too
+        dfc = opt.optimize_batch([holo] * 3, starts=np.array([start] * 3),
+                                 chunks=3)
         for k in tol:
             assert np.all(df[k].to_numpy() == r[k]), k
             assert np.all(dfs[k].to_numpy() == r[k]), k
+            assert np.all(dfc[k].to_numpy() == r[k]), k
         # the ideal model fits the aberrated data worse
         s0 = Sphere(a_p=start[3], n_p=start[4], k_p=0.)
         s0.r_p = start[:3]
