@@ -206,6 +206,22 @@ int lmb_jacobian(const double *coords, long long npts,
                  int flags, double *holo, double *jac, void *stream);
 
 /*
+ * lmb_jacobian for an instrument with spherical aberration: the hologram
+ * |E e^{i Phi} + x|^2 and its derivatives, with the phase and coefficient
+ * of lmb_fit_batch_aberrated (aberration = c = 4 n_m^3 s / k).  Fills the
+ * analytic-Jacobian slot for AberratedLorenzMie models (the reference's
+ * JAX backend differentiates the aberrated model, theory/Aberrated.py:
+ * 62-85 on theory/jaxLorenzMie.py:354-395); the spherical coefficient
+ * itself is not a column.  aberration 0 gives lmb_jacobian's output.
+ */
+int lmb_jacobian_aberrated(const double *coords, long long npts,
+                           const lmb_sphere *spheres, int nitems,
+                           const double *ab, const double *dab,
+                           const int *nmax, int nmax_cap, double k, int flags,
+                           double aberration, double *holo, double *jac,
+                           void *stream);
+
+/*
  * Vector-Jacobian product of the hologram: grad[i][j] =
  * sum_p gout[i][p] dH_i[p]/d param_j for single-sphere items, without
  * forming the Jacobian (the backward pass of an autograd function).

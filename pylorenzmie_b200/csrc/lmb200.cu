@@ -392,11 +392,20 @@ int lmb_chi2_crops(const double* coords, long long npts, const double* data,
                      workspace_bytes, stream, aberration);
 }
 
-int lmb_jacobian(const double* coords, long long npts,
-                 const lmb_sphere* spheres, int nitems, const double* ab,
-                 const double* dab, const int* nmax, int nmax_cap, double k,
-                 int flags, double* holo, double* jac, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// Hologram + Jacobian launch for lmb_jacobian (kAberr false) and
+// lmb_jacobian_aberrated.
+template <bool kAberr>
+int jacobian_launch(const double* coords, long long npts,
+                    const lmb_sphere* spheres, int nitems, const double* ab,
+                    const double* dab, const int* nmax, int nmax_cap, double k,
+                    int flags, double* holo, double* jac, void* stream,
+                    double aberr) {
   if (nitems < 0 || npts < 0 || bad_cap(nmax_cap)) return LMB_ERR_ARG;
+  if (!isfinite(aberr)) return LMB_ERR_ARG;
   if (nitems == 0 || npts == 0) return LMB_OK;
   if (!coords || !spheres || !ab || !dab || !nmax || !jac) return LMB_ERR_ARG;
   if (!(flags & LMB_CARTESIAN) || (flags & LMB_FP64)) return LMB_ERR_UNSUPPORTED;
@@ -404,22 +413,47 @@ int lmb_jacobian(const double* coords, long long npts,
   const int tpb = 128;
   const size_t psmem = sizeof(float4) * PAIR_QUADS * (size_t(nmax_cap) + 1);
   if (psmem <= kPairSmemLimit) {  // packed two-pixel loop
-    LMB_CK(smem_attr((const void*)k_jacobian_pair, psmem));
+    LMB_CK(smem_attr((const void*)k_jacobian_pair<kAberr>, psmem));
     dim3 grid(unsigned((npts + 2 * tpb - 1) / (2 * tpb)), unsigned(nitems));
-    k_jacobian_pair<<<grid, tpb, psmem, as_stream(stream)>>>(
+    k_jacobian_pair<kAberr><<<grid, tpb, psmem, as_stream(stream)>>>(
         coords, npts, spheres, reinterpret_cast<const zd*>(ab),
-        reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, holo, jac);
+        reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, holo, jac,
+        aberr);
     LMB_CK(cudaGetLastError());
     return LMB_OK;
   }
   const size_t smem = sizeof(Quad<float>) * JAC_QUADS * (size_t(nmax_cap) + 1);
-  LMB_CK(smem_attr((const void*)k_jacobian, smem));
+  LMB_CK(smem_attr((const void*)k_jacobian<kAberr>, smem));
   dim3 grid(unsigned((npts + tpb - 1) / tpb), unsigned(nitems));
-  k_jacobian<<<grid, tpb, smem, as_stream(stream)>>>(
+  k_jacobian<kAberr><<<grid, tpb, smem, as_stream(stream)>>>(
       coords, npts, spheres, reinterpret_cast<const zd*>(ab),
-      reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, holo, jac);
+      reinterpret_cast<const zd*>(dab), nmax, nmax_cap + 1, k, flags, holo, jac,
+      aberr);
   LMB_CK(cudaGetLastError());
   return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lmb_jacobian(const double* coords, long long npts,
+                 const lmb_sphere* spheres, int nitems, const double* ab,
+                 const double* dab, const int* nmax, int nmax_cap, double k,
+                 int flags, double* holo, double* jac, void* stream) {
+  return jacobian_launch<false>(coords, npts, spheres, nitems, ab, dab, nmax,
+                                nmax_cap, k, flags, holo, jac, stream, 0.);
+}
+
+int lmb_jacobian_aberrated(const double* coords, long long npts,
+                           const lmb_sphere* spheres, int nitems,
+                           const double* ab, const double* dab,
+                           const int* nmax, int nmax_cap, double k, int flags,
+                           double aberration, double* holo, double* jac,
+                           void* stream) {
+  return jacobian_launch<true>(coords, npts, spheres, nitems, ab, dab, nmax,
+                               nmax_cap, k, flags, holo, jac, stream,
+                               aberration);
 }
 
 size_t lmb_vjp_workspace_bytes(long long npts, int nitems) {

@@ -647,11 +647,14 @@ __device__ inline void holo_jac_pixel(const Geometry<float>& g,
   }
 }
 
+// kAberr: the spherical-aberration phase of coefficient aberr in the
+// hologram and the x_p, y_p, z_p columns (lmb_jacobian_aberrated).
+template <bool kAberr = false>
 __global__ void __launch_bounds__(128)
 k_jacobian(const double* __restrict__ coords, long long npts,
            const lmb_sphere* __restrict__ spheres, const zd* __restrict__ ab,
            const zd* __restrict__ dab, const int* __restrict__ nmax, int nmaxp,
-           double k, int flags, double* holo, double* jac) {
+           double k, int flags, double* holo, double* jac, double aberr = 0.) {
   extern __shared__ __align__(16) char smem[];
   Quad<float>* coef = reinterpret_cast<Quad<float>*>(smem);
   const int item = blockIdx.y;
@@ -666,7 +669,8 @@ k_jacobian(const double* __restrict__ coords, long long npts,
   const Geometry<float> g = geometry<float>(k, x - sp.x_p, y - sp.y_p, z - sp.z_p,
                                             z, sp.z_p, flags & LMB_BOHREN);
   float H, dH[6];
-  holo_jac_pixel(g, coef, nm, float(k), &H, dH);
+  holo_jac_pixel<kAberr>(g, coef, nm, float(k), &H, dH, aberr, x - sp.x_p,
+                         y - sp.y_p, sp.z_p);
   if (holo) holo[(size_t)item * npts + pix] = H;
   double* jo = jac + (size_t)item * 6 * npts;
   for (int j = 0; j < 6; ++j) jo[j * npts + pix] = dH[j];
@@ -674,11 +678,12 @@ k_jacobian(const double* __restrict__ coords, long long npts,
 
 // k_jacobian with the packed two-pixel loop: each thread takes two adjacent
 // pixels (pair records, stage_pair).
+template <bool kAberr = false>
 __global__ void __launch_bounds__(128, 3)
 k_jacobian_pair(const double* __restrict__ coords, long long npts,
                 const lmb_sphere* __restrict__ spheres, const zd* __restrict__ ab,
                 const zd* __restrict__ dab, const int* __restrict__ nmax, int nmaxp,
-                double k, int flags, double* holo, double* jac) {
+                double k, int flags, double* holo, double* jac, double aberr = 0.) {
   extern __shared__ __align__(16) char smem[];
   float4* rec = reinterpret_cast<float4*>(smem);
   const int item = blockIdx.y;
@@ -704,7 +709,14 @@ k_jacobian_pair(const double* __restrict__ coords, long long npts,
     const long long pix = l ? p1 : p0;
     const JacSums<float> A = pair_lane(P, l, g[l].smu);
     float H, dH[6];
-    holo_jac_reverse<float>(g[l], A, float(k), &H, dH);
+    if constexpr (kAberr) {
+      float dphi[3], hphi;
+      const cplx<float> w = aberration_wave<float>(aberr, dx[l], dy[l], sp.z_p, dphi);
+      holo_jac_reverse<float, true>(g[l], A, float(k), &H, dH, w, &hphi);
+      for (int j = 0; j < 3; ++j) dH[j] += hphi * dphi[j];
+    } else {
+      holo_jac_reverse<float>(g[l], A, float(k), &H, dH);
+    }
     if (holo) holo[(size_t)item * npts + pix] = H;
     for (int j = 0; j < 6; ++j) jo[j * npts + pix] = dH[j];
   }

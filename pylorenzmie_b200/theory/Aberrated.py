@@ -14,8 +14,9 @@ among an Optimizer's fixed parameters (a calibrated instrument), optimize,
 optimize_batch and optimize_stream fit this model on the GPU.  With it free
 -- the reference's default, whose fixed list does not name it -- the fit
 runs through scipy's host loop on this model's holograms, as the
-reference's does.  ``jac()`` does not include the aberration, and
-``jac_params`` is empty when spherical != 0.
+reference's does.  ``jac()`` includes the aberration
+(lmb_jacobian_aberrated); ``spherical`` itself has no column, so a host
+fit that frees it differentiates it numerically.
 '''
 from .LorenzMie import LorenzMie
 
@@ -37,10 +38,6 @@ def Aberrated(base_class):
         def properties(self, properties):
             base_class.properties.fset(self, properties)
 
-        @property
-        def jac_params(self):
-            return (base_class.jac_params if self.spherical == 0.
-                    else frozenset())
 
         def _aberration(self):
             if self.spherical == 0.:
@@ -48,10 +45,6 @@ def Aberrated(base_class):
             inst = self.instrument
             return 4. * inst.n_m ** 3 / inst.wavenumber() * self.spherical
 
-        def jac(self, *args, **kwargs):
-            if self.spherical != 0.:
-                raise TypeError('jac() does not include spherical aberration')
-            return super().jac(*args, **kwargs)
 
     return AberratedLorenzMie
 

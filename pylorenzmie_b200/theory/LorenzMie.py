@@ -244,7 +244,8 @@ class LorenzMie(LMObject):
         sp, _, ab, dab, nmax, cap = self._prepare([[self.particle]],
                                                   deriv=True)
         _, J = K.jacobian(self._coords, sp, ab, dab, nmax, cap,
-                          self.instrument.wavenumber())
+                          self.instrument.wavenumber(),
+                          aberration=self._aberration())
         J = J[0]
         if device:
             return {k: J[i] for i, k in enumerate(JAC_KEYS)}
@@ -256,5 +257,6 @@ class LorenzMie(LMObject):
         sp, _, ab, dab, nmax, cap = self._prepare([[self.particle]],
                                                   deriv=True)
         h, J = K.jacobian(self._coords, sp, ab, dab, nmax, cap,
-                          self.instrument.wavenumber(), bohren)
+                          self.instrument.wavenumber(), bohren,
+                          aberration=self._aberration())
         return h[0], J[0]

@@ -209,8 +209,11 @@ def field(coords, spheres, item_start, ab, nmax, cap, k, cartesian=True,
     return out
 
 
-def jacobian(coords, spheres, ab, dab, nmax, cap, k, bohren=True):
-    '''Holograms (n, npts) and Jacobians (n, 6, npts), float64, FP32 sums.'''
+def jacobian(coords, spheres, ab, dab, nmax, cap, k, bohren=True,
+             aberration=0.):
+    '''Holograms (n, npts) and Jacobians (n, 6, npts), float64, FP32 sums;
+    ``aberration``: the coefficient c of the spherical-aberration phase
+    (lmb_jacobian_aberrated; 0: ideal optics).'''
     coords, spheres, ab, dab, nmax = _contiguous(
         coords, spheres, ab, dab, nmax)
     lib = _native.load()
@@ -219,6 +222,12 @@ def jacobian(coords, spheres, ab, dab, nmax, cap, k, bohren=True):
     n = spheres.shape[0]
     holo = torch.empty((n, npts), dtype=torch.float64, device=dev)
     jac = torch.empty((n, 6, npts), dtype=torch.float64, device=dev)
+    if aberration:
+        _native.check(lib.lmb_jacobian_aberrated(
+            ptr(coords), npts, ptr(spheres), n, ptr(ab), ptr(dab), ptr(nmax),
+            cap, float(k), _flags(True, bohren, False), float(aberration),
+            ptr(holo), ptr(jac), stream_handle(dev)), 'lmb_jacobian_aberrated')
+        return holo, jac
     _native.check(lib.lmb_jacobian(ptr(coords), npts, ptr(spheres), n, ptr(ab),
                                    ptr(dab), ptr(nmax), cap, float(k),
                                    _flags(True, bohren, False), ptr(holo),
