@@ -32,6 +32,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = 'features fitted/s (LM, 201² crops)'
 UNIT = 'features/s'
+WORKLOAD = ('batched LM fit, 201x201 single-sphere crops (a_p 0.75 um, n_p '
+            '1.42, z_p 200 px, start +5%/+0.02/+10 px)')
 BATCH = 256
 SHAPE = (201, 201)
 ROTATE = 4  # distinct input batches cycled through (4 x 41 MB > 126 MB L2)
@@ -103,9 +105,12 @@ def reference_arm(args):
         'ms_per_step': 1e3 * sum(times) / len(times),
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f64', 'data': 'synthetic (seeded)',
-        'config': {'workload': f'LM fit of 201x201 single-sphere crops, '
-                               f'{sample} features per step on the host',
+        'config': {'workload': WORKLOAD + ', FP64 model + scipy lm with a '
+                               'forward-difference Jacobian (the reference '
+                               'algorithm)',
                    'global_batch': sample, 'crop': '201x201',
+                   'sample': f'{sample} features per step (a bounded sample '
+                             'of the GPU arm\'s 256-feature batch)',
                    'parallelism': f'{cores} host processes'},
         'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores,
                          'kind': 'port',
@@ -382,10 +387,8 @@ def b200_arm(args):
         'ms_per_step': ms / args.steps, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
         'data': 'synthetic (seeded); rendered by the FP64 kernel + N(0, 0.05)',
-        'config': {'workload': 'batched LM fit, 201x201 single-sphere crops '
-                               '(a_p 0.75 um, n_p 1.42, z_p 200 px, start '
-                               '+5%/+0.02/+10 px), FP64 Mie coefficients + '
-                               'FP32 sums + analytic Jacobian',
+        'config': {'workload': WORKLOAD + ', FP64 Mie coefficients + FP32 '
+                               'sums + analytic Jacobian',
                    'global_batch': B * world, 'per_gpu_batch': B,
                    'crop': '201x201', 'parallelism': f'features sharded '
                    f'over {world} GPU(s), no collective',
