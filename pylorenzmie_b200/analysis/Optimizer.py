@@ -325,7 +325,7 @@ class Optimizer(LMObject):
         return batch_frame(params, res, npix, self.variables)
 
 
-    def optimize_stream(self, batches, autotune=None, depth=2):
+    def optimize_stream(self, batches, autotune=None, depth=None):
         '''Fit a stream of batches (video frames, say), pipelined: while
         the GPU fits one batch, the next is converted and copied.  Yields
         one DataFrame per batch, in order, as optimize_batch returns it.
@@ -335,9 +335,11 @@ class Optimizer(LMObject):
                   list of Sphere or LayeredSphere start values
         autotune: time the evaluation kernel's launch shapes on the first
                   batch (default: when it has 64 features or more)
-        depth   : fits running at once (default 2, which keeps the GPU
-                  busy); the next batch is converted and copied while they
-                  run
+        depth   : fits running at once; the next batch is converted and
+                  copied while they run.  Default 2, which keeps the GPU
+                  busy; 4 when the first batch holds LayeredSphere
+                  particles, whose batches end with long single-fit tails
+                  that further fits fill
         '''
         if not self._device_fit_ok() and not (
                 set(self.variables) <= set(PARAM_KEYS)):
@@ -374,6 +376,8 @@ class Optimizer(LMObject):
         def chain():
             yield head
             yield from gen
+        if depth is None:
+            depth = 2 if head[2] is None else 4
         for params, res, npix in _fit.fit_stream(
                 chain(), self.model.instrument, variables, self.settings,
                 device=self.model.device, autotune=self._stream_tune,

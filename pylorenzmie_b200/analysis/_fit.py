@@ -590,20 +590,31 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
     Up to ``depth`` fits run at once, each driven by a worker thread on a
     stream of its own (consecutive fits overlap on the GPU).  The caller's
     thread converts the next batch into one of depth + 1 pinned buffers and
-    copies it on the copy stream before it waits for the oldest fit, so
-    that batch's data is on the device when a fit slot frees; its fit waits
-    for that copy on the device, not on the host.  A pinned buffer is
-    rewritten only after its previous copy has completed.'''
+    copies it on the copy stream before it waits for a fit slot, so that
+    batch's data is on the device when a slot frees; its fit waits for that
+    copy on the device, not on the host.  A slot frees when any running fit
+    ends, not only the oldest, so a batch whose slowest fit takes many
+    rounds holds one slot while later batches pass through the others;
+    finished batches wait, up to 8 x depth of them, to be yielded in order.
+    A pinned buffer is rewritten only after its previous copy has
+    completed.'''
     from collections import deque
+    from concurrent.futures import wait, FIRST_COMPLETED
     dev = get_device(device)
     _, s_copy = _fit_streams(dev)
     nstage = depth + 1
     while len(_stream_staging) < nstage:
         _stream_staging.append(_Staging())
-    pending = deque()          # (future, copy-done event)
+    pending = deque()          # (future or None, extra), submission order
+    running = {}               # future -> fit slot (its stream)
+    free = list(range(depth))
     done_events = [None] * nstage
     tile_config = None
     k = 0
+
+    def ready_head():
+        return pending and (pending[0][0] is None or pending[0][0].done())
+
     try:
         for items, starts, layers in batches:
             starts = np.ascontiguousarray(starts, dtype=np.float64
@@ -626,7 +637,6 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
                                               variables, nmax_cap, layers,
                                               dev)
             slot = k % nstage
-            s_fit = _stream_fit_stream(dev, k % depth)
             if done_events[slot] is not None:
                 done_events[slot].synchronize()  # its last copy has landed
             buf, offs, nbytes = stage(packed, starts, _stream_staging[slot])
@@ -635,16 +645,26 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
                 ev = torch.cuda.Event()
                 ev.record(s_copy)
             done_events[slot] = ev
+            # this batch's data is on its way: now wait for a fit slot
+            while not free:
+                finished, _ = wait(list(running), return_when=FIRST_COMPLETED)
+                for f in finished:
+                    free.append(running.pop(f))
+            while ready_head():
+                yield _collect(pending.popleft())
+            while len(pending) >= 8 * depth:   # bound the finished backlog
+                yield _collect(pending.popleft())
+            fit_slot = free.pop(0)
+            s_fit = _stream_fit_stream(dev, fit_slot)
             for v in views:
                 if v is not None:
                     v.record_stream(s_fit)
-            # this batch's data is on its way: now wait for a fit slot
-            while len(pending) >= depth:
-                yield _collect(pending.popleft())
-            pending.append((_stream_worker(depth).submit(
+            fut = _stream_worker(depth).submit(
                 _fit_after, s_fit, ev, views, B, packed.total, instrument,
                 variables, settings, nmax_cap, starts, tile_config, layers,
-                aberration), npix))
+                aberration)
+            running[fut] = fit_slot
+            pending.append((fut, npix))
             k += 1
         while pending:
             yield _collect(pending.popleft())
