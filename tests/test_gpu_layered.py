@@ -112,3 +112,42 @@ def test_layered_batch_fit_vs_oracle(tight):
     r = Optimizer(model=m, settings=dict(TIGHT) if tight else None
                   ).optimize(holos[0])
     assert abs(r['a_p'] - oracle[0]['a_p']) <= 1e-3
+
+
+def test_layered_aberrated_fit_vs_oracle():
+    """Three-layer spheres seen through spherical aberration (s = 1.5,
+    fixed): the device fit (lmb_fit_batch_aberrated with layers) and the
+    oracle fit of the same aberrated layered model, both converged tightly,
+    meet within a_p 1 nm, n_p 1e-4, x/y/z_p 0.02 px."""
+    from pylorenzmie_b200 import (AberratedLorenzMie, Optimizer, Hologram,
+                                  workloads)
+    sides, truth, start, frac, core = workloads.layered(2, seed=5)
+    sides[:] = [111, 121]
+    c = (sides - 1) / 2.
+    truth[:, 0] = c + 0.3
+    truth[:, 1] = c - 0.4
+    start[:, :2] = truth[:, :2]
+    holos, oracle = [], []
+    for i, s in enumerate(sides):
+        g = ofield.meshgrid((s, s))
+        h = ofield.aberrated_hologram(
+            g, [_oracle_particle(truth[i], frac[i], core[i])],
+            ofield.DEFAULT_INSTRUMENT, 1.5)
+        d = h + np.random.default_rng(80 + i).normal(0., 0.05, h.shape)
+        holos.append(Hologram(d.reshape(s, s)))
+        po = _oracle_particle(start[i], frac[i], core[i])
+        del po['layers']
+        oracle.append(ofit.fit(d, g, po, ofield.DEFAULT_INSTRUMENT,
+                               settings=dict(TIGHT), spherical=1.5))
+    particles = workloads.layered_spheres(start, frac, core)
+    opt = Optimizer(model=AberratedLorenzMie(coordinates=np.zeros((2, 1)),
+                                             spherical=1.5),
+                    settings=dict(TIGHT))
+    opt.fixed = opt.fixed + ['spherical']
+    df = opt.optimize_batch(holos, particles=particles)
+    tol = {'x_p': 0.02, 'y_p': 0.02, 'z_p': 0.02, 'a_p': 1e-3, 'n_p': 1e-4}
+    for i in range(2):
+        o = oracle[i]
+        assert o['success'] and df['success'][i]
+        for k, t in tol.items():
+            assert abs(df[k][i] - o[k]) <= t, (i, k, df[k][i], o[k])
