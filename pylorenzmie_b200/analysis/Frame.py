@@ -22,6 +22,30 @@ from .Hologram import Hologram
 from .Feature import Feature
 from .DEEstimator import estimate_many
 from . import _fit
+from ._fit import PARAM_KEYS
+
+
+def _result_table(n, tables):
+    '''DataFrame of n features' Optimizer.result rows (variables with their
+    uncertainties, success, npix, redchi) from the batched groups' arrays;
+    the same values and column types as pd.DataFrame of the Series.'''
+    variables = tables[0][1]
+    nv = len(variables)
+    x, dp = np.empty((n, nv)), np.empty((n, nv))
+    success = np.empty(n, dtype=bool)
+    npix = np.empty(n, dtype=np.int64)
+    redchi = np.empty(n)
+    for idx, _, xs, ds, ss, ns, rs in tables:
+        x[idx], dp[idx], success[idx], npix[idx], redchi[idx] = \
+            xs, ds, ss, ns, rs
+    cols = {}
+    for j, v in enumerate(variables):
+        cols[v] = x[:, j]
+        cols['d' + v] = dp[:, j]
+    cols['success'] = success
+    cols['npix'] = npix
+    cols['redchi'] = redchi
+    return pd.DataFrame(cols)
 
 
 class Frame(Hologram):
@@ -152,6 +176,7 @@ class Frame(Hologram):
                    str(f.model.device), opt._aberration())
             groups.setdefault(key, []).append(i)
         done = set()
+        tables = []   # per group: the columns of Optimizer.result
         for key, idx in groups.items():
             members = [feats[i] for i in idx]
             opt0 = members[0].optimizer
@@ -168,6 +193,17 @@ class Frame(Hologram):
                     items[j][2] is not None else f.flat_coordinates
                 f.optimizer._accept(params[j], res[j])
             done.update(idx)
+            cols = [PARAM_KEYS.index(v) for v in opt0.variables]
+            tables.append((idx, tuple(opt0.variables), params[:, cols],
+                           res['dparams'][:, cols],
+                           res['success'].astype(bool),
+                           np.array([np.asarray(it[0]).size for it in items]),
+                           res['redchi'].astype(float)))
+        if len(done) == len(feats) and len({t[1] for t in tables}) == 1:
+            # every feature fitted on the device with one variable list:
+            # the table of their result Series, built from the arrays
+            self._results = _result_table(len(feats), tables)
+            return self._results
         results = []
         for i, f in enumerate(feats):
             if i not in done:

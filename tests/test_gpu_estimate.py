@@ -239,6 +239,7 @@ def _frame_data(shape=(200, 400), seed=4):
 def test_frame_optimize_batches_features():
     '''Frame.optimize (one batched device fit) gives each feature exactly
     the result of its own Optimizer.optimize on the same pixels.'''
+    import pandas as pd
     from pylorenzmie_b200 import Frame, Instrument
     data, truth, bboxes = _frame_data()
     inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
@@ -262,6 +263,11 @@ def test_frame_optimize_batches_features():
         for k in batched.columns:
             assert batched.iloc[i][k] == single[i][k], (i, k)
         assert abs(batched.iloc[i]['a_p'] - truth[i][3]) < 0.03
+    # the table is the features' result Series, as the reference builds it
+    # (analysis/Frame.py:172-173): same values and column types
+    pd.testing.assert_frame_equal(batched, pd.DataFrame(single))
+    pd.testing.assert_frame_equal(
+        batched, pd.DataFrame([ft.optimizer.result for ft in fa.features]))
     # each feature keeps its own result, as after feature.optimize()
     for feat, (_, row) in zip(fa.features, batched.iterrows()):
         assert feat.optimizer.result['z_p'] == row['z_p']
