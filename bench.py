@@ -576,12 +576,13 @@ def run_extras(dev, inst, chosen_value):
     def _no_stop(xk, convergence):
         return False
 
-    def estimate_frame(side, scipy_code=False):
+    def estimate_frame(side, scipy_code=False, device=False):
         f = Frame(instrument=inst)
         f.data = fdata
         f.bboxes = boxes
         for i, feat in enumerate(f.features):
             feat.estimator.seed = 40 + i
+            feat.estimator.device_search = device
             if scipy_code:
                 feat.estimator.settings = dict(feat.estimator.settings,
                                                callback=_no_stop)
@@ -607,6 +608,8 @@ def run_extras(dev, inst, chosen_value):
     torch.cuda.synchronize()
     t_fit = time.perf_counter() - t0
     t_one, est_one, _ = estimate_frame(False)
+    estimate_frame(True, device=True)                 # warm-up
+    t_dev, est_dev, _ = estimate_frame(True, device=True)
     t_side_sp, est_side_sp, _ = estimate_frame(True, True)
     t_one_sp, est_one_sp, _ = estimate_frame(False, True)
     nref = 2
@@ -633,6 +636,16 @@ def run_extras(dev, inst, chosen_value):
         'oracle_numpy_per_s': nref / t_ref,
         'median_abs_a_p_error_vs_truth_um': float(
             np.median(np.abs(est_side[:, 1] - P[:, 3]))),
+        'device_search': {
+            'per_s': nest / t_dev,
+            'api': 'the same estimators with device_search=True (the '
+                   'search on the GPU, its own random stream)',
+            'median_abs_a_p_error_vs_truth_um': float(
+                np.median(np.abs(est_dev[:, 1] - P[:, 3]))),
+            'median_abs_z_p_error_vs_truth_px': float(
+                np.median(np.abs(est_dev[:, 0] - P[:, 2]))),
+            'scipy_median_abs_z_p_error_vs_truth_px': float(
+                np.median(np.abs(est_side[:, 0] - P[:, 2])))},
         'then_frame_optimize': {
             'features_per_s': nest / t_fit,
             'estimate_plus_optimize_frames_per_s': 1. / (t_side + t_fit),

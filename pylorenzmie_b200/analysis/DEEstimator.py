@@ -25,6 +25,7 @@ from scipy.optimize import differential_evolution
 from .BaseEstimator import BaseEstimator
 from .Mask import Mask
 from ._de import run_populations, supported
+from ._device_de import device_searches
 from ._population import (CropPopulations, PopulationChi2, aberration,
                           batchable, de_settings, lockstep_de)
 
@@ -57,10 +58,16 @@ class _HostObjective:
 
 
 def run_search(model, data, coords, variables, bounds, noise, popsize, seed,
-               settings):
+               settings, device_search=False):
     '''scipy differential_evolution over ``variables`` with the population
     objective; returns the OptimizeResult.  The model's coordinates are
-    restored on exit.'''
+    restored on exit.  ``device_search``: the whole search on the GPU
+    (device_searches), where the model and settings allow it.'''
+    if device_search and batchable(model, variables) and supported(settings):
+        return device_searches([dict(
+            model=model, data=data, coords=coords, variables=variables,
+            bounds=bounds, noise=noise, popsize=popsize, seed=seed,
+            settings=settings)])[0]
     saved = model.coordinates
     try:
         if batchable(model, variables):
@@ -101,8 +108,18 @@ def run_searches(searches, workers=256):
         key = (str(m.device), float(inst.n_m), float(inst.wavelength),
                float(inst.magnification), float(sr['noise']),
                bool(getattr(m, 'double_precision', False)), aberration(m))
+        if sr.get('device_search') and supported(sr['settings']):
+            # one device loop: the same variables, population and mutation
+            st = sr['settings'] or {}
+            key = key + ('device', tuple(sr['variables']), sr['popsize'],
+                         repr(st.get('mutation', (0.5, 1))))
         groups.setdefault(key, []).append(i)
     for key, idx in groups.items():
+        if key is not None and 'device' in key:
+            out = device_searches([searches[i] for i in idx])
+            for i, r in zip(idx, out):
+                results[i] = r
+            continue
         if key is None or len(idx) == 1:
             for i in idx:
                 results[i] = run_search(**searches[i])
@@ -151,6 +168,7 @@ class DEEstimator(BaseEstimator):
                                                      'polish': False,
                                                      'updating': 'deferred',
                                                      'workers': -1})
+    device_search: bool = False   # the whole search on the GPU
 
     @property
     def properties(self):
@@ -177,7 +195,8 @@ class DEEstimator(BaseEstimator):
                     variables=list(self.bounds.keys()),
                     bounds=list(self.bounds.values()),
                     noise=self.model.instrument.noise, popsize=self.popsize,
-                    seed=self.seed, settings=self.settings)
+                    seed=self.seed, settings=self.settings,
+                    device_search=self.device_search)
 
     def accept(self, search, result):
         '''Leave the model at the search's result; its properties as a

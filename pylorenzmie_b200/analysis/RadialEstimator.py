@@ -29,6 +29,7 @@ class RadialEstimator(BaseEstimator):
                                                      'polish': False,
                                                      'updating': 'deferred',
                                                      'workers': 1})
+    device_search: bool = False   # the whole search on the GPU
 
     @property
     def properties(self):
@@ -57,7 +58,8 @@ class RadialEstimator(BaseEstimator):
                     variables=list(self.bounds.keys()),
                     bounds=list(self.bounds.values()),
                     noise=self.model.instrument.noise, popsize=self.popsize,
-                    seed=self.seed, settings=self.settings)
+                    seed=self.seed, settings=self.settings,
+                    device_search=self.device_search)
 
     def accept(self, search, result):
         '''Leave the model at the search's result; its properties as a

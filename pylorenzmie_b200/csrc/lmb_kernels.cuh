@@ -1440,4 +1440,170 @@ __global__ void k_fit_finalize(FitCtx c) {
   c.results[f] = r;
 }
 
+// ---------------------------------------------------------------------------
+// Differential evolution on the device: the searches of many features
+// stepped together -- k_de_trial forms every search's trial population
+// (one thread per candidate) and the sphere records to evaluate, the caller
+// evaluates them (lmb_sphere_ab + lmb_chi2_crops), k_de_select keeps the
+// better of each pair and tests convergence (one warp per search).  The
+// step is scipy's best1bin with deferred updating, dithered mutation and
+// binomial crossover; the random numbers come from the SplitMix64 mixing
+// function (Steele, Lea and Flood, OOPSLA 2014) of a counter (search key,
+// generation, candidate, draw), so a search is reproducible for a seed but
+// does not follow scipy's random stream.
+
+__device__ inline unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Uniform in [0, 1) from the top 53 bits of the hash of (key, a, b).
+__device__ inline double de_uniform(unsigned long long key,
+                                    unsigned long long a,
+                                    unsigned long long b) {
+  const unsigned long long h = splitmix64(key ^ splitmix64(a ^ splitmix64(b)));
+  return double(h >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// pop, trial [S][N][P] in [0, 1]; mid, span [S][P]; base [S][6] (the fixed
+// sphere parameters); slots [P] (which of the six each variable is);
+// spheres [S * N] out.  With copy_only, or for a finished search, the trial
+// is the population itself.
+__global__ void k_de_trial(int S, int N, int P, const double* __restrict__ pop,
+                           double* __restrict__ trial,
+                           const unsigned long long* __restrict__ keys,
+                           int generation, double mut_lo, double mut_hi,
+                           const double* __restrict__ cr,
+                           const double* __restrict__ mid,
+                           const double* __restrict__ span,
+                           const double* __restrict__ base,
+                           const int* __restrict__ slots,
+                           const int* __restrict__ done, int copy_only,
+                           lmb_sphere* __restrict__ spheres) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)S * N) return;
+  const int s = int(i / N), c = int(i - (long long)s * N);
+  const double* ps = pop + (size_t)s * N * P;
+  const unsigned long long key = keys[s];
+  const unsigned long long gen = (unsigned long long)generation;
+  const unsigned long long ctr = (unsigned long long)c << 6;
+  const bool keep = copy_only || done[s];
+  double p[6];
+  for (int j = 0; j < 6; ++j) p[j] = base[(size_t)s * 6 + j];
+  // best1: pop[0] + F (pop[r0] - pop[r1]), r0 != r1 != c
+  const double scale =
+      mut_lo + (mut_hi - mut_lo) * de_uniform(key, gen, 0xFFFFFFFFull);
+  int r0 = min(int(de_uniform(key, gen, ctr + 1) * (N - 1)), N - 2);
+  if (r0 >= c) ++r0;
+  int r1 = min(int(de_uniform(key, gen, ctr + 2) * (N - 2)), N - 3);
+  const int lo = min(c, r0), hi = max(c, r0);
+  if (r1 >= lo) ++r1;
+  if (r1 >= hi) ++r1;
+  const int fill = min(int(de_uniform(key, gen, ctr + 3) * P), P - 1);
+  for (int j = 0; j < P; ++j) {
+    double v = ps[(size_t)c * P + j];
+    if (!keep) {
+      const double b = ps[j] + scale * (ps[(size_t)r0 * P + j] - ps[(size_t)r1 * P + j]);
+      if (j == fill || de_uniform(key, gen, ctr + 8 + j) < cr[s]) v = b;
+      if (v < 0. || v > 1.) v = de_uniform(key, gen, ctr + 32 + j);
+    }
+    trial[i * P + j] = v;
+    p[slots[j]] = mid[(size_t)s * P + j] + (v - 0.5) * span[(size_t)s * P + j];
+  }
+  lmb_sphere o;
+  o.x_p = p[0];
+  o.y_p = p[1];
+  o.z_p = p[2];
+  o.a_p = p[3];
+  o.n_p = p[4];
+  o.k_p = p[5];
+  spheres[i] = o;
+}
+
+// One warp per search: deferred selection (the trial replaces a candidate
+// whose energy it does not exceed), the best candidate moved to index 0,
+// and scipy's convergence test std(E) <= atol + tol |mean(E)| (no infinite
+// energy).  first: the initial population's energies (no selection).
+// done: 1 converged, 2 maxiter reached.
+__global__ void k_de_select(int S, int N, int P, double* __restrict__ pop,
+                            double* __restrict__ energies,
+                            const double* __restrict__ trial,
+                            const double* __restrict__ etrial,
+                            const double* __restrict__ tol,
+                            const double* __restrict__ atol,
+                            const int* __restrict__ maxiter,
+                            int* __restrict__ nit, int* __restrict__ done,
+                            int first) {
+  const int lane = threadIdx.x & 31;
+  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (s >= S || done[s]) return;
+  double* e = energies + (size_t)s * N;
+  double* ps = pop + (size_t)s * N * P;
+  const double* et = etrial + (size_t)s * N;
+  const double* ts = trial + (size_t)s * N * P;
+  for (int c = lane; c < N; c += 32) {
+    if (first || et[c] <= e[c]) {
+      e[c] = et[c];
+      if (!first)
+        for (int j = 0; j < P; ++j) ps[(size_t)c * P + j] = ts[(size_t)c * P + j];
+    }
+  }
+  __syncwarp();
+  // the best (the first of equal ones) to index 0; bi == N: none yet
+  double bv = 0.;
+  int bi = N;
+  for (int c = lane; c < N; c += 32)
+    if (bi == N || e[c] < bv) {
+      bv = e[c];
+      bi = c;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (oi != N && (bi == N || ov < bv || (ov == bv && oi < bi))) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  __syncwarp();
+  if (lane == 0 && bi > 0 && bi < N) {
+    const double t = e[0];
+    e[0] = e[bi];
+    e[bi] = t;
+    for (int j = 0; j < P; ++j) {
+      const double u = ps[j];
+      ps[j] = ps[(size_t)bi * P + j];
+      ps[(size_t)bi * P + j] = u;
+    }
+  }
+  __syncwarp();
+  if (first) return;
+  // convergence
+  double sum = 0.;
+  int inf = 0;
+  for (int c = lane; c < N; c += 32) {
+    sum += e[c];
+    inf |= isinf(e[c]) ? 1 : 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    inf |= __shfl_xor_sync(0xffffffffu, inf, o);
+  }
+  const double mean = sum / N;
+  double var = 0.;
+  for (int c = lane; c < N; c += 32) var += (e[c] - mean) * (e[c] - mean);
+  for (int o = 16; o > 0; o >>= 1) var += __shfl_xor_sync(0xffffffffu, var, o);
+  if (lane == 0) {
+    const int it = nit[s] + 1;
+    nit[s] = it;
+    const bool conv = !inf && sqrt(var / N) <= atol[s] + tol[s] * fabs(mean);
+    if (conv)
+      done[s] = 1;
+    else if (it >= maxiter[s])
+      done[s] = 2;
+  }
+}
+
 }  // namespace lmb

@@ -356,3 +356,57 @@ def test_frame_detect_estimate_optimize():
     assert len(res) == 3 and len(f.features) == 3
     with pytest.raises(RuntimeError):
         Frame(data).detect()       # no localizer
+
+
+def test_device_search():
+    '''The whole differential-evolution search on the GPU
+    (device_search=True: lmb_de_trial / lmb_de_select around the FP64
+    population chi^2, every feature's search in one generation loop):
+    reproducible for given seeds, and as good a search as scipy's.  Both
+    are stochastic and both can settle in a local basin, so they are
+    compared over several seeds: the runs whose estimate fits the full
+    crop within 2 % of the best chi^2 any run reached, per method.'''
+    from pylorenzmie_b200 import Frame, Instrument
+    data, truth, bboxes = _frame_data(seed=9)
+    inst = Instrument(wavelength=0.447, magnification=0.048, n_m=1.340)
+    bounds = {'z_p': (50., 400.), 'a_p': (0.3, 2.0), 'n_p': (1.35, 1.8)}
+    settings = {'tol': 1e-3, 'polish': False, 'updating': 'deferred',
+                'workers': 1}
+
+    def estimates(device, seed):
+        f = Frame(instrument=inst)
+        f.data = data
+        f.bboxes = bboxes
+        for i, feat in enumerate(f.features):
+            feat.model.double_precision = True
+            feat.estimator.fraction = 0.1
+            feat.estimator.bounds = dict(bounds)
+            feat.estimator.seed = seed + 10 * i
+            feat.estimator.popsize = 15
+            feat.estimator.settings = dict(settings)
+            feat.estimator.device_search = device
+        np.random.seed(seed)
+        f.estimate()
+        chi2 = []
+        for feat in f.features:
+            p = feat.particle
+            h = ofield.hologram(feat.coordinates.reshape(2, -1),
+                                [dict(zip(KEYS, [p.x_p, p.y_p, p.z_p, p.a_p,
+                                                 p.n_p, p.k_p]))],
+                                ofield.DEFAULT_INSTRUMENT)
+            chi2.append(float(np.sum(((h - feat.data.ravel()) / 0.05) ** 2)))
+        return np.array([[ft.particle.z_p, ft.particle.a_p, ft.particle.n_p]
+                         for ft in f.features]), np.array(chi2)
+    est1, _ = estimates(True, 30)
+    est2, _ = estimates(True, 30)
+    np.testing.assert_array_equal(est1, est2)
+    lo = [b[0] for b in bounds.values()]
+    hi = [b[1] for b in bounds.values()]
+    assert np.all((est1 >= lo) & (est1 <= hi))
+    seeds = (30, 31, 32, 33)
+    dev = np.array([estimates(True, sd)[1] for sd in seeds])
+    sp = np.array([estimates(False, sd)[1] for sd in seeds])
+    best = np.minimum(dev.min(axis=0), sp.min(axis=0))
+    good_dev = int((dev <= 1.02 * best).sum())
+    good_sp = int((sp <= 1.02 * best).sum())
+    assert good_dev >= good_sp - 2 and good_dev >= 6, (dev, sp)
