@@ -146,15 +146,31 @@ def device_searches(searches):
             ptr(d_slots), ptr(d_done), int(copy_only), ptr(d_spheres),
             stream), 'lmb_de_trial')
 
+    # the evaluation's buffers, made once: a generation allocates nothing
+    M = S * N
+    d_ab = torch.empty((M, cap + 1, 2, 2), dtype=torch.float64, device=dev)
+    d_nmax = torch.empty(M, dtype=torch.int32, device=dev)
+    d_status = torch.empty(M, dtype=torch.int32, device=dev)
+    d_chi2 = torch.empty(M, dtype=torch.float64, device=dev)
+    d_bad = torch.empty(M, dtype=torch.int32, device=dev)
+    ws_bytes = lib.lmb_chi2_workspace_bytes(int(pop_model.max_npts), M)
+    d_ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    coords, data = pop_model.coords.contiguous(), pop_model.data.contiguous()
+    flags = K._flags(True, True, True)
+
     def energies():
-        ab, _, nmax = K.sphere_ab(d_spheres, pop_model.n_m,
-                                  pop_model.wavelength, cap, check=False)
-        chi2, _ = K.chi2_crops(pop_model.coords, pop_model.data,
-                               pop_model.noise, pop_model.crop_start,
-                               item_crop, pop_model.max_npts, d_spheres,
-                               item_start, ab, nmax, cap, pop_model.k,
-                               fp64=True, aberration=pop_model.aberr)
-        return chi2
+        _native.check(lib.lmb_sphere_ab(
+            ptr(d_spheres), M, float(pop_model.n_m),
+            float(pop_model.wavelength), cap, ptr(d_ab), None, ptr(d_nmax),
+            ptr(d_status), stream), 'lmb_sphere_ab')
+        _native.check(lib.lmb_chi2_crops(
+            ptr(coords), coords.shape[1], ptr(data), float(pop_model.noise),
+            ptr(pop_model.crop_start), S, ptr(item_crop),
+            int(pop_model.max_npts), ptr(d_spheres), ptr(item_start), M,
+            ptr(d_ab), ptr(d_nmax), cap, float(pop_model.k), flags,
+            ptr(d_chi2), ptr(d_bad), ptr(d_ws), ws_bytes, stream,
+            float(pop_model.aberr)), 'lmb_chi2_crops')
+        return d_chi2
 
     def select(e, first_call):
         _native.check(lib.lmb_de_select(
