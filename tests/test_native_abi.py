@@ -84,6 +84,52 @@ def test_argument_checks_without_gpu(lib):
                              None) == _native.LMB_ERR_ARG
 
 
+def test_argument_checks_of_the_search_and_variant_entry_points(lib):
+    '''The device differential evolution, the crops chi^2 and the
+    aberrated entry points reject bad sizes and coefficients before any
+    device work (no GPU needed for these answers).'''
+    nan = float('nan')
+    ARG, OK = _native.LMB_ERR_ARG, _native.LMB_OK
+    # lmb_de_trial: nsearch, npop >= 3, nparam 1..6, mutation in [0, 2)
+    assert lib.lmb_de_trial(0, 10, 3, None, None, None, 0, 0.5, 1., None,
+                            None, None, None, None, None, 0, None,
+                            None) == OK
+    for ns, npop, npar in ((-1, 10, 3), (2, 2, 3), (2, 10, 0), (2, 10, 7)):
+        assert lib.lmb_de_trial(ns, npop, npar, None, None, None, 0, 0.5,
+                                1., None, None, None, None, None, None, 0,
+                                None, None) == ARG
+    assert lib.lmb_de_trial(2, 10, 3, None, None, None, 0, 0.5, 1., None,
+                            None, None, None, None, None, 0, None,
+                            None) == ARG          # null buffers
+    assert lib.lmb_de_select(0, 10, 3, None, None, None, None, None, None,
+                             None, None, None, 0, None) == OK
+    assert lib.lmb_de_select(2, 2, 3, None, None, None, None, None, None,
+                             None, None, None, 0, None) == ARG
+    assert lib.lmb_de_select(2, 10, 3, None, None, None, None, None, None,
+                             None, None, None, 0, None) == ARG
+    # lmb_chi2_crops: no items is a no-op; items without crops are not
+    assert lib.lmb_chi2_crops(None, 0, None, 0.05, None, 0, None, 0, None,
+                              None, 0, None, None, 10, 1., 3, None, None,
+                              None, 0, None, 0.) == OK
+    assert lib.lmb_chi2_crops(None, 10, None, 0.05, None, 0, None, 5, None,
+                              None, 2, None, None, 10, 1., 3, None, None,
+                              None, 0, None, 0.) == ARG
+    # non-finite aberration coefficients
+    assert lib.lmb_jacobian_aberrated(None, 0, None, 0, None, None, None, 10,
+                                      1., 3, nan, None, None, None) == ARG
+    assert lib.lmb_jacobian_aberrated(None, 0, None, 0, None, None, None, 10,
+                                      1., 3, 2.5, None, None, None) == OK
+    st = _native.FitSettings()
+    assert lib.lmb_fit_batch_aberrated(None, 0, 0, None, None, None, 1, None,
+                                       None, 1.34, 0.447, 0.048, 0.05, 10,
+                                       2.5, st, None, None, 0, None,
+                                       None) == OK
+    assert lib.lmb_fit_batch_aberrated(None, 2, 10, None, None, None, 1,
+                                       None, None, 1.34, 0.447, 0.048, 0.05,
+                                       10, 2.5, st, None, None, 0, None,
+                                       None) == ARG
+
+
 def test_workspace_sizes(lib):
     a = lib.lmb_fit_workspace_bytes(256, 256 * 201 * 201, 40)
     b = lib.lmb_fit_workspace_bytes(512, 512 * 201 * 201, 40)
