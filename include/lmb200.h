@@ -203,35 +203,41 @@ int lmb_chi2_crops(const double *coords, long long npts, const double *data,
  * are a counter-based hash (SplitMix64) of (keys[s], generation,
  * candidate, draw): reproducible for given keys, not scipy's stream.
  *
- * lmb_de_trial: for nsearch searches of npop candidates (>= 3) of nparam
- * (1..6) parameters, from pop [nsearch][npop][nparam] (unit cube) write the
- * trial population trial [same shape] and its sphere records spheres
- * [nsearch * npop]: parameter j is mid[s][j] + (v - 0.5) span[s][j] in
+ * Both step the searches live[0..nlive) of the nsearch (indices in
+ * [0, nsearch); others are skipped), so that finished searches cost
+ * nothing: their candidates are laid out by position k in live.
+ *
+ * lmb_de_trial: for searches of npop candidates (>= 3) of nparam (1..6)
+ * parameters, from pop [nsearch][npop][nparam] (unit cube) write the trial
+ * population trial [same shape] and the sphere records of the live
+ * searches spheres [nlive * npop] (search live[k] at k * npop): parameter
+ * j is mid[s][j] + (v - 0.5) span[s][j] in
  * slot slots[j] of the six, the rest from base [nsearch][6].  Mutation F
  * uniform in [mutation_lo, mutation_hi] per search and generation (equal
  * bounds: constant), recombination [nsearch].  With copy_only, or for a
  * search with done[s] != 0, the trial is the population itself (for the
  * first evaluation).
  *
- * lmb_de_select: with the trial energies [nsearch * npop], keep each
+ * lmb_de_select: with the trial energies [nlive * npop], keep each
  * trial whose energy does not exceed its candidate's (first: take all, the
  * initial population's energies), move each search's best to index 0, and
  * count the generation in nit [nsearch]; done[s] becomes 1 when
  * std(E) <= atol[s] + tol[s] |mean(E)| with no infinite energy, 2 when
  * nit reaches maxiter[s].  Finished searches are left as they are.
  */
-int lmb_de_trial(int nsearch, int npop, int nparam, const double *pop,
-                 double *trial, const unsigned long long *keys, int generation,
+int lmb_de_trial(int nsearch, int nlive, const int *live, int npop,
+                 int nparam, const double *pop, double *trial,
+                 const unsigned long long *keys, int generation,
                  double mutation_lo, double mutation_hi,
                  const double *recombination, const double *mid,
                  const double *span, const double *base, const int *slots,
                  const int *done, int copy_only, lmb_sphere *spheres,
                  void *stream);
-int lmb_de_select(int nsearch, int npop, int nparam, double *pop,
-                  double *energies, const double *trial,
-                  const double *trial_energies, const double *tol,
-                  const double *atol, const int *maxiter, int *nit, int *done,
-                  int first, void *stream);
+int lmb_de_select(int nsearch, int nlive, const int *live, int npop,
+                  int nparam, double *pop, double *energies,
+                  const double *trial, const double *trial_energies,
+                  const double *tol, const double *atol, const int *maxiter,
+                  int *nit, int *done, int first, void *stream);
 
 /*
  * Hologram and its Jacobian for nitems single-sphere items, FP32 sums,

@@ -84,10 +84,10 @@ _SIGNATURES = {
                                     _d, _i, _d, _vp, _vp]),
     'lmb_jacobian': (_i, [_vp, _ll, _vp, _i, _vp, _vp, _vp, _i, _d, _i, _vp,
                           _vp, _vp]),
-    'lmb_de_trial': (_i, [_i, _i, _i, _vp, _vp, _vp, _i, _d, _d, _vp, _vp,
-                          _vp, _vp, _vp, _vp, _i, _vp, _vp]),
-    'lmb_de_select': (_i, [_i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                           _vp, _vp, _i, _vp]),
+    'lmb_de_trial': (_i, [_i, _i, _vp, _i, _i, _vp, _vp, _vp, _i, _d, _d,
+                          _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
+    'lmb_de_select': (_i, [_i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp,
+                           _vp, _vp, _vp, _i, _vp]),
     'lmb_jacobian_aberrated': (_i, [_vp, _ll, _vp, _i, _vp, _vp, _vp, _i, _d,
                                     _i, _d, _vp, _vp, _vp]),
     'lmb_vjp_workspace_bytes': (_sz, [_ll, _i]),

@@ -5,12 +5,12 @@ analysis/RadialEstimator.py:150-158) run scipy's differential_evolution
 on the host; run_populations (``_de``) keeps scipy's exact algorithm and
 random stream, so each generation still costs per-candidate host work.
 ``device_searches`` moves the search itself to the device: every
-generation of every feature's search is three launches -- the trial
+generation of every running search is three launches -- the trial
 populations and their sphere records (lmb_de_trial), the Mie coefficients
 and FP64 chi^2 of every trial against its own crop (lmb_sphere_ab,
 lmb_chi2_crops), the selection and convergence test (lmb_de_select) --
 with no host work between generations; the host reads the finished flags
-every few generations.
+every few generations and drops the finished searches from the launches.
 
 The algorithm is scipy's best1bin with deferred updating, latin-hypercube
 start, dithered mutation, binomial crossover and scipy's convergence test,
@@ -127,8 +127,16 @@ def device_searches(searches):
     d_done = torch.zeros(S, dtype=torch.int32, device=dev)
     d_spheres = torch.empty((S * N, 6), dtype=torch.float64, device=dev)
     item_start = torch.arange(S * N + 1, dtype=torch.int32, device=dev)
-    item_crop = torch.arange(S, dtype=torch.int32,
-                             device=dev).repeat_interleave(N)
+    # the searches still running, by position: their candidates are
+    # evaluated (sphere records and energies laid out by position)
+    state = {}
+
+    def set_live(live):
+        state['L'] = len(live)
+        state['live'] = torch.as_tensor(np.asarray(live, dtype=np.int32),
+                                        device=dev)
+        state['crop'] = state['live'].repeat_interleave(N)
+    set_live(np.arange(S))
     # capacity: the largest sphere the bounds allow
     hi = np.array([b[1] for b in bounds])
     lo = np.array([b[0] for b in bounds])
@@ -141,10 +149,10 @@ def device_searches(searches):
 
     def trial(generation, copy_only):
         _native.check(lib.lmb_de_trial(
-            S, N, P, ptr(d_pop), ptr(d_trial), ptr(d_keys), generation, mlo,
-            mhi, ptr(d_cr), ptr(d_mid), ptr(d_span), ptr(d_base),
-            ptr(d_slots), ptr(d_done), int(copy_only), ptr(d_spheres),
-            stream), 'lmb_de_trial')
+            S, state['L'], ptr(state['live']), N, P, ptr(d_pop), ptr(d_trial),
+            ptr(d_keys), generation, mlo, mhi, ptr(d_cr), ptr(d_mid),
+            ptr(d_span), ptr(d_base), ptr(d_slots), ptr(d_done),
+            int(copy_only), ptr(d_spheres), stream), 'lmb_de_trial')
 
     # the evaluation's buffers, made once: a generation allocates nothing
     M = S * N
@@ -159,14 +167,15 @@ def device_searches(searches):
     flags = K._flags(True, True, True)
 
     def energies():
+        m = state['L'] * N
         _native.check(lib.lmb_sphere_ab(
-            ptr(d_spheres), M, float(pop_model.n_m),
+            ptr(d_spheres), m, float(pop_model.n_m),
             float(pop_model.wavelength), cap, ptr(d_ab), None, ptr(d_nmax),
             ptr(d_status), stream), 'lmb_sphere_ab')
         _native.check(lib.lmb_chi2_crops(
             ptr(coords), coords.shape[1], ptr(data), float(pop_model.noise),
-            ptr(pop_model.crop_start), S, ptr(item_crop),
-            int(pop_model.max_npts), ptr(d_spheres), ptr(item_start), M,
+            ptr(pop_model.crop_start), S, ptr(state['crop']),
+            int(pop_model.max_npts), ptr(d_spheres), ptr(item_start), m,
             ptr(d_ab), ptr(d_nmax), cap, float(pop_model.k), flags,
             ptr(d_chi2), ptr(d_bad), ptr(d_ws), ws_bytes, stream,
             float(pop_model.aberr)), 'lmb_chi2_crops')
@@ -174,9 +183,10 @@ def device_searches(searches):
 
     def select(e, first_call):
         _native.check(lib.lmb_de_select(
-            S, N, P, ptr(d_pop), ptr(d_energy), ptr(d_trial), ptr(e),
-            ptr(d_tol), ptr(d_atol), ptr(d_maxiter), ptr(d_nit), ptr(d_done),
-            int(first_call), stream), 'lmb_de_select')
+            S, state['L'], ptr(state['live']), N, P, ptr(d_pop),
+            ptr(d_energy), ptr(d_trial), ptr(e), ptr(d_tol), ptr(d_atol),
+            ptr(d_maxiter), ptr(d_nit), ptr(d_done), int(first_call),
+            stream), 'lmb_de_select')
 
     trial(0, True)
     select(energies(), True)
@@ -185,8 +195,11 @@ def device_searches(searches):
         trial(generation, False)
         select(energies(), False)
         if generation % _CHECK_EVERY == 0 or generation == limit:
-            if bool((d_done != 0).all()):
+            live = np.flatnonzero(d_done.cpu().numpy() == 0)
+            if not len(live):
                 break
+            if len(live) < state['L']:
+                set_live(live)
     pop = d_pop.cpu().numpy()
     energy = d_energy.cpu().numpy()
     nit = d_nit.cpu().numpy()

@@ -437,44 +437,51 @@ int jacobian_launch(const double* coords, long long npts,
 
 extern "C" {
 
-int lmb_de_trial(int nsearch, int npop, int nparam, const double* pop,
-                 double* trial, const unsigned long long* keys, int generation,
+int lmb_de_trial(int nsearch, int nlive, const int* live, int npop,
+                 int nparam, const double* pop, double* trial,
+                 const unsigned long long* keys, int generation,
                  double mutation_lo, double mutation_hi,
                  const double* recombination, const double* mid,
                  const double* span, const double* base, const int* slots,
                  const int* done, int copy_only, lmb_sphere* spheres,
                  void* stream) {
-  if (nsearch < 0 || npop < 3 || nparam < 1 || nparam > 6) return LMB_ERR_ARG;
-  if (nsearch == 0) return LMB_OK;
-  if (!pop || !trial || !keys || !recombination || !mid || !span || !base ||
-      !slots || !done || !spheres)
+  if (nsearch < 0 || nlive < 0 || nlive > nsearch || npop < 3 || nparam < 1 ||
+      nparam > 6)
+    return LMB_ERR_ARG;
+  if (nlive == 0) return LMB_OK;
+  if (!live || !pop || !trial || !keys || !recombination || !mid || !span ||
+      !base || !slots || !done || !spheres)
     return LMB_ERR_ARG;
   if (!(mutation_lo >= 0.) || !(mutation_hi >= mutation_lo) || !(mutation_hi < 2.) ||
       generation < 0)
     return LMB_ERR_ARG;
-  const long long n = (long long)nsearch * npop;
+  const long long n = (long long)nlive * npop;
   const int tpb = 128;
   k_de_trial<<<unsigned((n + tpb - 1) / tpb), tpb, 0, as_stream(stream)>>>(
-      nsearch, npop, nparam, pop, trial, keys, generation, mutation_lo,
+      nsearch, nlive, live, npop, nparam, pop, trial, keys, generation,
+      mutation_lo,
       mutation_hi, recombination, mid, span, base, slots, done, copy_only,
       spheres);
   LMB_CK(cudaGetLastError());
   return LMB_OK;
 }
 
-int lmb_de_select(int nsearch, int npop, int nparam, double* pop,
-                  double* energies, const double* trial,
-                  const double* trial_energies, const double* tol,
-                  const double* atol, const int* maxiter, int* nit, int* done,
-                  int first, void* stream) {
-  if (nsearch < 0 || npop < 3 || nparam < 1 || nparam > 6) return LMB_ERR_ARG;
-  if (nsearch == 0) return LMB_OK;
-  if (!pop || !energies || !trial || !trial_energies || !tol || !atol ||
-      !maxiter || !nit || !done)
+int lmb_de_select(int nsearch, int nlive, const int* live, int npop,
+                  int nparam, double* pop, double* energies,
+                  const double* trial, const double* trial_energies,
+                  const double* tol, const double* atol, const int* maxiter,
+                  int* nit, int* done, int first, void* stream) {
+  if (nsearch < 0 || nlive < 0 || nlive > nsearch || npop < 3 || nparam < 1 ||
+      nparam > 6)
+    return LMB_ERR_ARG;
+  if (nlive == 0) return LMB_OK;
+  if (!live || !pop || !energies || !trial || !trial_energies || !tol ||
+      !atol || !maxiter || !nit || !done)
     return LMB_ERR_ARG;
   const int wpb = 4;  // warps (searches) per block
-  k_de_select<<<unsigned((nsearch + wpb - 1) / wpb), 32 * wpb, 0,
-                as_stream(stream)>>>(nsearch, npop, nparam, pop, energies,
+  k_de_select<<<unsigned((nlive + wpb - 1) / wpb), 32 * wpb, 0,
+                as_stream(stream)>>>(nsearch, nlive, live, npop, nparam, pop,
+                                     energies,
                                      trial, trial_energies, tol, atol, maxiter,
                                      nit, done, first);
   LMB_CK(cudaGetLastError());

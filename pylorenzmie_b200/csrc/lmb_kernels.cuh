@@ -1468,10 +1468,12 @@ __device__ inline double de_uniform(unsigned long long key,
 }
 
 // pop, trial [S][N][P] in [0, 1]; mid, span [S][P]; base [S][6] (the fixed
-// sphere parameters); slots [P] (which of the six each variable is);
-// spheres [S * N] out.  With copy_only, or for a finished search, the trial
-// is the population itself.
-__global__ void k_de_trial(int S, int N, int P, const double* __restrict__ pop,
+// sphere parameters); slots [P] (which of the six each variable is).  The
+// searches stepped are live[0..L) (indices into the S); spheres [L * N]
+// out, search live[k]'s candidates at k * N.  With copy_only, or for a
+// finished search, the trial is the population itself.
+__global__ void k_de_trial(int S, int L, const int* __restrict__ live, int N,
+                           int P, const double* __restrict__ pop,
                            double* __restrict__ trial,
                            const unsigned long long* __restrict__ keys,
                            int generation, double mut_lo, double mut_hi,
@@ -1483,9 +1485,12 @@ __global__ void k_de_trial(int S, int N, int P, const double* __restrict__ pop,
                            const int* __restrict__ done, int copy_only,
                            lmb_sphere* __restrict__ spheres) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)S * N) return;
-  const int s = int(i / N), c = int(i - (long long)s * N);
+  if (i >= (long long)L * N) return;
+  const int k = int(i / N), c = int(i - (long long)k * N);
+  const int s = live[k];
+  if (s < 0 || s >= S) return;  // not a search of this call
   const double* ps = pop + (size_t)s * N * P;
+  const size_t row = (size_t)s * N + c;  // the candidate in pop / trial
   const unsigned long long key = keys[s];
   const unsigned long long gen = (unsigned long long)generation;
   const unsigned long long ctr = (unsigned long long)c << 6;
@@ -1509,7 +1514,7 @@ __global__ void k_de_trial(int S, int N, int P, const double* __restrict__ pop,
       if (j == fill || de_uniform(key, gen, ctr + 8 + j) < cr[s]) v = b;
       if (v < 0. || v > 1.) v = de_uniform(key, gen, ctr + 32 + j);
     }
-    trial[i * P + j] = v;
+    trial[row * P + j] = v;
     p[slots[j]] = mid[(size_t)s * P + j] + (v - 0.5) * span[(size_t)s * P + j];
   }
   lmb_sphere o;
@@ -1522,12 +1527,14 @@ __global__ void k_de_trial(int S, int N, int P, const double* __restrict__ pop,
   spheres[i] = o;
 }
 
-// One warp per search: deferred selection (the trial replaces a candidate
-// whose energy it does not exceed), the best candidate moved to index 0,
-// and scipy's convergence test std(E) <= atol + tol |mean(E)| (no infinite
-// energy).  first: the initial population's energies (no selection).
-// done: 1 converged, 2 maxiter reached.
-__global__ void k_de_select(int S, int N, int P, double* __restrict__ pop,
+// One warp per live search (live[0..L)): deferred selection (the trial
+// replaces a candidate whose energy it does not exceed), the best candidate
+// moved to index 0, and scipy's convergence test std(E) <= atol +
+// tol |mean(E)| (no infinite energy).  etrial [L * N] in the order of
+// k_de_trial's spheres.  first: the initial population's energies (no
+// selection).  done: 1 converged, 2 maxiter reached.
+__global__ void k_de_select(int S, int L, const int* __restrict__ live, int N,
+                            int P, double* __restrict__ pop,
                             double* __restrict__ energies,
                             const double* __restrict__ trial,
                             const double* __restrict__ etrial,
@@ -1537,11 +1544,13 @@ __global__ void k_de_select(int S, int N, int P, double* __restrict__ pop,
                             int* __restrict__ nit, int* __restrict__ done,
                             int first) {
   const int lane = threadIdx.x & 31;
-  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (s >= S || done[s]) return;
+  const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (k >= L) return;
+  const int s = live[k];
+  if (s < 0 || s >= S || done[s]) return;
   double* e = energies + (size_t)s * N;
   double* ps = pop + (size_t)s * N * P;
-  const double* et = etrial + (size_t)s * N;
+  const double* et = etrial + (size_t)k * N;
   const double* ts = trial + (size_t)s * N * P;
   for (int c = lane; c < N; c += 32) {
     if (first || et[c] <= e[c]) {

@@ -91,22 +91,18 @@ def test_argument_checks_of_the_search_and_variant_entry_points(lib):
     nan = float('nan')
     ARG, OK = _native.LMB_ERR_ARG, _native.LMB_OK
     # lmb_de_trial: nsearch, npop >= 3, nparam 1..6, mutation in [0, 2)
-    assert lib.lmb_de_trial(0, 10, 3, None, None, None, 0, 0.5, 1., None,
-                            None, None, None, None, None, 0, None,
-                            None) == OK
-    for ns, npop, npar in ((-1, 10, 3), (2, 2, 3), (2, 10, 0), (2, 10, 7)):
-        assert lib.lmb_de_trial(ns, npop, npar, None, None, None, 0, 0.5,
-                                1., None, None, None, None, None, None, 0,
-                                None, None) == ARG
-    assert lib.lmb_de_trial(2, 10, 3, None, None, None, 0, 0.5, 1., None,
-                            None, None, None, None, None, 0, None,
-                            None) == ARG          # null buffers
-    assert lib.lmb_de_select(0, 10, 3, None, None, None, None, None, None,
-                             None, None, None, 0, None) == OK
-    assert lib.lmb_de_select(2, 2, 3, None, None, None, None, None, None,
-                             None, None, None, 0, None) == ARG
-    assert lib.lmb_de_select(2, 10, 3, None, None, None, None, None, None,
-                             None, None, None, 0, None) == ARG
+    def trial(ns, nl, npop, npar):
+        return lib.lmb_de_trial(ns, nl, None, npop, npar, None, None, None, 0,
+                                0.5, 1., None, None, None, None, None, None,
+                                0, None, None)
+
+    def select(ns, nl, npop, npar):
+        return lib.lmb_de_select(ns, nl, None, npop, npar, None, None, None,
+                                 None, None, None, None, None, None, 0, None)
+    assert trial(4, 0, 10, 3) == OK and select(4, 0, 10, 3) == OK
+    for args in ((-1, 0, 10, 3), (2, 3, 10, 3), (2, 2, 2, 3), (2, 2, 10, 0),
+                 (2, 2, 10, 7), (2, 2, 10, 3)):    # the last: null buffers
+        assert trial(*args) == ARG and select(*args) == ARG, args
     # lmb_chi2_crops: no items is a no-op; items without crops are not
     assert lib.lmb_chi2_crops(None, 0, None, 0.05, None, 0, None, 0, None,
                               None, 0, None, None, 10, 1., 3, None, None,
