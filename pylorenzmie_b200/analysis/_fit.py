@@ -581,6 +581,60 @@ def _stream_fit_stream(dev, slot):
     return _stream_fit_streams[key]
 
 
+class _Slots:
+    '''The scheduling of fit_stream: at most ``depth`` jobs run at once,
+    each on a slot of its own (a stream); a slot frees when any job ends;
+    results leave in submission order, with at most ``backlog`` finished
+    ones held back.  ``wait_slot()`` blocks until a slot is free;
+    ``submit(fn, extra, *args)`` takes it and calls fn(slot, *args) ->
+    future; ``ready()`` yields the results whose turn has come (and the
+    oldest ones past the backlog bound, waiting for them); ``drain()``
+    yields the rest.  ``add_done(extra)`` queues a result that needs no job
+    (an empty batch); it passes through as ``extra``.'''
+
+    def __init__(self, depth, backlog=None):
+        from collections import deque
+        self.depth = depth
+        self.backlog = 8 * depth if backlog is None else backlog
+        self.pending = deque()      # (future or None, extra)
+        self.running = {}           # future -> slot
+        self.free = list(range(depth))
+
+    def add_done(self, extra):
+        self.pending.append((None, extra))
+
+    def wait_slot(self):
+        from concurrent.futures import wait, FIRST_COMPLETED
+        while not self.free:
+            finished, _ = wait(list(self.running),
+                               return_when=FIRST_COMPLETED)
+            for f in finished:
+                self.free.append(self.running.pop(f))
+
+    def ready(self):
+        while self.pending and (self.pending[0][0] is None or
+                                self.pending[0][0].done()):
+            yield _collect(self.pending.popleft())
+        while len(self.pending) >= self.backlog:
+            yield _collect(self.pending.popleft())
+
+    def submit(self, fn, extra, *args):
+        slot = self.free.pop(0)
+        fut = fn(slot, *args)
+        self.running[fut] = slot
+        self.pending.append((fut, extra))
+        return slot
+
+    def drain(self):
+        while self.pending:
+            yield _collect(self.pending.popleft())
+
+    def wait_all(self):
+        for fut, _ in self.pending:
+            if fut is not None:
+                fut.result()
+
+
 def fit_stream(batches, instrument, variables, settings=None, device=None,
                autotune=False, depth=2, aberration=0.):
     '''Fit a sequence of batches, pipelined; yields, in order, (params
@@ -598,22 +652,24 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
     finished batches wait, up to 8 x depth of them, to be yielded in order.
     A pinned buffer is rewritten only after its previous copy has
     completed.'''
-    from collections import deque
-    from concurrent.futures import wait, FIRST_COMPLETED
     dev = get_device(device)
     _, s_copy = _fit_streams(dev)
     nstage = depth + 1
     while len(_stream_staging) < nstage:
         _stream_staging.append(_Staging())
-    pending = deque()          # (future or None, extra), submission order
-    running = {}               # future -> fit slot (its stream)
-    free = list(range(depth))
+    slots = _Slots(depth)
     done_events = [None] * nstage
     tile_config = None
     k = 0
 
-    def ready_head():
-        return pending and (pending[0][0] is None or pending[0][0].done())
+    def launch(fit_slot, ev, views, B, total, nmax_cap, starts, layers):
+        s_fit = _stream_fit_stream(dev, fit_slot)
+        for v in views:
+            if v is not None:
+                v.record_stream(s_fit)
+        return _stream_worker(depth).submit(
+            _fit_after, s_fit, ev, views, B, total, instrument, variables,
+            settings, nmax_cap, starts, tile_config, layers, aberration)
 
     try:
         for items, starts, layers in batches:
@@ -623,8 +679,8 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
             packed = PackedFeatures(items)
             npix = packed.features['npix'].astype(np.int64)
             if B == 0:
-                pending.append((None, (starts.copy(), np.zeros(
-                    0, dtype=_native.RESULT_DTYPE), npix)))
+                slots.add_done((starts.copy(), np.zeros(
+                    0, dtype=_native.RESULT_DTYPE), npix))
                 k += 1
                 continue
             nmax_cap = fit_capacity(starts, float(instrument.n_m),
@@ -646,32 +702,14 @@ def fit_stream(batches, instrument, variables, settings=None, device=None,
                 ev.record(s_copy)
             done_events[slot] = ev
             # this batch's data is on its way: now wait for a fit slot
-            while not free:
-                finished, _ = wait(list(running), return_when=FIRST_COMPLETED)
-                for f in finished:
-                    free.append(running.pop(f))
-            while ready_head():
-                yield _collect(pending.popleft())
-            while len(pending) >= 8 * depth:   # bound the finished backlog
-                yield _collect(pending.popleft())
-            fit_slot = free.pop(0)
-            s_fit = _stream_fit_stream(dev, fit_slot)
-            for v in views:
-                if v is not None:
-                    v.record_stream(s_fit)
-            fut = _stream_worker(depth).submit(
-                _fit_after, s_fit, ev, views, B, packed.total, instrument,
-                variables, settings, nmax_cap, starts, tile_config, layers,
-                aberration)
-            running[fut] = fit_slot
-            pending.append((fut, npix))
+            slots.wait_slot()
+            yield from slots.ready()
+            slots.submit(launch, npix, ev, views, B, packed.total, nmax_cap,
+                         starts, layers)
             k += 1
-        while pending:
-            yield _collect(pending.popleft())
+        yield from slots.drain()
     finally:
-        for fut, _ in pending:
-            if fut is not None:
-                fut.result()
+        slots.wait_all()
         s_copy.synchronize()
 
 
