@@ -14,8 +14,8 @@ pylorenzmie that the CUDA library replaces:
   call scipy's ``least_squares(method='lm')`` (MINPACK ``lmder``).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this package.  It is the checker, never the thing
-measured or shipped: the product (``pylorenzmie_b200``) never imports it.
+``bench.py`` may import this package.  It is test infrastructure that
+results are compared against, never the thing measured or shipped: the product (``pylorenzmie_b200``) never imports it.
 
 Pinning: ``tests/golden/make_golden.py`` imports the reference itself and
 writes the fixtures in ``tests/golden/``; ``tests/test_oracle_golden.py``
