@@ -559,19 +559,8 @@ def run_extras(dev, inst, chosen_value):
     # oracle's numpy search
     from pylorenzmie_b200 import Frame
     from oracle import estimate as oest, field as ofield
-    rng = np.random.default_rng(21)
     nest = 32
-    P = np.zeros((nest, 6))
-    P[:, 0] = 80. + 160. * (np.arange(nest) % 8) + rng.uniform(-3., 3., nest)
-    P[:, 1] = 80. + 160. * (np.arange(nest) // 8) + rng.uniform(-3., 3., nest)
-    P[:, 2] = rng.uniform(100., 300., nest)
-    P[:, 3] = rng.uniform(0.5, 1.5, nest)
-    P[:, 4] = rng.uniform(1.38, 1.60, nest)
-    fm = LorenzMie(coordinates=LorenzMie.meshgrid((640, 1280)),
-                   particle=workloads.spheres(P), instrument=inst, device=dev)
-    fdata = (fm.hologram() + rng.normal(0., inst.noise, 640 * 1280)
-             ).reshape(640, 1280)
-    boxes = [((int(x) - 60, int(y) - 60), 121, 121) for x, y in P[:, :2]]
+    P, fdata, boxes = workloads.estimate_frame(nest, 21, inst, dev)
 
     def _no_stop(xk, convergence):
         return False

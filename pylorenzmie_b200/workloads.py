@@ -20,6 +20,10 @@ of sigma = 0.05 (the instrument's noise).
   z_p ~ U(200, 600) px.
 * layered     -- three-layer core-shell spheres in crops of 101..201 px
   (the video-stream workload; see ``layered``).
+* estimate_frame -- a 1280x640 frame of 32 spheres on an 8x4 grid of
+  160 px pitch (+-3 px), z_p ~ U(100, 300) px, a_p ~ U(0.5, 1.5) um,
+  n_p ~ U(1.38, 1.60), with a 121x121 box around each (the global-estimate
+  workload of a frame's features).
 '''
 import numpy as np
 
@@ -74,6 +78,27 @@ def frame(seed=0, shape=(1024, 1280), magnification=0.048):
     p[:, 0] = rng.uniform(0., shape[1], n)
     p[:, 1] = rng.uniform(0., shape[0], n)
     return p
+
+
+def estimate_frame(n=32, seed=21, instrument=None, device=None):
+    '''(params (n, 6), frame (640, 1280) float64 numpy, boxes) of the
+    estimate workload: the FP32 hologram of the n spheres plus noise, and
+    one ((x0, y0), 121, 121) box per sphere.'''
+    from .theory import LorenzMie, Instrument
+    inst = instrument or Instrument()
+    rng = np.random.default_rng(seed)
+    p = np.zeros((n, 6))
+    p[:, 0] = 80. + 160. * (np.arange(n) % 8) + rng.uniform(-3., 3., n)
+    p[:, 1] = 80. + 160. * (np.arange(n) // 8) + rng.uniform(-3., 3., n)
+    p[:, 2] = rng.uniform(100., 300., n)
+    p[:, 3] = rng.uniform(0.5, 1.5, n)
+    p[:, 4] = rng.uniform(1.38, 1.60, n)
+    m = LorenzMie(coordinates=LorenzMie.meshgrid((640, 1280)),
+                  particle=spheres(p), instrument=inst, device=device)
+    data = (m.hologram() + rng.normal(0., inst.noise, 640 * 1280)
+            ).reshape(640, 1280)
+    boxes = [((int(x) - 60, int(y) - 60), 121, 121) for x, y in p[:, :2]]
+    return p, data, boxes
 
 
 def large(B, seed=0, side=401):
@@ -172,3 +197,38 @@ def render_particles(particles, shapes, seed=0, instrument=None, device=None,
                                     dtype=h.dtype)
         out.append(h.float().reshape(shape).cpu().numpy())
     return out
+
+
+def _run_estimate_frame(device_search, repeat):
+    '''Frame.estimate of the estimate workload, ``repeat`` times (the first
+    one warms up); prints the seconds each took.'''
+    import time
+    import torch
+    from .theory import Instrument
+    from .analysis import Frame
+    inst = Instrument()
+    _, data, boxes = estimate_frame(32, 21, inst)
+    for rep in range(repeat):
+        f = Frame(instrument=inst)
+        f.data = data
+        f.bboxes = boxes
+        for i, feat in enumerate(f.features):
+            feat.estimator.seed = 40 + i
+            feat.estimator.device_search = device_search
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f.estimate()
+        torch.cuda.synchronize()
+        print(f'estimate_frame {rep}: {time.perf_counter() - t0:.4f} s')
+
+
+if __name__ == '__main__':
+    # python -m pylorenzmie_b200.workloads estimate_frame [--device-search]
+    # runs one workload through the public API, e.g. under a profiler
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument('workload', choices=['estimate_frame'])
+    ap.add_argument('--device-search', action='store_true')
+    ap.add_argument('--repeat', type=int, default=2)
+    a = ap.parse_args()
+    _run_estimate_frame(a.device_search, a.repeat)
