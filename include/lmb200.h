@@ -449,6 +449,22 @@ int lmb_pack_crops(const void *const *sources, const long long *counts,
                    int nsources, int src_type, float *dst, int nthreads);
 
 /*
+ * Host-side draws of a differential-evolution generation: count times,
+ * shuffle index[0..n) in place exactly as numpy's Generator.shuffle and
+ * RandomState.shuffle do (Fisher-Yates, partners by numpy's masked
+ * rejection on the generator's 32-bit draws), and copy the first keep
+ * entries to out[c * keep ..].  bitgen is numpy's bitgen_t of the
+ * generator (BitGenerator.ctypes.bit_generator); the caller holds the bit
+ * generator's lock.  Replaces the per-candidate shuffle of scipy's
+ * DifferentialEvolutionSolver._select_samples, which the reference's
+ * estimators reach through differential_evolution
+ * (analysis/DEEstimator.py:158-166, analysis/RadialEstimator.py:150-158):
+ * the same draws in the same order, so a seeded search is unchanged.
+ */
+int lmb_de_shuffles(void *bitgen, long long *index, long long n,
+                    long long count, int keep, long long *out);
+
+/*
  * lmb_fit_batch (any layer count) that starts before all of its pixel data
  * is on the device.  No counterpart in the reference, whose fits run one
  * feature at a time on the host.

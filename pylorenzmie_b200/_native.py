@@ -120,6 +120,7 @@ _SIGNATURES = {
                            ctypes.POINTER(FitStats), _vp]),
     'lmb_measure_fp32_peak': (_i, [ctypes.POINTER(_d), _vp]),
     'lmb_pack_crops': (_i, [_vp, _vp, _i, _i, _vp, _i]),
+    'lmb_de_shuffles': (_i, [_vp, _vp, _ll, _ll, _i, _vp]),
 }
 
 _lock = threading.Lock()

@@ -140,18 +140,21 @@ def run_searches(searches, workers=256):
     return results
 
 
-def estimate_many(estimators, holograms):
+def estimate_many(estimators, holograms, series=True):
     '''estimator.estimate(hologram) for each pair, the searches side by
-    side (run_searches); returns the Series in order.  Estimators that
-    share a model run one after another, as the model carries each
-    search's start.'''
+    side (run_searches); returns the Series in order (with
+    ``series=False`` only the models are left at the estimates, and the
+    result is None).  Estimators that share a model run one after another,
+    as the model carries each search's start.'''
     estimators, holograms = list(estimators), list(holograms)
     if len({id(e.model) for e in estimators}) < len(estimators):
-        return [e.estimate(h) for e, h in zip(estimators, holograms)]
+        out = [e.estimate(h) for e, h in zip(estimators, holograms)]
+        return out if series else None
     searches = [e.search(h) for e, h in zip(estimators, holograms)]
     results = run_searches(searches)
-    return [e.accept(sr, r) for e, sr, r in zip(estimators, searches,
-                                                 results)]
+    out = [e.accept(sr, r, series=series)
+           for e, sr, r in zip(estimators, searches, results)]
+    return out if series else None
 
 
 @dataclass
@@ -198,11 +201,13 @@ class DEEstimator(BaseEstimator):
                     seed=self.seed, settings=self.settings,
                     device_search=self.device_search)
 
-    def accept(self, search, result):
+    def accept(self, search, result, series=True):
         '''Leave the model at the search's result; its properties as a
-        Series.'''
+        Series (None with ``series=False``, for callers that keep only the
+        model state).'''
         self.model.properties = dict(zip(search['variables'], result.x))
-        return pd.Series(self.model.particle.properties)
+        if series:
+            return pd.Series(self.model.particle.properties)
 
     def estimate(self, hologram):
         '''Estimate particle parameters; returns the particle's properties

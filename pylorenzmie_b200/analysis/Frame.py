@@ -151,7 +151,7 @@ class Frame(Hologram):
                 hasattr(f.estimator, 'accept')]
         rest = feats
         if len(side) > 1:
-            estimate_many([f.estimator for f in side], side)
+            estimate_many([f.estimator for f in side], side, series=False)
             rest = [f for f in feats if not any(f is g for g in side)]
         for f in rest:
             f.estimate()

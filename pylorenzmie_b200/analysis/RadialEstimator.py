@@ -61,11 +61,13 @@ class RadialEstimator(BaseEstimator):
                     seed=self.seed, settings=self.settings,
                     device_search=self.device_search)
 
-    def accept(self, search, result):
+    def accept(self, search, result, series=True):
         '''Leave the model at the search's result; its properties as a
-        Series.'''
+        Series (None with ``series=False``, for callers that keep only the
+        model state).'''
         self.model.properties = dict(zip(search['variables'], result.x))
-        return pd.Series(self.model.particle.properties)
+        if series:
+            return pd.Series(self.model.particle.properties)
 
     def estimate(self, hologram):
         search = self.search(hologram)

@@ -26,6 +26,8 @@ import numbers
 import numpy as np
 from scipy.optimize import OptimizeResult
 
+from .. import _native
+
 _SUCCESS = 'Optimization terminated successfully.'
 _MAXITER = 'Maximum number of iterations has been exceeded.'
 
@@ -81,6 +83,21 @@ def _integers(rng, high, size):
     if isinstance(rng, np.random.Generator):
         return rng.integers(high, size=size, dtype='int64')
     return rng.randint(high, size=size, dtype='int64')
+
+
+def _shuffles(rng, index, count, out):
+    '''``count`` times: rng.shuffle(index), then out[c] = index[:3] --
+    in one native call on the generator's own bit generator
+    (lmb_de_shuffles: numpy's shuffle restated, the same draws in the same
+    order).'''
+    bg = (rng.bit_generator if isinstance(rng, np.random.Generator)
+          else rng._bit_generator)
+    lib = _native.load()
+    with bg.lock:
+        st = lib.lmb_de_shuffles(bg.ctypes.bit_generator, index.ctypes.data,
+                                 len(index), count, out.shape[1],
+                                 out.ctypes.data)
+    _native.check(st, 'lmb_de_shuffles')
 
 
 class Populations:
@@ -145,7 +162,7 @@ class Populations:
         self.pop = np.array(pops)
         self.energies = np.full((S, self.N), np.inf)
         self.trial = np.zeros_like(self.pop)
-        self.index = [np.arange(self.N) for _ in range(S)]
+        self.index = [np.arange(self.N, dtype=np.int64) for _ in range(S)]
         self.trialed = np.zeros(S, dtype=bool)   # last request was a trial
         self.nfev = np.zeros(S, dtype=int)
         self.nit = np.zeros(S, dtype=int)
@@ -176,10 +193,7 @@ class Populations:
                                             self.dither[s][1])
             # mutation, best1: for each candidate the first two of a fresh
             # shuffle of the kept permutation other than the candidate
-            shuffle, index, fs = rng.shuffle, self.index[s], first[i]
-            for c in range(N):
-                shuffle(index)
-                fs[c] = index[:3]
+            _shuffles(rng, self.index[s], N, first[i])
             fill[i] = _integers(rng, P, N)
             cross[i] = rng.uniform(size=(N, P)) < self.cr[s]
         c = np.arange(N)

@@ -170,3 +170,65 @@ extern "C" int lmb_pack_crops(const void* const* sources,
   pool().run(job);
   return LMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Differential-evolution sample draws on numpy's own bit generator.
+//
+// numpy's bitgen_t (numpy/random/bitgen.h), as BitGenerator.ctypes
+// .bit_generator points to it: the generator's state and its draw
+// functions.
+namespace {
+
+struct NpBitgen {
+  void* state;
+  uint64_t (*next_uint64)(void*);
+  uint32_t (*next_uint32)(void*);
+  double (*next_double)(void*);
+  uint64_t (*next_raw)(void*);
+};
+
+// numpy's random_interval (random/src/distributions/distributions.c): an
+// integer uniform on [0, max] by rejection of the draws masked to the
+// smallest all-ones mask >= max; 32-bit draws while max fits in 32 bits.
+uint64_t np_interval(NpBitgen* g, uint64_t max) {
+  if (max == 0) return 0;
+  uint64_t mask = max;
+  mask |= mask >> 1;
+  mask |= mask >> 2;
+  mask |= mask >> 4;
+  mask |= mask >> 8;
+  mask |= mask >> 16;
+  mask |= mask >> 32;
+  uint64_t v;
+  if (max <= 0xffffffffULL) {
+    do {
+      v = g->next_uint32(g->state) & mask;
+    } while (v > max);
+  } else {
+    do {
+      v = g->next_uint64(g->state) & mask;
+    } while (v > max);
+  }
+  return v;
+}
+
+}  // namespace
+
+extern "C" int lmb_de_shuffles(void* bitgen, long long* index, long long n,
+                               long long count, int keep, long long* out) {
+  if (!bitgen || n < 0 || count < 0 || keep < 0 || keep > n) return LMB_ERR_ARG;
+  if ((n > 0 && !index) || (count > 0 && keep > 0 && !out)) return LMB_ERR_ARG;
+  NpBitgen* g = static_cast<NpBitgen*>(bitgen);
+  for (long long c = 0; c < count; ++c) {
+    // Generator.shuffle / RandomState.shuffle of a 1-d array: Fisher-Yates
+    // from the last entry down, partner drawn on [0, i]
+    for (long long i = n - 1; i >= 1; --i) {
+      const long long j = (long long)np_interval(g, (uint64_t)i);
+      const long long t = index[i];
+      index[i] = index[j];
+      index[j] = t;
+    }
+    for (int k = 0; k < keep; ++k) out[c * keep + k] = index[k];
+  }
+  return LMB_OK;
+}

@@ -195,3 +195,33 @@ def test_one_shape_group_matches_scipy():
                                          **de_settings(p['settings']))
         _assert_same(r, ref)
     assert len({r.nit for r in got}) > 3      # they finished apart
+
+
+@pytest.mark.parametrize('kind', ['RandomState', 'Generator'])
+def test_native_shuffles_are_numpys(kind):
+    '''lmb_de_shuffles (the per-candidate sample draws of a generation in
+    one native call on the generator's own bit generator) against numpy's
+    shuffle: the same permutations and the same state after, from any
+    point of the stream (an odd number of 32-bit draws consumed too), for
+    sizes 0 to past 2**16.'''
+    from pylorenzmie_b200.analysis._de import _shuffles
+    for seed in range(12):
+        for n in (0, 1, 2, 3, 30, 33, 70000):
+            a, b = ((np.random.RandomState(seed), np.random.RandomState(seed))
+                    if kind == 'RandomState' else
+                    (np.random.default_rng(seed), np.random.default_rng(seed)))
+            for r in (a, b):
+                r.uniform(size=3)
+                r.randint(7) if kind == 'RandomState' else r.integers(7)
+            count = 3 if n > 1000 else 20
+            keep = min(3, n)
+            ia, ib = np.arange(n), np.arange(n, dtype=np.int64)
+            ref = np.empty((count, keep), dtype=np.int64)
+            for c in range(count):
+                a.shuffle(ia)
+                ref[c] = ia[:keep]
+            out = np.empty((count, keep), dtype=np.int64)
+            _shuffles(b, ib, count, out)
+            np.testing.assert_array_equal(out, ref)
+            np.testing.assert_array_equal(ib, ia)
+            assert a.uniform() == b.uniform()

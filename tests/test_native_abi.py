@@ -103,6 +103,16 @@ def test_argument_checks_of_the_search_and_variant_entry_points(lib):
     for args in ((-1, 0, 10, 3), (2, 3, 10, 3), (2, 2, 2, 3), (2, 2, 10, 0),
                  (2, 2, 10, 7), (2, 2, 10, 3)):    # the last: null buffers
         assert trial(*args) == ARG and select(*args) == ARG, args
+    # lmb_de_shuffles (host): a bit generator is required, keep <= n
+    idx = np.arange(4, dtype=np.int64)
+    out = np.zeros((2, 3), dtype=np.int64)
+    assert lib.lmb_de_shuffles(None, idx.ctypes.data, 4, 2, 3,
+                               out.ctypes.data) == ARG
+    bg = np.random.default_rng(0).bit_generator
+    assert lib.lmb_de_shuffles(bg.ctypes.bit_generator, idx.ctypes.data, 4,
+                               2, 5, out.ctypes.data) == ARG
+    assert lib.lmb_de_shuffles(bg.ctypes.bit_generator, idx.ctypes.data, 4,
+                               0, 3, None) == OK
     # lmb_chi2_crops: no items is a no-op; items without crops are not
     assert lib.lmb_chi2_crops(None, 0, None, 0.05, None, 0, None, 0, None,
                               None, 0, None, None, 10, 1., 3, None, None,
