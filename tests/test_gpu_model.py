@@ -54,6 +54,55 @@ def test_sphere_ab_matches_reference(golden_ab):
         assert err < 1e-11, (i, err)
 
 
+def test_sphere_ab_large_spheres_vs_oracle():
+    '''Spheres of 64..421 orders (the estimators' bounds reach a_p = 10 um
+    with n_p = 3), where the medium's D1 is formed by the warp scan: a_n,
+    b_n against the oracle's serial recurrences to 1e-11 of their largest
+    value, and the a_p / n_p derivatives against central differences of
+    the oracle to 1e-6 of their largest value plus the differences' own
+    error (steps h and h/2: sharp resonances of lossless spheres).'''
+    import torch
+    from oracle import mie as omie
+    from pylorenzmie_b200.theory import _kernels as K
+    rng = np.random.default_rng(17)
+    n_m, lam = 1.34, 0.447
+    cases = [(10., 3., 0.), (10., 1.0, 0.), (2.6, 1.7, 1e-3), (6., 2.,
+                                                                0.), (4., 1.2, 0.)]
+    cases += [(rng.uniform(2.8, 10.), rng.uniform(1.0, 3.0),
+               rng.choice([0., 0.02])) for _ in range(11)]
+    P = np.zeros((len(cases), 6))
+    P[:, 3:] = cases
+    refs = [omie.mie_coefficients(a, n, k, n_m, lam) for a, n, k in cases]
+    nmaxs = [len(r) - 1 for r in refs]
+    assert min(nmaxs) >= 64 and max(nmaxs) >= 400
+    cap = max(nmaxs)
+    ab, dab, nmax = K.sphere_ab(torch.as_tensor(P, device='cuda:0'), n_m,
+                                lam, cap, deriv=True)
+    ab = ab.cpu().numpy().view(np.complex128)[..., 0]
+    dab = dab.cpu().numpy().view(np.complex128)[..., 0]
+    np.testing.assert_array_equal(nmax.cpu().numpy(), nmaxs)
+    for i, (a, n, k) in enumerate(cases):
+        ref = refs[i]
+        nm = nmaxs[i]
+        err = np.abs(ab[i, :nm + 1] - ref).max() / np.abs(ref).max()
+        assert err < 1e-11, (cases[i], err)
+        assert np.all(ab[i, nm + 1:] == 0)
+        for j, (da, dn) in enumerate(((1e-6, 0.), (0., 1e-7))):
+            fds = []
+            for f in (1., 0.5):
+                up = omie.mie_coefficients(a + f * da, n + f * dn, k, n_m,
+                                           lam)
+                lo = omie.mie_coefficients(a - f * da, n - f * dn, k, n_m,
+                                           lam)
+                L = min(len(up), len(lo), nm + 1)
+                fds.append((up[:L] - lo[:L]) / (2 * f * (da + dn)))
+            L = min(len(fds[0]), len(fds[1]))
+            fd = fds[1][:L]
+            allowed = 1e-6 * np.abs(fd).max() + 4. * np.abs(fds[0][:L] - fd)
+            got = dab[i, :L, 2 * j:2 * j + 2]
+            assert np.all(np.abs(got - fd) <= allowed), (cases[i], j)
+
+
 @pytest.mark.parametrize('name', HOLO_CASES)
 def test_hologram_fp32(golden_holo, name):
     m, cart, bohren = model_for(golden_holo, name)
