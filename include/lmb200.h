@@ -465,6 +465,23 @@ int lmb_de_shuffles(void *bitgen, long long *index, long long n,
                     long long count, int keep, long long *out);
 
 /*
+ * All draws of one search's generation, in scipy's order, on numpy's bit
+ * generator (its lock held by the caller): with dither, *scale =
+ * rng.uniform(dlo, dhi); then n shuffles of index as lmb_de_shuffles
+ * (count = n, the first keep entries of each to first[c * keep ..]); then
+ * fill[0..n) = rng.integers(nparam, size=n) (masked != 0: the masked
+ * rejection of RandomState.randint; 0: Generator.integers, Lemire's
+ * method); then cross[0..n*nparam) = rng.uniform(size=(n, nparam)) < cr.
+ * The same draws as DifferentialEvolutionSolver's best1bin trial
+ * construction with binomial crossover and dithered mutation, which the
+ * reference's estimators reach (analysis/DEEstimator.py:158-166).
+ */
+int lmb_de_draws(void *bitgen, int masked, int dither, double dlo,
+                 double dhi, double *scale, long long *index, long long n,
+                 int keep, long long *first, int nparam, double cr,
+                 long long *fill, unsigned char *cross);
+
+/*
  * lmb_fit_batch (any layer count) that starts before all of its pixel data
  * is on the device.  No counterpart in the reference, whose fits run one
  * feature at a time on the host.

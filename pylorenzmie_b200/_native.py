@@ -121,6 +121,8 @@ _SIGNATURES = {
     'lmb_measure_fp32_peak': (_i, [ctypes.POINTER(_d), _vp]),
     'lmb_pack_crops': (_i, [_vp, _vp, _i, _i, _vp, _i]),
     'lmb_de_shuffles': (_i, [_vp, _vp, _ll, _ll, _i, _vp]),
+    'lmb_de_draws': (_i, [_vp, _i, _i, _d, _d, _vp, _vp, _ll, _i, _vp, _i,
+                          _d, _vp, _vp]),
 }
 
 _lock = threading.Lock()

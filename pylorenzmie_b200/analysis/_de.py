@@ -21,6 +21,7 @@ each is a valid search but not the one a lone call would make.
 ``supported`` tells which settings this covers; the estimators run the rest
 through scipy.
 '''
+import ctypes
 import numbers
 
 import numpy as np
@@ -78,26 +79,28 @@ def _generator(seed):
     raise ValueError(f'{seed!r} cannot seed a numpy.random.RandomState')
 
 
-def _integers(rng, high, size):
-    '''Integers in [0, high), as scipy's rng_integers.'''
-    if isinstance(rng, np.random.Generator):
-        return rng.integers(high, size=size, dtype='int64')
-    return rng.randint(high, size=size, dtype='int64')
-
-
-def _shuffles(rng, index, count, out):
-    '''``count`` times: rng.shuffle(index), then out[c] = index[:3] --
-    in one native call on the generator's own bit generator
-    (lmb_de_shuffles: numpy's shuffle restated, the same draws in the same
-    order).'''
-    bg = (rng.bit_generator if isinstance(rng, np.random.Generator)
-          else rng._bit_generator)
+def _draws(rng, dither, index, N, P, cr, first, fill, cross):
+    '''One search's draws of a generation in scipy's order, in one native
+    call on the generator's own bit generator (lmb_de_draws: numpy's
+    algorithms restated, the same draws in the same order): the dithered
+    scale rng.uniform(*dither) (returned; None without dither), N times
+    rng.shuffle(index) keeping index[:3] in first (N, 3), fill (N,) =
+    the crossover's forced parameter, cross (N, P) = rng.uniform(size=(N,
+    P)) < cr.'''
+    gen = isinstance(rng, np.random.Generator)
+    bg = rng.bit_generator if gen else rng._bit_generator
+    scale = ctypes.c_double(0.)
+    lo, hi = (float(dither[0]), float(dither[1])) if dither is not None \
+        else (0., 0.)
     lib = _native.load()
     with bg.lock:
-        st = lib.lmb_de_shuffles(bg.ctypes.bit_generator, index.ctypes.data,
-                                 len(index), count, out.shape[1],
-                                 out.ctypes.data)
-    _native.check(st, 'lmb_de_shuffles')
+        st = lib.lmb_de_draws(bg.ctypes.bit_generator, int(not gen),
+                              int(dither is not None), lo, hi,
+                              ctypes.addressof(scale), index.ctypes.data, N,
+                              first.shape[1], first.ctypes.data, P, float(cr),
+                              fill.ctypes.data, cross.ctypes.data)
+    _native.check(st, 'lmb_de_draws')
+    return scale.value if dither is not None else None
 
 
 class Populations:
@@ -187,15 +190,13 @@ class Populations:
         fill = np.empty((len(T), N), dtype='int64')
         cross = np.empty((len(T), N, P), dtype=bool)
         for i, s in enumerate(T):
-            rng = self.rngs[s]
-            if self.dither[s] is not None:
-                self.scale[s] = rng.uniform(self.dither[s][0],
-                                            self.dither[s][1])
-            # mutation, best1: for each candidate the first two of a fresh
-            # shuffle of the kept permutation other than the candidate
-            _shuffles(rng, self.index[s], N, first[i])
-            fill[i] = _integers(rng, P, N)
-            cross[i] = rng.uniform(size=(N, P)) < self.cr[s]
+            # dithered scale; mutation, best1: for each candidate the first
+            # two of a fresh shuffle of the kept permutation other than the
+            # candidate; binomial crossover's forced parameter and draws
+            scale = _draws(self.rngs[s], self.dither[s], self.index[s], N, P,
+                           self.cr[s], first[i], fill[i], cross[i])
+            if scale is not None:
+                self.scale[s] = scale
         c = np.arange(N)
         f0, f1, f2 = first[..., 0], first[..., 1], first[..., 2]
         r0 = np.where(f0 == c, f1, f0)

@@ -232,3 +232,61 @@ extern "C" int lmb_de_shuffles(void* bitgen, long long* index, long long n,
   }
   return LMB_OK;
 }
+
+namespace {
+
+// numpy's bounded integers on [0, rng] for rng < 2^32 (the 32-bit branch
+// of random_bounded_uint64_fill): masked rejection for RandomState,
+// Lemire's multiply-shift rejection (Lemire 2019) for Generator.
+uint64_t np_bounded32(NpBitgen* g, uint32_t rng, bool masked) {
+  if (rng == 0) return 0;
+  if (rng == 0xffffffffu) return g->next_uint32(g->state);
+  if (masked) {
+    uint32_t mask = rng;
+    mask |= mask >> 1;
+    mask |= mask >> 2;
+    mask |= mask >> 4;
+    mask |= mask >> 8;
+    mask |= mask >> 16;
+    uint32_t v;
+    do {
+      v = g->next_uint32(g->state) & mask;
+    } while (v > rng);
+    return v;
+  }
+  const uint32_t excl = rng + 1;
+  uint64_t m = uint64_t(g->next_uint32(g->state)) * excl;
+  uint32_t left = uint32_t(m);
+  if (left < excl) {
+    const uint32_t threshold = (0xffffffffu - rng) % excl;
+    while (left < threshold) {
+      m = uint64_t(g->next_uint32(g->state)) * excl;
+      left = uint32_t(m);
+    }
+  }
+  return m >> 32;
+}
+
+}  // namespace
+
+extern "C" int lmb_de_draws(void* bitgen, int masked, int dither, double dlo,
+                            double dhi, double* scale, long long* index,
+                            long long n, int keep, long long* first,
+                            int nparam, double cr, long long* fill,
+                            unsigned char* cross) {
+  if (!bitgen || n < 1 || keep < 0 || keep > n || nparam < 1) return LMB_ERR_ARG;
+  if (!index || (keep > 0 && !first) || !fill || !cross) return LMB_ERR_ARG;
+  if (dither && !scale) return LMB_ERR_ARG;
+  NpBitgen* g = static_cast<NpBitgen*>(bitgen);
+  // rng.uniform(lo, hi): lower + range * next_double
+  if (dither) *scale = dlo + (dhi - dlo) * g->next_double(g->state);
+  const int st = lmb_de_shuffles(bitgen, index, n, n, keep, first);
+  if (st != LMB_OK) return st;
+  // rng.integers(nparam, size=n) / rng.randint(nparam, size=n)
+  for (long long c = 0; c < n; ++c)
+    fill[c] = (long long)np_bounded32(g, uint32_t(nparam - 1), masked != 0);
+  // rng.uniform(size=(n, nparam)) < cr
+  for (long long k = 0; k < n * nparam; ++k)
+    cross[k] = g->next_double(g->state) < cr;
+  return LMB_OK;
+}

@@ -197,19 +197,27 @@ def test_one_shape_group_matches_scipy():
     assert len({r.nit for r in got}) > 3      # they finished apart
 
 
+def _pair(kind, seed):
+    if kind == 'RandomState':
+        return np.random.RandomState(seed), np.random.RandomState(seed)
+    return np.random.default_rng(seed), np.random.default_rng(seed)
+
+
+def _bitgen(rng):
+    return (rng.bit_generator if isinstance(rng, np.random.Generator)
+            else rng._bit_generator)
+
+
 @pytest.mark.parametrize('kind', ['RandomState', 'Generator'])
 def test_native_shuffles_are_numpys(kind):
-    '''lmb_de_shuffles (the per-candidate sample draws of a generation in
-    one native call on the generator's own bit generator) against numpy's
-    shuffle: the same permutations and the same state after, from any
-    point of the stream (an odd number of 32-bit draws consumed too), for
-    sizes 0 to past 2**16.'''
-    from pylorenzmie_b200.analysis._de import _shuffles
+    '''lmb_de_shuffles against numpy's shuffle: the same permutations and
+    the same state after, from any point of the stream (an odd number of
+    32-bit draws consumed too), for sizes 0 to past 2**16.'''
+    from pylorenzmie_b200 import _native
+    lib = _native.load()
     for seed in range(12):
         for n in (0, 1, 2, 3, 30, 33, 70000):
-            a, b = ((np.random.RandomState(seed), np.random.RandomState(seed))
-                    if kind == 'RandomState' else
-                    (np.random.default_rng(seed), np.random.default_rng(seed)))
+            a, b = _pair(kind, seed)
             for r in (a, b):
                 r.uniform(size=3)
                 r.randint(7) if kind == 'RandomState' else r.integers(7)
@@ -221,7 +229,48 @@ def test_native_shuffles_are_numpys(kind):
                 a.shuffle(ia)
                 ref[c] = ia[:keep]
             out = np.empty((count, keep), dtype=np.int64)
-            _shuffles(b, ib, count, out)
+            bg = _bitgen(b)
+            with bg.lock:
+                assert lib.lmb_de_shuffles(bg.ctypes.bit_generator,
+                                           ib.ctypes.data, n, count, keep,
+                                           out.ctypes.data) == 0
             np.testing.assert_array_equal(out, ref)
             np.testing.assert_array_equal(ib, ia)
             assert a.uniform() == b.uniform()
+
+
+@pytest.mark.parametrize('kind', ['RandomState', 'Generator'])
+def test_native_generation_draws_are_numpys(kind):
+    '''_draws (lmb_de_draws: a search's whole generation of draws in one
+    native call) against the numpy calls scipy makes, in its order: the
+    dithered scale, the N shuffles, the crossover's forced parameters
+    (RandomState.randint / Generator.integers) and the crossover uniforms;
+    identical values and the same generator state after.'''
+    from pylorenzmie_b200.analysis._de import _draws
+    for seed in range(10):
+        for N, P in ((5, 1), (30, 3), (31, 5), (60, 6)):
+            for dither in (None, (0.5, 1.0)):
+                a, b = _pair(kind, seed)
+                for r in (a, b):
+                    r.uniform(size=seed % 3)
+                ia = np.arange(N, dtype=np.int64)
+                ib = ia.copy()
+                sa = a.uniform(*dither) if dither else None
+                fa = np.empty((N, 3), dtype=np.int64)
+                for c in range(N):
+                    a.shuffle(ia)
+                    fa[c] = ia[:3]
+                filla = (a.integers(P, size=N, dtype='int64')
+                         if kind == 'Generator' else
+                         a.randint(P, size=N, dtype='int64'))
+                crossa = a.uniform(size=(N, P)) < 0.7
+                fb = np.empty_like(fa)
+                fillb = np.empty(N, dtype=np.int64)
+                crossb = np.empty((N, P), dtype=bool)
+                sb = _draws(b, dither, ib, N, P, 0.7, fb, fillb, crossb)
+                assert sb == sa
+                np.testing.assert_array_equal(fb, fa)
+                np.testing.assert_array_equal(fillb, filla)
+                np.testing.assert_array_equal(crossb, crossa)
+                np.testing.assert_array_equal(ib, ia)
+                assert a.uniform() == b.uniform()

@@ -113,6 +113,19 @@ def test_argument_checks_of_the_search_and_variant_entry_points(lib):
                                2, 5, out.ctypes.data) == ARG
     assert lib.lmb_de_shuffles(bg.ctypes.bit_generator, idx.ctypes.data, 4,
                                0, 3, None) == OK
+    # lmb_de_draws (host): n >= 1, keep <= n, nparam >= 1, buffers
+    fill = np.zeros(4, dtype=np.int64)
+    cross = np.zeros((4, 2), dtype=bool)
+    first = np.zeros((4, 3), dtype=np.int64)
+    def draws(n, keep, npar, fb=fill.ctypes.data):
+        return lib.lmb_de_draws(bg.ctypes.bit_generator, 1, 0, 0., 0., None,
+                                idx.ctypes.data, n, keep, first.ctypes.data,
+                                npar, 0.7, fb, cross.ctypes.data)
+    assert draws(0, 0, 2) == ARG and draws(4, 5, 2) == ARG
+    assert draws(4, 3, 0) == ARG and draws(4, 3, 2, None) == ARG
+    assert lib.lmb_de_draws(bg.ctypes.bit_generator, 1, 1, 0.5, 1., None,
+                            idx.ctypes.data, 4, 3, first.ctypes.data, 2, 0.7,
+                            fill.ctypes.data, cross.ctypes.data) == ARG
     # lmb_chi2_crops: no items is a no-op; items without crops are not
     assert lib.lmb_chi2_crops(None, 0, None, 0.05, None, 0, None, 0, None,
                               None, 0, None, None, 10, 1., 3, None, None,
