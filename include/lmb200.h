@@ -482,6 +482,20 @@ int lmb_de_draws(void *bitgen, int masked, int dither, double dlo,
                  long long *fill, unsigned char *cross);
 
 /*
+ * lmb_de_draws for nsearch searches in turn (each search's draws complete
+ * before the next, so searches that share a generator draw in the order of
+ * separate calls): per search s its bit generator, flags, dither bounds,
+ * crossover probability and index row; outputs packed by search (scale[s],
+ * first + s*n*keep, fill + s*n, cross + s*n*nparam).  The caller holds
+ * every generator's lock.
+ */
+int lmb_de_draws_many(int nsearch, void *const *bitgens, const int *masked,
+                      const int *dither, const double *dlo, const double *dhi,
+                      double *scale, long long *const *index, long long n,
+                      int keep, long long *first, int nparam, const double *cr,
+                      long long *fill, unsigned char *cross);
+
+/*
  * lmb_fit_batch (any layer count) that starts before all of its pixel data
  * is on the device.  No counterpart in the reference, whose fits run one
  * feature at a time on the host.

@@ -79,28 +79,45 @@ def _generator(seed):
     raise ValueError(f'{seed!r} cannot seed a numpy.random.RandomState')
 
 
-def _draws(rng, dither, index, N, P, cr, first, fill, cross):
-    '''One search's draws of a generation in scipy's order, in one native
-    call on the generator's own bit generator (lmb_de_draws: numpy's
-    algorithms restated, the same draws in the same order): the dithered
-    scale rng.uniform(*dither) (returned; None without dither), N times
-    rng.shuffle(index) keeping index[:3] in first (N, 3), fill (N,) =
-    the crossover's forced parameter, cross (N, P) = rng.uniform(size=(N,
-    P)) < cr.'''
-    gen = isinstance(rng, np.random.Generator)
-    bg = rng.bit_generator if gen else rng._bit_generator
-    scale = ctypes.c_double(0.)
-    lo, hi = (float(dither[0]), float(dither[1])) if dither is not None \
-        else (0., 0.)
-    lib = _native.load()
-    with bg.lock:
-        st = lib.lmb_de_draws(bg.ctypes.bit_generator, int(not gen),
-                              int(dither is not None), lo, hi,
-                              ctypes.addressof(scale), index.ctypes.data, N,
-                              first.shape[1], first.ctypes.data, P, float(cr),
-                              fill.ctypes.data, cross.ctypes.data)
-    _native.check(st, 'lmb_de_draws')
-    return scale.value if dither is not None else None
+def _draws(rngs, dithers, crs, index_rows, N, P, first, fill, cross):
+    '''The draws of one generation of several searches in scipy's order, in
+    one native call on the generators' own bit generators (lmb_de_draws_many:
+    numpy's algorithms restated, the same draws in the same order, search
+    after search).  Per search s: the dithered scale rng.uniform(*dither)
+    (returned in scale[s]; NaN without dither), N times
+    rng.shuffle(index_rows[s]) keeping its first three entries in first[s]
+    (N, 3), fill[s] (N,) = the crossover's forced parameters, cross[s]
+    (N, P) = rng.uniform(size=(N, P)) < crs[s].'''
+    S = len(rngs)
+    bgs = [r.bit_generator if isinstance(r, np.random.Generator)
+           else r._bit_generator for r in rngs]
+    ptrs = np.array([bg.ctypes.bit_generator.value for bg in bgs],
+                    dtype=np.uintp)
+    masked = np.array([not isinstance(r, np.random.Generator) for r in rngs],
+                      dtype=np.int32)
+    has = np.array([d is not None for d in dithers], dtype=np.int32)
+    lo = np.array([d[0] if d is not None else 0. for d in dithers], dtype=float)
+    hi = np.array([d[1] if d is not None else 0. for d in dithers], dtype=float)
+    cr = np.ascontiguousarray(crs, dtype=float)
+    rows = np.array([r.ctypes.data for r in index_rows], dtype=np.uintp)
+    scale = np.empty(S)
+    locks = {id(bg): bg.lock for bg in bgs}
+    held = []
+    try:
+        for k in sorted(locks):
+            locks[k].acquire()
+            held.append(locks[k])
+        st = _native.load().lmb_de_draws_many(
+            S, ptrs.ctypes.data, masked.ctypes.data, has.ctypes.data,
+            lo.ctypes.data, hi.ctypes.data, scale.ctypes.data,
+            rows.ctypes.data, N, first.shape[-1], first.ctypes.data, P,
+            cr.ctypes.data, fill.ctypes.data, cross.ctypes.data)
+    finally:
+        for lock in held:
+            lock.release()
+    _native.check(st, 'lmb_de_draws_many')
+    scale[has == 0] = np.nan
+    return scale
 
 
 class Populations:
@@ -165,7 +182,7 @@ class Populations:
         self.pop = np.array(pops)
         self.energies = np.full((S, self.N), np.inf)
         self.trial = np.zeros_like(self.pop)
-        self.index = [np.arange(self.N, dtype=np.int64) for _ in range(S)]
+        self.index = np.tile(np.arange(self.N, dtype=np.int64), (S, 1))
         self.trialed = np.zeros(S, dtype=bool)   # last request was a trial
         self.nfev = np.zeros(S, dtype=int)
         self.nit = np.zeros(S, dtype=int)
@@ -189,14 +206,14 @@ class Populations:
         first = np.empty((len(T), N, 3), dtype=self.index[0].dtype)
         fill = np.empty((len(T), N), dtype='int64')
         cross = np.empty((len(T), N, P), dtype=bool)
-        for i, s in enumerate(T):
-            # dithered scale; mutation, best1: for each candidate the first
-            # two of a fresh shuffle of the kept permutation other than the
-            # candidate; binomial crossover's forced parameter and draws
-            scale = _draws(self.rngs[s], self.dither[s], self.index[s], N, P,
-                           self.cr[s], first[i], fill[i], cross[i])
-            if scale is not None:
-                self.scale[s] = scale
+        # dithered scale; mutation, best1: for each candidate the first two
+        # of a fresh shuffle of the kept permutation other than the
+        # candidate; binomial crossover's forced parameter and draws
+        scale = _draws([self.rngs[s] for s in T],
+                       [self.dither[s] for s in T], self.cr[T],
+                       [self.index[s] for s in T], N, P, first, fill, cross)
+        dithered = ~np.isnan(scale)
+        self.scale[T[dithered]] = scale[dithered]
         c = np.arange(N)
         f0, f1, f2 = first[..., 0], first[..., 1], first[..., 2]
         r0 = np.where(f0 == c, f1, f0)

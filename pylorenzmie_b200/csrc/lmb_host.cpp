@@ -290,3 +290,29 @@ extern "C" int lmb_de_draws(void* bitgen, int masked, int dither, double dlo,
     cross[k] = g->next_double(g->state) < cr;
   return LMB_OK;
 }
+
+extern "C" int lmb_de_draws_many(int nsearch, void* const* bitgens,
+                                 const int* masked, const int* dither,
+                                 const double* dlo, const double* dhi,
+                                 double* scale, long long* const* index,
+                                 long long n, int keep, long long* first,
+                                 int nparam, const double* cr,
+                                 long long* fill, unsigned char* cross) {
+  if (nsearch < 0) return LMB_ERR_ARG;
+  if (nsearch == 0) return LMB_OK;
+  if (!bitgens || !masked || !dither || !dlo || !dhi || !scale || !index ||
+      !cr)
+    return LMB_ERR_ARG;
+  // search by search, each search's draws complete before the next: the
+  // order of lmb_de_draws called in turn, also where searches share a
+  // generator
+  for (int s = 0; s < nsearch; ++s) {
+    const int st = lmb_de_draws(
+        bitgens[s], masked[s], dither[s], dlo[s], dhi[s], scale + s, index[s],
+        n, keep, first ? first + size_t(s) * n * keep : nullptr, nparam, cr[s],
+        fill ? fill + size_t(s) * n : nullptr,
+        cross ? cross + size_t(s) * n * nparam : nullptr);
+    if (st != LMB_OK) return st;
+  }
+  return LMB_OK;
+}

@@ -239,38 +239,57 @@ def test_native_shuffles_are_numpys(kind):
             assert a.uniform() == b.uniform()
 
 
-@pytest.mark.parametrize('kind', ['RandomState', 'Generator'])
-def test_native_generation_draws_are_numpys(kind):
-    '''_draws (lmb_de_draws: a search's whole generation of draws in one
-    native call) against the numpy calls scipy makes, in its order: the
-    dithered scale, the N shuffles, the crossover's forced parameters
-    (RandomState.randint / Generator.integers) and the crossover uniforms;
-    identical values and the same generator state after.'''
+def _numpy_draws(rng, dither, index, N, P, cr):
+    '''One search's generation of draws by numpy's own calls, scipy's
+    order.'''
+    scale = rng.uniform(*dither) if dither else np.nan
+    first = np.empty((N, 3), dtype=np.int64)
+    for c in range(N):
+        rng.shuffle(index)
+        first[c] = index[:3]
+    fill = (rng.integers(P, size=N, dtype='int64')
+            if isinstance(rng, np.random.Generator) else
+            rng.randint(P, size=N, dtype='int64'))
+    return scale, first, fill, rng.uniform(size=(N, P)) < cr
+
+
+def test_native_generation_draws_are_numpys():
+    '''_draws (lmb_de_draws_many: a generation of several searches' draws
+    in one native call) against the numpy calls scipy makes, search after
+    search: the dithered scale, the N shuffles, the crossover's forced
+    parameters (RandomState.randint / Generator.integers) and the crossover
+    uniforms; identical values and the same generator states after, with
+    RandomState and Generator searches mixed and two searches sharing one
+    generator.'''
     from pylorenzmie_b200.analysis._de import _draws
-    for seed in range(10):
+    for seed in range(8):
         for N, P in ((5, 1), (30, 3), (31, 5), (60, 6)):
-            for dither in (None, (0.5, 1.0)):
-                a, b = _pair(kind, seed)
-                for r in (a, b):
+            def make():
+                shared = np.random.RandomState(seed + 100)
+                rngs = [np.random.RandomState(seed),
+                        np.random.default_rng(seed), shared,
+                        np.random.default_rng(seed + 1), shared]
+                for r in rngs[:4]:
                     r.uniform(size=seed % 3)
-                ia = np.arange(N, dtype=np.int64)
-                ib = ia.copy()
-                sa = a.uniform(*dither) if dither else None
-                fa = np.empty((N, 3), dtype=np.int64)
-                for c in range(N):
-                    a.shuffle(ia)
-                    fa[c] = ia[:3]
-                filla = (a.integers(P, size=N, dtype='int64')
-                         if kind == 'Generator' else
-                         a.randint(P, size=N, dtype='int64'))
-                crossa = a.uniform(size=(N, P)) < 0.7
-                fb = np.empty_like(fa)
-                fillb = np.empty(N, dtype=np.int64)
-                crossb = np.empty((N, P), dtype=bool)
-                sb = _draws(b, dither, ib, N, P, 0.7, fb, fillb, crossb)
-                assert sb == sa
-                np.testing.assert_array_equal(fb, fa)
-                np.testing.assert_array_equal(fillb, filla)
-                np.testing.assert_array_equal(crossb, crossa)
-                np.testing.assert_array_equal(ib, ia)
+                return rngs
+            ra, rb = make(), make()
+            dithers = [None, (0.5, 1.0), (0.4, 0.9), None, (0.5, 1.0)]
+            crs = np.array([0.7, 0.9, 0.5, 0.7, 0.3])
+            S = len(ra)
+            ia = np.tile(np.arange(N, dtype=np.int64), (S, 1))
+            ib = ia.copy()
+            ref = [_numpy_draws(ra[s], dithers[s], ia[s], N, P, crs[s])
+                   for s in range(S)]
+            first = np.empty((S, N, 3), dtype=np.int64)
+            fill = np.empty((S, N), dtype=np.int64)
+            cross = np.empty((S, N, P), dtype=bool)
+            scale = _draws(rb, dithers, crs, [ib[s] for s in range(S)], N, P,
+                           first, fill, cross)
+            for s in range(S):
+                np.testing.assert_array_equal(scale[s], ref[s][0])
+                np.testing.assert_array_equal(first[s], ref[s][1])
+                np.testing.assert_array_equal(fill[s], ref[s][2])
+                np.testing.assert_array_equal(cross[s], ref[s][3])
+            np.testing.assert_array_equal(ib, ia)
+            for a, b in zip(ra, rb):
                 assert a.uniform() == b.uniform()

@@ -126,6 +126,10 @@ def test_argument_checks_of_the_search_and_variant_entry_points(lib):
     assert lib.lmb_de_draws(bg.ctypes.bit_generator, 1, 1, 0.5, 1., None,
                             idx.ctypes.data, 4, 3, first.ctypes.data, 2, 0.7,
                             fill.ctypes.data, cross.ctypes.data) == ARG
+    assert lib.lmb_de_draws_many(0, None, None, None, None, None, None,
+                                 None, 4, 3, None, 2, None, None, None) == OK
+    assert lib.lmb_de_draws_many(2, None, None, None, None, None, None,
+                                 None, 4, 3, None, 2, None, None, None) == ARG
     # lmb_chi2_crops: no items is a no-op; items without crops are not
     assert lib.lmb_chi2_crops(None, 0, None, 0.05, None, 0, None, 0, None,
                               None, 0, None, None, 10, 1., 3, None, None,
