@@ -17,6 +17,8 @@ import numpy as np
 import torch
 from scipy.optimize import differential_evolution
 
+from .. import _native
+from .._device import ptr, stream_handle
 from ..theory import _kernels as K
 
 SPHERE_KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
@@ -197,22 +199,80 @@ class CropPopulations:
             out[i] = float(v[0]) if np.ndim(batch[i]) == 1 else v
         return out
 
+    def _buffers(self, n, cap):
+        '''Pinned staging and device buffers for n candidates of up to cap
+        orders, kept between generations and grown when needed (a
+        generation ends with its results read back, so the next one may
+        reuse them).'''
+        b = getattr(self, '_bufs', None)
+        if b is None or b['n'] < n or b['cap'] < cap:
+            n = max(n, b['n'] if b else 0)
+            cap = max(cap, b['cap'] if b else 0)
+            dev = self.device
+            lib = _native.load()
+            ws = lib.lmb_chi2_workspace_bytes(int(self.max_npts), n)
+            b = dict(n=n, cap=cap, ws_bytes=ws,
+                     host_in=torch.empty(n * 52, dtype=torch.uint8,
+                                         pin_memory=True),
+                     dev_in=torch.empty(n * 52, dtype=torch.uint8,
+                                        device=dev),
+                     host_out=torch.empty(n * 12, dtype=torch.uint8,
+                                          pin_memory=True),
+                     item_start=torch.arange(n + 1, dtype=torch.int32,
+                                             device=dev),
+                     ab=torch.empty(n * (cap + 1) * 4, dtype=torch.float64,
+                                    device=dev),
+                     nmax=torch.empty(n, dtype=torch.int32, device=dev),
+                     status=torch.empty(n, dtype=torch.int32, device=dev),
+                     chi2=torch.empty(n, dtype=torch.float64, device=dev),
+                     bad=torch.empty(n, dtype=torch.int32, device=dev),
+                     ws=torch.empty(max(ws, 1), dtype=torch.uint8,
+                                    device=dev))
+            self._bufs = b
+        return b
+
     def _launch(self, P, crop):
+        '''chi^2 of candidates P (n, 6) against their crops: the sphere
+        records and crop indices in one copy from pinned memory, the
+        coefficients and sums into kept buffers (lmb_sphere_ab,
+        lmb_chi2_crops), the sums and overflow counts read back together;
+        FP32 sums that overflowed are redone in FP64.'''
         dev = self.device
-        sp = K.spheres_tensor(_records(P), dev)
+        n = len(P)
         cap = K.nmax_cap_for(P[:, 3], P[:, 4], P[:, 5], self.n_m,
                              self.wavelength)
-        ab, _, nmax = K.sphere_ab(sp, self.n_m, self.wavelength, cap,
-                                  check=False)
-        n = len(P)
-        item_start = torch.arange(n + 1, dtype=torch.int32, device=dev)
-        item_crop = K.to_device_async(crop, dev)
-        chi2, bad = K.chi2_crops(self.coords, self.data, self.noise,
-                                 self.crop_start, item_crop, self.max_npts,
-                                 sp, item_start, ab, nmax, cap, self.k,
-                                 fp64=self.fp64, aberration=self.aberr)
-        bad = bad.cpu().numpy()
-        chi2 = chi2.cpu().numpy()
+        b = self._buffers(n, cap)
+        hin = b['host_in'].numpy()
+        hin[:48 * n].view(np.float64)[:] = np.ascontiguousarray(
+            P, dtype=np.float64).ravel()
+        hin[48 * n:52 * n].view(np.int32)[:] = crop
+        b['dev_in'][:52 * n].copy_(b['host_in'][:52 * n], non_blocking=True)
+        sp = b['dev_in'][:48 * n].view(torch.float64).view(n, 6)
+        item_crop = b['dev_in'][48 * n:52 * n].view(torch.int32)
+        ab = b['ab'][:n * (cap + 1) * 4].view(n, cap + 1, 2, 2)
+        nmax = b['nmax'][:n]
+        lib = _native.load()
+        stream = stream_handle(dev)
+        _native.check(lib.lmb_sphere_ab(
+            ptr(sp), n, float(self.n_m), float(self.wavelength), cap, ptr(ab),
+            None, ptr(nmax), ptr(b['status']), stream), 'lmb_sphere_ab')
+        _native.check(lib.lmb_chi2_crops(
+            ptr(self.coords), self.coords.shape[1], ptr(self.data),
+            float(self.noise), ptr(self.crop_start),
+            self.crop_start.shape[0] - 1, ptr(item_crop), int(self.max_npts),
+            ptr(sp), ptr(b['item_start']), n, ptr(ab), ptr(nmax), cap,
+            float(self.k), K._flags(True, True, self.fp64), ptr(b['chi2']),
+            ptr(b['bad']), ptr(b['ws']), b['ws_bytes'], stream,
+            float(self.aberr)), 'lmb_chi2_crops')
+        hout = b['host_out']
+        hout[:8 * n].view(torch.float64).copy_(b['chi2'][:n],
+                                               non_blocking=True)
+        hout[8 * n:12 * n].view(torch.int32).copy_(b['bad'][:n],
+                                                   non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        out = hout.numpy()
+        chi2 = out[:8 * n].view(np.float64).copy()
+        bad = out[8 * n:12 * n].view(np.int32).copy()
         redo = np.flatnonzero(bad) if not self.fp64 else []
         if len(redo):
             # FP32 overflow where the focal plane cuts the sphere: FP64
