@@ -71,13 +71,17 @@ def run_search(model, data, coords, variables, bounds, noise, popsize, seed,
     saved = model.coordinates
     try:
         if batchable(model, variables):
-            objective = PopulationChi2(model, data, coords, variables, noise)
             if supported(settings):
+                # the crops objective over this one crop: the same values
+                # as PopulationChi2, with its buffers kept between
+                # generations
+                pop = CropPopulations([(model, data, coords, variables)],
+                                      noise)
                 problem = dict(bounds=bounds, popsize=popsize, seed=seed,
                                settings=settings)
                 with np.errstate(over='ignore', invalid='ignore'):
-                    return run_populations(
-                        [problem], lambda b: {0: objective(b[0])})[0]
+                    return run_populations([problem], pop.evaluate)[0]
+            objective = PopulationChi2(model, data, coords, variables, noise)
         else:
             model.coordinates = coords
             objective = _HostObjective(model, data, variables, noise)
