@@ -199,9 +199,10 @@ def render_particles(particles, shapes, seed=0, instrument=None, device=None,
     return out
 
 
-def _run_estimate_frame(device_search, repeat):
+def _run_estimate_frame(device_search, repeat, optimize=False):
     '''Frame.estimate of the estimate workload, ``repeat`` times (the first
-    one warms up); prints the seconds each took.'''
+    one warms up), and with ``optimize`` Frame.optimize after each; prints
+    the seconds each took.'''
     import time
     import torch
     from .theory import Instrument
@@ -220,15 +221,22 @@ def _run_estimate_frame(device_search, repeat):
         f.estimate()
         torch.cuda.synchronize()
         print(f'estimate_frame {rep}: {time.perf_counter() - t0:.4f} s')
+        if optimize:
+            t0 = time.perf_counter()
+            f.optimize()
+            torch.cuda.synchronize()
+            print(f'optimize_frame {rep}: {time.perf_counter() - t0:.4f} s')
 
 
 if __name__ == '__main__':
     # python -m pylorenzmie_b200.workloads estimate_frame [--device-search]
+    #     [--optimize]
     # runs one workload through the public API, e.g. under a profiler
     import argparse
     ap = argparse.ArgumentParser()
     ap.add_argument('workload', choices=['estimate_frame'])
     ap.add_argument('--device-search', action='store_true')
     ap.add_argument('--repeat', type=int, default=2)
+    ap.add_argument('--optimize', action='store_true')
     a = ap.parse_args()
-    _run_estimate_frame(a.device_search, a.repeat)
+    _run_estimate_frame(a.device_search, a.repeat, a.optimize)
