@@ -788,7 +788,11 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
         status = LMB_ERR_CUDA;
         break;
       }
-      int issued = 1, consumed = 0, depth = 2, eval_rounds = 0;
+      // Rounds in flight outside the tail: 2 for large batches, whose
+      // rounds outlast the host's turnaround; 4 for small ones (at most
+      // 128 features), whose rounds take tens of microseconds.
+      const int base_depth = nfeatures <= 128 ? 4 : 2;
+      int issued = 1, consumed = 0, depth = base_depth, eval_rounds = 0;
       bool capped = false;
       for (;;) {
         while (!capped && issued - consumed < depth) {
@@ -822,7 +826,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
         counted_evals = r;
         if (capped || cnt[1] == 0) break;
         const bool tail = cnt[1] * 16 <= nfeatures;
-        depth = tail ? std::min(2 * depth, 16) : 2;
+        depth = tail ? std::min(2 * depth, 16) : base_depth;
       }
       if (status != LMB_OK) break;
     } else {
