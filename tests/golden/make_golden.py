@@ -1,34 +1,39 @@
 '''Generate the golden fixtures of tests/golden/ by running the reference.
 
-Run from the repository root on a machine that has the reference checkout
-(default ``/root/reference``; override with ``LM_REFERENCE``):
+Run from the repository root on a machine that has the reference checkout,
+naming it with ``--reference`` or the ``LM_REFERENCE`` environment variable:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference PATH [fixture ...]
 
-The reference package is made importable as ``pylorenzmie`` through a
-symlink in a temporary directory, with an empty ``trackpy`` stub (its
-analysis/__init__.py imports Localizer, which imports trackpy).  The numpy
-FP64 model is imported explicitly from ``pylorenzmie.theory.LorenzMie``
-because the package-level ``LorenzMie`` resolves to the fastmath numba
-backend (theory/__init__.py:33-38).
+(no fixture names: all of them).  The reference package is made importable
+as ``pylorenzmie`` through a symlink in a temporary directory, with an empty
+``trackpy`` stub (its analysis/__init__.py imports Localizer, which imports
+trackpy).  The numpy FP64 model is imported explicitly from
+``pylorenzmie.theory.LorenzMie`` because the package-level ``LorenzMie``
+resolves to the fastmath numba backend (theory/__init__.py:33-38).
 
 Outputs (small, committed):
   ab.npz        Sphere.mie_coefficients for a table of spheres
-  layered.npz   sphere_coefficients (one layer, scalar input) for a table
+  layered.npz   sphere_coefficients: one layer (scalar input, as the
+                reference accepts it) and 2- to 4-layer spheres (the
+                reference's recurrences with its input handling repaired;
+                see reference_layered below)
   holo.npz      LorenzMie.field/hologram for the reference tests' geometries
   fit.npz       a seeded 201x201 fit by the reference Optimizer
   estimate.npz  seeded DEEstimator and RadialEstimator searches (81x81 crop)
   variants.npz  AberratedLorenzMie and Dimer holograms
 '''
+import argparse
 import os
 import sys
 import tempfile
+import types
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = os.environ.get('LM_REFERENCE', '/root/reference')
+REFERENCE = None  # set by main()
 
 
 def import_reference():
@@ -73,6 +78,58 @@ def make_ab():
     np.savez_compressed(HERE / 'ab.npz', **out)
 
 
+# The reference's multilayer entry point (lib/obsolete/sphere_coefficients.py)
+# cannot take more than one layer as written: it wraps its inputs in an
+# extra dimension and counts layers by ndim (:85-87), checks the indices the
+# same way (:89-90), and takes the builtin max of arrays in wiscombe_yang
+# (:61).  These three replacements repair only that input handling, so that
+# the recurrences of :126-215 run unchanged on 1-D radii and indices
+# ordered from the core outwards.
+LAYERED_INPUT_FIXES = [
+    ('    a_p = np.array([a_p])\n    n_p = np.array([n_p])\n'
+     '    nlayers = a_p.ndim\n',
+     '    a_p = np.atleast_1d(np.asarray(a_p, dtype=float))\n'
+     '    n_p = np.atleast_1d(np.asarray(n_p, dtype=complex))\n'
+     '    nlayers = a_p.size\n'),
+    ('    assert n_p.ndim == nlayers,', '    assert n_p.size == nlayers,'),
+    ('    nstop = max(ns, xm, xm_1)',
+     '    nstop = max(ns, np.max(xm), np.max(xm_1))'),
+]
+
+
+def reference_layered():
+    '''The reference module's sphere_coefficients, executed from its own
+    source file with LAYERED_INPUT_FIXES applied (each must match once).'''
+    path = Path(REFERENCE) / 'lib' / 'obsolete' / 'sphere_coefficients.py'
+    src = path.read_text()
+    for old, new in LAYERED_INPUT_FIXES:
+        if src.count(old) != 1:
+            raise RuntimeError(f'reference source changed: {old!r}')
+        src = src.replace(old, new)
+    mod = types.ModuleType('reference_sphere_coefficients')
+    mod.__file__ = str(path)
+    exec(compile(src, str(path), 'exec'), mod.__dict__)
+    return mod.sphere_coefficients
+
+
+def layered_cases():
+    '''Multilayer table: (radii core -> outer [um], indices core -> outer,
+    n_m, wavelength).  The last four are seeded draws of the layered-stream
+    workload (3 layers, fractions U(0.3, 0.9) nested, indices U(1.33,
+    1.80), outer radius U(0.5, 2.5) um).'''
+    cases = [([0.3, 0.75], [1.6, 1.45 + 0.002j], 1.34, 0.447),
+             ([0.4, 0.8, 1.2], [1.8 + 0.01j, 1.33, 1.5], 1.34, 0.447),
+             ([0.5, 1.25, 2.0], [1.4, 1.7, 1.55 + 0.001j], 1.34, 0.447),
+             ([0.2, 0.35, 0.5, 0.9], [2.0, 1.4, 1.6, 1.38], 1.333, 0.532)]
+    rng = np.random.default_rng(31)
+    for _ in range(4):
+        a = rng.uniform(0.5, 2.5)
+        frac = np.sort(rng.uniform(0.3, 0.9, 2))
+        idx = rng.uniform(1.33, 1.80, 3)
+        cases.append((list(np.append(frac * a, a)), list(idx), 1.34, 0.447))
+    return cases
+
+
 def make_layered():
     from pylorenzmie.lib.obsolete.sphere_coefficients import \
         sphere_coefficients
@@ -81,6 +138,20 @@ def make_layered():
     out = {'cases': np.array(cases, dtype=complex)}
     for i, (a, n, nm, lam) in enumerate(cases):
         out[f'ab_{i}'] = sphere_coefficients(a, n, nm, lam, resolution=None)
+    repaired = reference_layered()
+    multi = layered_cases()
+    out['multi_count'] = np.array(len(multi))
+    for i, (radii, idx, nm, lam) in enumerate(multi):
+        out[f'multi_radii_{i}'] = np.array(radii, dtype=float)
+        out[f'multi_indices_{i}'] = np.array(idx, dtype=complex)
+        out[f'multi_medium_{i}'] = np.array([nm, lam])
+        out[f'multi_ab_{i}'] = repaired(radii, idx, nm, lam, resolution=None)
+    # the repaired entry point on one layer is the reference's own output
+    # (to rounding: the index enters as complex instead of real)
+    for i, (a, n, nm, lam) in enumerate(cases):
+        ref = out[f'ab_{i}']
+        got = repaired([a], [n], nm, lam, resolution=None)
+        assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
     np.savez_compressed(HERE / 'layered.npz', **out)
 
 
@@ -238,12 +309,29 @@ def make_variants():
     np.savez_compressed(HERE / 'variants.npz', **out)
 
 
-if __name__ == '__main__':
+MAKERS = {'ab': lambda: make_ab(), 'layered': lambda: make_layered(),
+          'holo': lambda: make_holo(), 'fit': lambda: make_fit(),
+          'estimate': lambda: make_estimate(),
+          'variants': lambda: make_variants()}
+
+
+def main(argv=None):
+    global REFERENCE
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument('--reference', default=os.environ.get('LM_REFERENCE'),
+                    help='path of the reference checkout (or LM_REFERENCE)')
+    ap.add_argument('fixtures', nargs='*', choices=[[], *MAKERS],
+                    help='fixtures to write (default: all)')
+    a = ap.parse_args(argv)
+    if not a.reference:
+        ap.error('name the reference checkout with --reference or '
+                 'LM_REFERENCE')
+    REFERENCE = a.reference
     import_reference()
-    make_ab()
-    make_layered()
-    make_holo()
-    make_fit()
-    make_estimate()
-    make_variants()
+    for name in a.fixtures or list(MAKERS):
+        MAKERS[name]()
     print('golden fixtures written to', HERE)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,8 +1,9 @@
 '''GPU: multilayer (core-shell) spheres -- Yang coefficients, holograms,
 Jacobians and batched fits -- against the FP64 oracle (a restatement of
-lib/obsolete/sphere_coefficients.py with its input handling repaired; the
-one-layer case is pinned to the reference's own output, the multilayer
-values are parity unpinned beyond the oracle).'''
+lib/obsolete/sphere_coefficients.py with its input handling repaired).  The
+coefficients are pinned to the reference's own output: one layer as the
+reference accepts it, and 2-4 layers from the reference's recurrences run
+with only their input handling repaired (tests/golden/make_golden.py).'''
 import numpy as np
 import pytest
 
@@ -32,6 +33,20 @@ def test_layered_ab_matches_oracle(golden_layered):
                           core_indices=core)
         ab = s.ab(1.34, 0.447)
         ref = mie.layered_coefficients(s.radii, s.indices, 1.34, 0.447)
+        assert ab.shape == ref.shape
+        assert np.abs(ab - ref).max() <= 1e-11 * np.abs(ref).max()
+
+
+def test_layered_ab_matches_reference_multilayer(golden_layered):
+    '''2-, 3- and 4-layer coefficients from the device kernel against the
+    reference's own recurrences.'''
+    from pylorenzmie_b200 import LayeredSphere
+    from tests.test_oracle_golden import multilayer_cases
+    for radii, idx, nm, lam, ref in multilayer_cases(golden_layered):
+        s = LayeredSphere(a_p=radii[-1], n_p=idx[-1].real, k_p=idx[-1].imag,
+                          fractions=tuple(radii[:-1] / radii[-1]),
+                          core_indices=tuple(idx[:-1]))
+        ab = s.ab(nm, lam)
         assert ab.shape == ref.shape
         assert np.abs(ab - ref).max() <= 1e-11 * np.abs(ref).max()
 

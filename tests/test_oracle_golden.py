@@ -38,6 +38,27 @@ def test_layered_one_layer(golden_layered):
         assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def multilayer_cases(golden_layered):
+    for i in range(int(golden_layered['multi_count'])):
+        nm, lam = golden_layered[f'multi_medium_{i}']
+        yield (golden_layered[f'multi_radii_{i}'],
+               golden_layered[f'multi_indices_{i}'], nm, lam,
+               golden_layered[f'multi_ab_{i}'])
+
+
+def test_layered_multilayer(golden_layered):
+    '''2-, 3- and 4-layer spheres against the reference's own Yang
+    recurrences (lib/obsolete/sphere_coefficients.py:126-215, run with its
+    input handling repaired by tests/golden/make_golden.py).'''
+    n = 0
+    for radii, idx, nm, lam, ref in multilayer_cases(golden_layered):
+        ab = mie.layered_coefficients(radii, idx, nm, lam)
+        assert ab.shape == ref.shape
+        assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()
+        n += 1
+    assert n >= 8
+
+
 def test_layered_reduces_to_homogeneous():
     '''Equal indices in every layer: the multilayer recurrence reproduces
     the homogeneous sphere (up to its D1 start one order higher).'''
