@@ -184,6 +184,17 @@ int field_launch(const double* coords, long long npts, const lmb_sphere* spheres
         coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
         nmax_cap + 1, k, flags, aberr, out);
     LMB_CK(cudaGetLastError());
+    if constexpr (kHolo) {
+      // FP64 re-summation of the pixels marked by the FP32 pass
+      const size_t smem64 = sizeof(Quad<double>) * 2 * (size_t(nmax_cap) + 1);
+      auto fix = k_field<double, true, true>;
+      LMB_CK(smem_attr((const void*)fix, smem64));
+      dim3 grid64(unsigned((npts + tpb - 1) / tpb), unsigned(nitems));
+      fix<<<grid64, tpb, smem64, as_stream(stream)>>>(
+          coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
+          nmax_cap + 1, k, flags, aberr, out);
+      LMB_CK(cudaGetLastError());
+    }
     return LMB_OK;
   }
   const size_t smem = sizeof(Quad<R>) * 2 * (size_t(nmax_cap) + 1);

@@ -373,7 +373,11 @@ __device__ inline cplx<R> aberration_phase(double c, double dx, double dy,
 }
 
 // aberr: the coefficient c above, 0 for an ideal instrument.
-template <typename R, bool kHologram>
+// kFix (FP64 holograms only): sum again only the pixels that the FP32
+// hologram kernel marked with a negative value in out (its error bound
+// exceeded HOLO_TOL) and overwrite them with the FP32-rounded FP64 value;
+// blocks without such a pixel return at once.
+template <typename R, bool kHologram, bool kFix = false>
 __global__ void __launch_bounds__(256)
 k_field(const double* __restrict__ coords, long long npts,
         const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
@@ -383,7 +387,12 @@ k_field(const double* __restrict__ coords, long long npts,
   Quad<R>* coef = reinterpret_cast<Quad<R>*>(smem);
   const int item = blockIdx.y;
   const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = pix < npts;
+  bool live = pix < npts;
+  if constexpr (kFix) {
+    static_assert(kHologram, "the FP64 fix-up pass is for holograms");
+    if (live) live = reinterpret_cast<const float*>(out)[(size_t)item * npts + pix] < 0.f;
+    if (!__syncthreads_or(live)) return;
+  }
   const bool cart = flags & LMB_CARTESIAN;
   const bool bohren = flags & LMB_BOHREN;
   double x = 0., y = 0., z = 0.;
@@ -415,7 +424,10 @@ k_field(const double* __restrict__ coords, long long npts,
     }
   }
   if (!live) return;
-  if (kHologram) {
+  if constexpr (kFix) {
+    float* o = reinterpret_cast<float*>(out) + (size_t)item * npts;
+    o[pix] = float(intensity<R>(e));
+  } else if (kHologram) {
     R* o = reinterpret_cast<R*>(out) + (size_t)item * npts;
     o[pix] = intensity<R>(e);
   } else {
@@ -432,8 +444,11 @@ k_field(const double* __restrict__ coords, long long npts,
 
 // FP32 field / hologram with the packed two-pixel loop: each thread takes
 // two adjacent pixels (the last thread of an odd count pairs its pixel with
-// itself).  Same inputs, outputs and arithmetic as k_field<float, holo>;
-// the order loop runs in f32x2 (order_sum_pair).
+// itself).  Same inputs and outputs as k_field<float, holo>; the order loop
+// runs in f32x2 (order_sum_pair) and the phase argument in FP64.  Holograms
+// also accumulate each pixel's error bound (holo_needs_fp64) and write -1 in
+// place of the pixels that need FP64, which k_field<double, true, true>
+// then sums again.
 template <bool kHologram>
 __global__ void __launch_bounds__(256)
 k_field_pair(const double* __restrict__ coords, long long npts,
@@ -461,18 +476,27 @@ k_field_pair(const double* __restrict__ coords, long long npts,
   cplx<float> e[2][3];
   for (int l = 0; l < 2; ++l)
     for (int c = 0; c < 3; ++c) e[l][c] = mk(0.f, 0.f);
+  float m1[2] = {0.f, 0.f}, m0[2] = {0.f, 0.f};  // error bound (holograms)
+  __shared__ float s_amp;
   const int pb = item_start[item], pe = item_start[item + 1];
   for (int p = pb; p < pe; ++p) {
     const int nm = min(max(nmax[p], 0), nmaxp - 1);
+    const zd* abp = ab + size_t(p) * nmaxp * 2;
     __syncthreads();
-    stage_pair_value(ab + size_t(p) * nmaxp * 2, nm, rec);
+    stage_pair_value(abp, nm, rec);
+    if (kHologram && threadIdx.x < 32) {
+      double a = 0.;
+      for (int n = 1 + threadIdx.x; n <= nm; n += 32) a += order_amplitude(abp + 2 * n, n);
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (threadIdx.x == 0) s_amp = float(a);
+    }
     __syncthreads();
     if (live0) {
       const lmb_sphere sp = spheres[p];
       Geometry<float> g[2];
       for (int l = 0; l < 2; ++l)
-        g[l] = geometry<float>(k, x[l] - sp.x_p, y[l] - sp.y_p, z[l] - sp.z_p, z[l],
-                               sp.z_p, bohren);
+        g[l] = geometry<float, true>(k, x[l] - sp.x_p, y[l] - sp.y_p, z[l] - sp.z_p,
+                                     z[l], sp.z_p, bohren);
       PairSumsV S;
       order_sum_pair(pair_in(g[0], g[1]), rec, nm, S);
 #pragma unroll
@@ -486,6 +510,7 @@ k_field_pair(const double* __restrict__ coords, long long npts,
           for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
         }
         for (int c = 0; c < 3; ++c) e[l][c] = e[l][c] + ep[c];
+        if (kHologram) holo_bound_add(ep, s_amp, g[l].ikr, m1[l], m0[l]);
       }
     }
   }
@@ -495,7 +520,8 @@ k_field_pair(const double* __restrict__ coords, long long npts,
     const long long pix = l ? p1 : p0;
     if (kHologram) {
       float* o = reinterpret_cast<float*>(out) + (size_t)item * npts;
-      o[pix] = intensity<float>(e[l]);
+      const float h = intensity<float>(e[l]);
+      o[pix] = holo_needs_fp64(h, m1[l], m0[l]) ? -1.f : h;
     } else {
       float2* o = reinterpret_cast<float2*>(out) + (size_t)item * 3 * npts;
       for (int c = 0; c < 3; ++c) o[c * npts + pix] = make_float2(e[l][c].re, e[l][c].im);

@@ -82,7 +82,26 @@ struct Geometry {
 //   z: the pixel's own z coordinate; zp: the particle's z
 LMB_HD double reduce_2pi(double t) { return remainder(t, 6.283185307179586); }
 
-template <typename R>
+// t reduced to about [-pi, pi] by Cody and Waite's additive reduction
+// (W. J. Cody, W. Waite, Software Manual for the Elementary Functions,
+// 1980) with 2 pi split into a double C1 and its remainder C2: with a fused
+// multiply-add, t - q C1 is exact for |q| < 2^20, so the result carries an
+// absolute error of about 1e-16 + q 1e-32.  For the phase arguments of the
+// field kernels (|t| up to ~10^4 rad); larger |t| take reduce_2pi.
+LMB_HD double reduce_2pi_cw(double t) {
+  const double C1 = 6.283185307179586;       // 2 pi rounded to double
+  const double C2 = 2.4492935982947064e-16;  // 2 pi - C1
+  if (!(fabs(t) < 1e6)) return reduce_2pi(t);
+  const double q = rint(t * 0.15915494309189535);
+  return fma(-q, C2, fma(-q, C1, t));
+}
+
+// kPhase64: form the phase argument sign(kz) (kr - |kz|) - k z in FP64 from
+// the FP64 offsets (R = float only).  Far from the particle (kr ~ 10^3 rad)
+// the FP32 argument, and even the FP32 roundings of kx, ky and kz that it
+// is formed from, are off by ~1e-4 rad; in FP64 the phase is exact to FP32
+// rounding.  The fits' crops (kr ~ 10^2) do not need it.
+template <typename R, bool kPhase64 = false>
 LMB_HD Geometry<R> geometry(double k, double dx, double dy, double dzc,
                             double z, double zp, bool bohren) {
   Geometry<R> g;
@@ -117,9 +136,17 @@ LMB_HD Geometry<R> geometry(double k, double dx, double dy, double dzc,
     g.h0 = mk(R(0), -sigma);
     if (sigma == s) {
       // sign(kz) (kr - |kz|) - k z, with kr - |kz| = krho^2/(kr + |kz|)
-      R arg = s * krho2 / (kr + labs_(kz));
-      if (z != 0.) arg += R(reduce_2pi(-k * z));
-      g.phase = cis(arg);
+      if (kPhase64) {
+        const double rho2 = dx * dx + dy * dy;
+        const double r = sqrt(rho2 + dzc * dzc);
+        double arg = double(s) * k * rho2 / (r + fabs(dzc));
+        if (z != 0.) arg -= k * z;
+        g.phase = cis(R(reduce_2pi_cw(arg)));
+      } else {
+        R arg = s * krho2 / (kr + labs_(kz));
+        if (z != 0.) arg += R(reduce_2pi(-k * z));
+        g.phase = cis(arg);
+      }
     } else {
       const double kr64 = k * sqrt(dx * dx + dy * dy + dzc * dzc);
       g.phase = cis(R(reduce_2pi(double(sigma) * kr64 - k * zp)));
@@ -834,6 +861,51 @@ LMB_HD cplx<R> aberration_wave(double c, double dx, double dy, double zp,
 template <typename R>
 LMB_HD R intensity(const cplx<R>* e) {
   return norm2(e[0]) + norm2(e[1]) + norm2(e[2]) + R(2) * e[0].re + R(1);
+}
+
+// ---------------------------------------------------------------------------
+// Error bound of an FP32 hologram pixel, for the FP64 re-summation of the
+// pixels where FP32 cannot reach HOLO_TOL.
+//
+// The FP32 field of one particle at a pixel (phase in FP64, as the field
+// kernels form it) differs from its FP64 value by at most about
+//   HOLO_FIELD_REL |E_p| + HOLO_FIELD_FLOOR A_p / kr,
+// where A_p = sum_n (n + 1/2)(|a_n| + |b_n|) is the particle's partial-wave
+// amplitude and A_p / kr the size of the terms of its sums at the pixel.
+// The first term is the relative error of the coefficient records and the
+// recurrences (a few ulp of the field where it is large, e.g. on the axis
+// of a big sphere that focuses the light), the second the rounding left
+// where the sums cancel.  Measured on the CPU build of the packed loop over
+// 21 frames of 1280x1024 px with 3-16 spheres each (a_p 0.4-3 um, n_p
+// 1.38-1.70, z_p 50-600 px and at least 10 px above the sphere's top): the
+// actual hologram error is at most 0.59 of the bound below, the bound
+// exceeds HOLO_TOL on 0.06-1.1 % of the pixels, and the largest error left
+// on the others is 8.5e-6.  Since dH = 2 Re(conj(E + x) dE), the hologram
+// is off by at most
+//   2 sqrt(H) sum_p (HOLO_FIELD_REL |E_p| + HOLO_FIELD_FLOOR A_p / kr),
+// and pixels where that exceeds HOLO_TOL are summed again in FP64.
+#define HOLO_FIELD_REL 3e-6f
+#define HOLO_FIELD_FLOOR 1e-7f
+#define HOLO_TOL 2e-5f
+
+// (n + 1/2)(|a_n| + |b_n|): order n's share of A_p.
+LMB_HD double order_amplitude(const cplx<double>* ab, int n) {
+  return (double(n) + 0.5) * (sqrt(norm2(ab[0])) + sqrt(norm2(ab[1])));
+}
+
+// Per-pixel accumulation of the bound over the particles: m1 += |E_p|,
+// m0 += A_p / kr.
+LMB_HD void holo_bound_add(const cplx<float>* ep, float amp, float ikr,
+                           float& m1, float& m0) {
+  m1 += sqrtf(norm2(ep[0]) + norm2(ep[1]) + norm2(ep[2]));
+  m0 += amp * ikr;
+}
+
+// True when the FP32 value h may be off by more than HOLO_TOL.
+LMB_HD bool holo_needs_fp64(float h, float m1, float m0) {
+  const float bound =
+      2.f * sqrtf(fmaxf(h, 0.f)) * (HOLO_FIELD_REL * m1 + HOLO_FIELD_FLOOR * m0);
+  return bound > HOLO_TOL;
 }
 
 }  // namespace lmb

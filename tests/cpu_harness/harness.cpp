@@ -197,7 +197,8 @@ API void h_field(const double* coords, long long npts, const double* p,
 }
 
 // Field of one sphere through the packed two-pixel value loop (pixels i and
-// i + 1 share one pass; an odd last pixel is paired with itself), FP32.
+// i + 1 share one pass; an odd last pixel is paired with itself), FP32 with
+// the phase argument in FP64, as k_field_pair computes it.
 API void h_field_pair(const double* coords, long long npts, const double* p,
                   const double* ab, int nmax, double k, int flags,
                   double* out) {
@@ -216,7 +217,7 @@ API void h_field_pair(const double* coords, long long npts, const double* p,
     for (int l = 0; l < 2; ++l) {
       const long long ii = l ? i1 : i;
       const double x = coords[ii], y = coords[npts + ii], z = coords[2 * npts + ii];
-      g[l] = geometry<float>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
+      g[l] = geometry<float, true>(k, x - p[0], y - p[1], z - p[2], z, p[2], flags & 2);
     }
     PairSumsV S;
     order_sum_pair(pair_in(g[0], g[1]), q.data(), nmax, S);
@@ -227,6 +228,66 @@ API void h_field_pair(const double* coords, long long npts, const double* p,
       for (int c = 0; c < 3; ++c) {
         out[2 * (c * npts + ii)] = e[c].re;
         out[2 * (c * npts + ii) + 1] = e[c].im;
+      }
+    }
+  }
+}
+
+// FP32 hologram of np spheres p [np][6] through the packed two-pixel value
+// loop with the FP64 phase and the per-pixel error bound, as
+// k_field_pair<true> computes it: holo[i] = H, or -1 where the bound asks
+// for the FP64 sum (flags & 8: the FP32 value everywhere).  ab:
+// [np][cap+1][2] complex, nmax: [np].  terms (optional, [2][npts]):
+// 2 sqrt(H) sum |E_p| and 2 sqrt(H) sum A_p / kr.
+API void h_hologram_pair(const double* coords, long long npts, const double* p,
+                         int np, const double* ab, const int* nmax, int cap,
+                         double k, int flags, float* holo, float* terms) {
+  std::vector<std::vector<Quad<float>>> q(np);
+  std::vector<float> amp(np);
+  for (int j = 0; j < np; ++j) {
+    const double* abj = ab + size_t(j) * (cap + 1) * 4;
+    q[j].resize(PAIRV_QUADS * (nmax[j] + 1));
+    double a = 0.;
+    for (int n = 0; n <= nmax[j]; ++n) {
+      zd c[2];
+      for (int i = 0; i < 2; ++i) c[i] = mk(abj[4 * n + 2 * i], abj[4 * n + 2 * i + 1]);
+      float v[PAIRV_VALUES];
+      pair_value_record(c, n, v);
+      for (int i = 0; i < PAIRV_QUADS; ++i)
+        q[j][PAIRV_QUADS * n + i] = Quad<float>{v[2 * i], v[2 * i], v[2 * i + 1], v[2 * i + 1]};
+      if (n > 0) a += order_amplitude(c, n);
+    }
+    amp[j] = float(a);
+  }
+  for (long long i = 0; i < npts; i += 2) {
+    const long long i1 = i + 1 < npts ? i + 1 : i;
+    cplx<float> e[2][3];
+    float m1[2] = {0.f, 0.f}, m0[2] = {0.f, 0.f};
+    for (int l = 0; l < 2; ++l)
+      for (int c = 0; c < 3; ++c) e[l][c] = mk(0.f, 0.f);
+    for (int j = 0; j < np; ++j) {
+      const double* pj = p + 6 * j;
+      Geometry<float> g[2];
+      for (int l = 0; l < 2; ++l) {
+        const long long ii = l ? i1 : i;
+        const double x = coords[ii], y = coords[npts + ii], z = coords[2 * npts + ii];
+        g[l] = geometry<float, true>(k, x - pj[0], y - pj[1], z - pj[2], z, pj[2], flags & 2);
+      }
+      PairSumsV S;
+      order_sum_pair(pair_in(g[0], g[1]), q[j].data(), nmax[j], S);
+      for (int l = 0; l < 2; ++l) {
+        cplx<float> ep[3];
+        epilogue<float>(g[l], pair_lane_value(S, l, g[l].smu), flags & 1, ep);
+        for (int c = 0; c < 3; ++c) e[l][c] = e[l][c] + ep[c];
+        holo_bound_add(ep, amp[j], g[l].ikr, m1[l], m0[l]);
+      }
+    }
+    for (int l = 0; l < 2; ++l) {
+      const float h = intensity<float>(e[l]);
+      holo[l ? i1 : i] = (flags & 8) == 0 && holo_needs_fp64(h, m1[l], m0[l]) ? -1.f : h;
+      if (terms) {  // the bound's two terms before their constants
+        terms[l ? i1 : i] = 2.f * sqrtf(fmaxf(h, 0.f)) * m1[l];
+        terms[npts + (l ? i1 : i)] = 2.f * sqrtf(fmaxf(h, 0.f)) * m0[l];
       }
     }
   }

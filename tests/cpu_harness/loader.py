@@ -55,6 +55,11 @@ def load():
     lib.h_field_pair.argtypes = [_dp, ctypes.c_longlong, _dp, _dp,
                                  ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                  _dp]
+    lib.h_hologram_pair.argtypes = [_dp, ctypes.c_longlong, _dp, ctypes.c_int,
+                                    _dp, _ip, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_float)]
     lib.h_jacobian_pair.argtypes = [_dp, ctypes.c_longlong, _dp, _dp, _dp,
                                     ctypes.c_int, ctypes.c_double,
                                     ctypes.c_int, _dp, _dp]
@@ -175,6 +180,29 @@ class Harness:
                               (1 if cartesian else 0) | (2 if bohren else 0),
                               ptr(out))
         return out[..., 0] + 1j * out[..., 1]
+
+    def hologram_pair(self, coords, particles, k, cap=400, flag=True):
+        '''FP32 hologram of several spheres (rows of x, y, z, a_p, n_p, k_p)
+        as k_field_pair computes it: (H with -1 where its error bound asks
+        for the FP64 sum (unless flag is False), the bound's two terms
+        (2, npts)).'''
+        c = np.ascontiguousarray(coords, dtype=float)
+        npts = c.shape[1]
+        P = np.ascontiguousarray(particles, dtype=float).reshape(-1, 6)
+        ab = np.zeros((P.shape[0], cap + 1, 2, 2))
+        nmax = np.zeros(P.shape[0], np.int32)
+        for j, p in enumerate(P):
+            a = self.sphere_ab(p[3], p[4], p[5], 1.34, 0.447, cap)
+            nmax[j] = a.shape[0] - 1
+            ab[j, :a.shape[0], :, 0] = a.real
+            ab[j, :a.shape[0], :, 1] = a.imag
+        holo = np.zeros(npts, np.float32)
+        terms = np.zeros((2, npts), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.lib.h_hologram_pair(ptr(c), npts, ptr(P), P.shape[0], ptr(ab),
+                                 ptr(nmax, _ip), cap, k, 3 | (0 if flag else 8),
+                                 ptr(holo, fp), ptr(terms, fp))
+        return holo, terms
 
     def jacobian_aberrated(self, coords, p, ab, dab, k, aberration,
                            bohren=True, fp64=False):

@@ -221,6 +221,17 @@ def test_layered_one_layer_matches_reference(h, golden_layered):
         assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def test_layered_multilayer_matches_reference(h, golden_layered):
+    '''The kernels' Yang recurrences (both the serial and the split shell
+    forms) against the reference's own 2-4 layer coefficients.'''
+    from tests.test_oracle_golden import multilayer_cases
+    for radii, idx, nm, lam, ref in multilayer_cases(golden_layered):
+        for split in (False, True):
+            ab = h.layered_ab(radii, idx, nm, lam, split=split)
+            assert ab.shape == ref.shape
+            assert np.abs(ab - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize('shape,p', [
     ((48, 48), [20.3, 25.7, 120., 0.9, 1.6, 0.01]),
     ((40, 40), [20., 20., -130., 0.6, 1.5, 0.]),
@@ -312,3 +323,30 @@ def test_layered_split_shell_is_identical(h, radii, idx):
     a2, d2 = h.layered_ab(radii, idx, 1.34, 0.447, deriv=True, split=True)
     np.testing.assert_array_equal(a1, a2)
     np.testing.assert_array_equal(d1, d2)
+
+
+def test_hologram_error_bound(h):
+    '''The per-pixel error bound of the FP32 hologram kernel.  A 3 um sphere
+    10 px above its top focuses light to H ~ 60 on its axis, where FP32
+    is off by more than 2e-5; the bound must cover the FP32 error at every
+    pixel, mark those pixels for the FP64 sum, and leave the others within
+    2e-5.'''
+    P = np.array([[80.3, 79.6, 72.5, 3.0, 1.56, 0.],
+                  [20.2, 150.7, 200., 1.5, 1.50, 1e-3],
+                  [150.1, 10.4, 130., 2.5, 1.65, 0.]])
+    c = field.meshgrid((160, 160))
+    ref = field.hologram(c, [dict(zip(KEYS, p)) for p in P],
+                         field.DEFAULT_INSTRUMENT)
+    h32, terms = h.hologram_pair(field.coordinates3(c), P, K, flag=False)
+    err = np.abs(h32.astype(float) - ref)
+    assert err.max() > 2e-5        # FP32 alone misses the tolerance here
+    bound = 3e-6 * terms[0].astype(float) + 1e-7 * terms[1]
+    assert np.all(err <= 0.75 * bound)
+    marked, _ = h.hologram_pair(field.coordinates3(c), P, K)
+    flag = marked < 0
+    assert np.all(flag[bound > 2e-5 * (1 + 1e-4)])
+    assert not np.any(flag[bound < 2e-5 * (1 - 1e-4)])
+    assert np.all(marked[~flag] == h32[~flag])
+    assert np.all(err[~flag] <= 2e-5)
+    # the window is centred on the focus; over whole frames about 0.5 %
+    assert flag.any() and flag.mean() < 0.25

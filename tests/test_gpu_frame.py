@@ -2,11 +2,12 @@
 larger mixed crops, against the FP64 oracle.
 
 Frames: the FP32 kernel against the FP64 kernel on every pixel, and against
-the numpy oracle on 20 000 random pixels of the frame (the oracle over the
-whole frame would take minutes).  Tolerance per pixel: 2e-5 + 2e-6 H.  Big
-spheres close to the focal plane focus light to H of 20-60 on the axis,
-where FP32 rounding of the order coefficients alone (about 6 ulp of the
-field) exceeds 2e-5 absolute; the relative error stays below 2e-6.
+the numpy oracle on 20 000 random pixels of the frame plus its brightest
+pixels (the oracle over the whole frame would take minutes).  Tolerance per
+pixel: 2e-5 absolute.  Big spheres close to the focal plane focus light to
+H of 20-70 on their axis, where FP32 sums are off by up to ~1e-4; the FP32
+kernel bounds its own error per pixel and those pixels are summed again in
+FP64 (lmb_hologram), so no pixel may exceed 2e-5.
 '''
 import numpy as np
 import pytest
@@ -18,27 +19,57 @@ pytestmark = pytest.mark.gpu
 KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
 
 
-@pytest.mark.parametrize('seed', [0, 1, 2])
+def bench_frame():
+    '''The 16-sphere frame that bench.py times.'''
+    from pylorenzmie_b200 import workloads
+    p = workloads.frame(seed=5)
+    while p.shape[0] < 16:
+        p = np.vstack([p, workloads.frame(seed=5 + p.shape[0])])[:16]
+    return p
+
+
+@pytest.mark.parametrize('seed', [0, 1, 2, 'bench'])
 def test_frame_fp32_vs_fp64_and_oracle(seed):
     from pylorenzmie_b200 import LorenzMie, workloads
-    P = workloads.frame(seed=seed)
+    P = bench_frame() if seed == 'bench' else workloads.frame(seed=seed)
     spheres = workloads.spheres(P)
     coords = LorenzMie.meshgrid((1024, 1280))
     h32 = LorenzMie(coordinates=coords, particle=spheres).hologram()
     h64 = LorenzMie(coordinates=coords, particle=spheres,
                     double_precision=True).hologram()
     assert h32.shape == (1024 * 1280,)
-    assert np.all(np.abs(h32 - h64) <= 2e-5 + 2e-6 * h64)
-    rng = np.random.default_rng(seed)
+    assert np.all(np.abs(h32 - h64) <= 2e-5)
+    rng = np.random.default_rng(7 if seed == 'bench' else seed)
     idx = rng.choice(coords.shape[1], 20000, replace=False)
+    # and the brightest pixels, where FP32 alone would miss the tolerance
+    idx = np.union1d(idx, np.argsort(h64)[-200:])
     sub = coords[:, idx]
     ref = ofield.hologram(sub, [dict(zip(KEYS, p)) for p in P],
                           ofield.DEFAULT_INSTRUMENT)
     assert np.abs(h64[idx] - ref).max() <= 1e-10
-    assert np.all(np.abs(h32[idx] - ref) <= 2e-5 + 2e-6 * ref)
+    assert np.all(np.abs(h32[idx] - ref) <= 2e-5)
     # the same pixels as an explicit coordinate list give the same values
     m = LorenzMie(coordinates=sub, particle=spheres)
     assert np.abs(m.hologram() - h32[idx]).max() <= 1e-6
+
+
+def test_frame_batch_items_fp64_resum():
+    '''Several frames in one launch (batch_hologram): each item's marked
+    pixels are summed again in FP64.'''
+    from pylorenzmie_b200 import LorenzMie, workloads
+    coords = LorenzMie.meshgrid((256, 320))
+    lists, refs = [], []
+    for seed in range(3):
+        P = workloads.frame(seed=seed, shape=(256, 320))[:4]
+        P[0] = [160.3, 127.8, 2.9 / 0.048 + 10., 2.9, 1.55, 0.]
+        lists.append(workloads.spheres(P))
+        refs.append(LorenzMie(coordinates=coords, particle=lists[-1],
+                              double_precision=True).hologram())
+    m = LorenzMie(coordinates=coords)
+    h = m.batch_hologram(lists)
+    for i in range(3):
+        assert np.abs(h[i] - refs[i]).max() <= 2e-5
+        assert refs[i].max() > 20.
 
 
 def test_fit_mixed_large_crops_vs_oracle():
