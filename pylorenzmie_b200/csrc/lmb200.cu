@@ -175,26 +175,28 @@ int field_launch(const double* coords, long long npts, const lmb_sphere* spheres
                  void* out, void* stream) {
   const int tpb = 256;
   if constexpr (sizeof(R) == sizeof(float)) {
-    // FP32: the packed two-pixel loop, two adjacent pixels per thread
-    const size_t smem = sizeof(float4) * PAIRV_QUADS * (size_t(nmax_cap) + 1);
+    // FP32: the packed two-pixel loop, two adjacent pixels per thread.  A
+    // ~100 KB block (two blocks per SM, as the registers allow) holds the
+    // records of many particles at once (at least one at nmax_cap), and for
+    // holograms the FP64 re-summation of the pixels that FP32 cannot
+    // resolve: particles in groups whose FP64 records fit.
+    const size_t nmaxp = size_t(nmax_cap) + 1;
+    const size_t budget = 100 * 1024;
+    size_t smem = std::max(budget, sizeof(float4) * PAIRV_QUADS * nmaxp);
+    int group = 1;
+    if (kHolo) {
+      const size_t fixed = RESUM_LIST_BYTES + RESUM_ACC_BYTES;
+      const size_t per = 2 * sizeof(Quad<double>) * nmaxp;
+      group = int(std::min<size_t>(32, std::max<size_t>(1, (budget - fixed) / per)));
+      smem = std::max(smem, fixed + per * size_t(group));
+    }
     auto fn = k_field_pair<kHolo>;
     LMB_CK(smem_attr((const void*)fn, smem));
     dim3 grid(unsigned((npts + 2 * tpb - 1) / (2 * tpb)), unsigned(nitems));
     fn<<<grid, tpb, smem, as_stream(stream)>>>(
         coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
-        nmax_cap + 1, k, flags, aberr, out);
+        nmax_cap + 1, k, flags, aberr, out, int(smem / sizeof(float4)), group);
     LMB_CK(cudaGetLastError());
-    if constexpr (kHolo) {
-      // FP64 re-summation of the pixels marked by the FP32 pass
-      const size_t smem64 = sizeof(Quad<double>) * 2 * (size_t(nmax_cap) + 1);
-      auto fix = k_field<double, true, true>;
-      LMB_CK(smem_attr((const void*)fix, smem64));
-      dim3 grid64(unsigned((npts + tpb - 1) / tpb), unsigned(nitems));
-      fix<<<grid64, tpb, smem64, as_stream(stream)>>>(
-          coords, npts, spheres, item_start, reinterpret_cast<const zd*>(ab), nmax,
-          nmax_cap + 1, k, flags, aberr, out);
-      LMB_CK(cudaGetLastError());
-    }
     return LMB_OK;
   }
   const size_t smem = sizeof(Quad<R>) * 2 * (size_t(nmax_cap) + 1);

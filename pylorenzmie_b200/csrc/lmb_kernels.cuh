@@ -308,6 +308,11 @@ __global__ void k_layered_ab(const double* radii, const double* indices, int L,
 // ---------------------------------------------------------------------------
 // Staging of per-order records (see lmb_pixel.cuh, struct Quad).
 
+// Shared-memory layout of the FP64 re-summation in k_field_pair<true>
+// (256 threads, 512 pixels a block): the marked-pixel list, the FP64 field
+// accumulators of up to 512 pixels, then the particles' FP64 records.
+enum { RESUM_LIST_BYTES = 512 * 4, RESUM_ACC_BYTES = 512 * 6 * 8 };
+
 template <typename R, bool kJac>
 __device__ void stage_coef(const zd* ab, const zd* dab, int nmax,
                            Quad<R>* sm) {
@@ -373,11 +378,7 @@ __device__ inline cplx<R> aberration_phase(double c, double dx, double dy,
 }
 
 // aberr: the coefficient c above, 0 for an ideal instrument.
-// kFix (FP64 holograms only): sum again only the pixels that the FP32
-// hologram kernel marked with a negative value in out (its error bound
-// exceeded HOLO_TOL) and overwrite them with the FP32-rounded FP64 value;
-// blocks without such a pixel return at once.
-template <typename R, bool kHologram, bool kFix = false>
+template <typename R, bool kHologram>
 __global__ void __launch_bounds__(256)
 k_field(const double* __restrict__ coords, long long npts,
         const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
@@ -387,12 +388,7 @@ k_field(const double* __restrict__ coords, long long npts,
   Quad<R>* coef = reinterpret_cast<Quad<R>*>(smem);
   const int item = blockIdx.y;
   const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = pix < npts;
-  if constexpr (kFix) {
-    static_assert(kHologram, "the FP64 fix-up pass is for holograms");
-    if (live) live = reinterpret_cast<const float*>(out)[(size_t)item * npts + pix] < 0.f;
-    if (!__syncthreads_or(live)) return;
-  }
+  const bool live = pix < npts;
   const bool cart = flags & LMB_CARTESIAN;
   const bool bohren = flags & LMB_BOHREN;
   double x = 0., y = 0., z = 0.;
@@ -424,10 +420,7 @@ k_field(const double* __restrict__ coords, long long npts,
     }
   }
   if (!live) return;
-  if constexpr (kFix) {
-    float* o = reinterpret_cast<float*>(out) + (size_t)item * npts;
-    o[pix] = float(intensity<R>(e));
-  } else if (kHologram) {
+  if (kHologram) {
     R* o = reinterpret_cast<R*>(out) + (size_t)item * npts;
     o[pix] = intensity<R>(e);
   } else {
@@ -442,28 +435,120 @@ k_field(const double* __restrict__ coords, long long npts,
   }
 }
 
+// FP64 re-summation, inside k_field_pair<true>, of the block's pixels whose
+// FP32 error bound exceeded HOLO_TOL (mark0/mark1: the thread's two
+// pixels).  One warp per marked pixel and one lane per particle, so that a
+// pixel's particles run their FP64 recurrences side by side; the particles
+// go in groups of `group` (<= 32), whose FP64 records (2 Quad<double> per
+// order, nmaxp orders per slot) are staged in smem after the marked-pixel
+// list and the FP64 field accumulators.  Lanes are combined by a fixed
+// shuffle tree and groups in order, so the result does not depend on
+// scheduling.  Every thread of the block calls this.
+__device__ void holo_resum64(bool mark0, long long q0, bool mark1, long long q1,
+                             long long base, char* smem, int group,
+                             const double* __restrict__ coords, long long npts,
+                             const lmb_sphere* __restrict__ spheres, int pb, int pe,
+                             const zd* __restrict__ ab, const int* __restrict__ nmax,
+                             int nmaxp, double k, int flags, double aberr, float* o) {
+  __shared__ int s_n;
+  if (threadIdx.x == 0) s_n = 0;
+  if (!__syncthreads_or(mark0 || mark1)) return;
+  int* list = reinterpret_cast<int*>(smem);                      // [2 * blockDim]
+  double* acc = reinterpret_cast<double*>(smem + RESUM_LIST_BYTES);  // [.][6]
+  Quad<double>* rec =
+      reinterpret_cast<Quad<double>*>(smem + RESUM_LIST_BYTES + RESUM_ACC_BYTES);
+  if (mark0) list[atomicAdd(&s_n, 1)] = int(q0 - base);
+  if (mark1) list[atomicAdd(&s_n, 1)] = int(q1 - base);
+  __syncthreads();
+  const int F = s_n;
+  for (int i = threadIdx.x; i < 6 * F; i += blockDim.x) acc[i] = 0.;
+  const bool cart = flags & LMB_CARTESIAN;
+  const bool bohren = flags & LMB_BOHREN;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  for (int g0 = pb; g0 < pe; g0 += group) {
+    const int G = min(group, pe - g0);
+    __syncthreads();  // the previous group's records are no longer read
+    for (int j = 0; j < G; ++j) {
+      const int nm = min(max(nmax[g0 + j], 0), nmaxp - 1);
+      stage_coef<double, false>(ab + size_t(g0 + j) * nmaxp * 2, (const zd*)0, nm,
+                                rec + size_t(j) * 2 * nmaxp);
+    }
+    __syncthreads();
+    for (int f = warp; f < F; f += nwarps) {
+      const long long pix = base + list[f];
+      cplx<double> e[3];
+      for (int c = 0; c < 3; ++c) e[c] = mk(0., 0.);
+      if (lane < G) {
+        const int p = g0 + lane;
+        const int nm = min(max(nmax[p], 0), nmaxp - 1);
+        const lmb_sphere sp = spheres[p];
+        const double x = coords[pix], y = coords[npts + pix], z = coords[2 * npts + pix];
+        const Geometry<double> g =
+            geometry<double>(k, x - sp.x_p, y - sp.y_p, z - sp.z_p, z, sp.z_p, bohren);
+        const Sums<double> sm = order_sum<double>(g, rec + size_t(lane) * 2 * nmaxp, nm);
+        epilogue<double>(g, sm, cart, e);
+        if (aberr != 0.) {
+          const cplx<double> ph = aberration_phase<double>(aberr, x - sp.x_p, y - sp.y_p, sp.z_p);
+          for (int c = 0; c < 3; ++c) e[c] = ph * e[c];
+        }
+      }
+      for (int o2 = 16; o2 > 0; o2 >>= 1)
+        for (int c = 0; c < 3; ++c) {
+          e[c].re += __shfl_xor_sync(0xffffffffu, e[c].re, o2);
+          e[c].im += __shfl_xor_sync(0xffffffffu, e[c].im, o2);
+        }
+      if (lane == 0)
+        for (int c = 0; c < 3; ++c) {
+          acc[6 * f + 2 * c] += e[c].re;
+          acc[6 * f + 2 * c + 1] += e[c].im;
+        }
+    }
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < F; f += blockDim.x) {
+    cplx<double> e[3];
+    for (int c = 0; c < 3; ++c) e[c] = mk(acc[6 * f + 2 * c], acc[6 * f + 2 * c + 1]);
+    o[base + list[f]] = float(intensity<double>(e));
+  }
+}
+
 // FP32 field / hologram with the packed two-pixel loop: each thread takes
 // two adjacent pixels (the last thread of an odd count pairs its pixel with
 // itself).  Same inputs and outputs as k_field<float, holo>; the order loop
-// runs in f32x2 (order_sum_pair) and the phase argument in FP64.  Holograms
-// also accumulate each pixel's error bound (holo_needs_fp64) and write -1 in
-// place of the pixels that need FP64, which k_field<double, true, true>
-// then sums again.
+// runs in f32x2 (order_sum_pair) and the phase in FP64 (phase_turns64).
+//
+// The particles of an item are summed in groups of up to 32 whose records
+// fit the block's shared memory (rec_quads float4): a group's records (and,
+// for holograms, the particles' amplitudes A_p, one warp per particle in a
+// fixed order) are staged by the whole block at once, so the block passes
+// one barrier pair per group rather than per particle.
+//
+// Holograms also accumulate each pixel's error bound (holo_needs_fp64); the
+// block then sums its pixels whose bound exceeds HOLO_TOL again in FP64
+// (holo_resum64, particles in groups of resum_group) and writes those.
 template <bool kHologram>
 __global__ void __launch_bounds__(256)
 k_field_pair(const double* __restrict__ coords, long long npts,
              const lmb_sphere* __restrict__ spheres, const int* __restrict__ item_start,
              const zd* __restrict__ ab, const int* __restrict__ nmax, int nmaxp,
-             double k, int flags, double aberr, void* out) {
+             double k, int flags, double aberr, void* out, int rec_quads,
+             int resum_group) {
   extern __shared__ __align__(16) char smem[];
   float4* rec = reinterpret_cast<float4*>(smem);
+  __shared__ int s_off[33];   // record offsets (float4) of the group's particles
+  __shared__ int s_nm[32];
+  __shared__ int s_count;     // particles in the group
+  __shared__ float s_amp[32];
   const int item = blockIdx.y;
-  const long long p0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+  const long long base = (long long)blockIdx.x * blockDim.x * 2;
+  const long long p0 = base + threadIdx.x * 2;
   const bool live0 = p0 < npts;
   const bool live1 = p0 + 1 < npts;
   const long long p1 = live1 ? p0 + 1 : p0;
   const bool cart = flags & LMB_CARTESIAN;
   const bool bohren = flags & LMB_BOHREN;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double x[2] = {0., 0.}, y[2] = {0., 0.}, z[2] = {0., 0.};
   if (live0) {
     x[0] = coords[p0];
@@ -477,53 +562,101 @@ k_field_pair(const double* __restrict__ coords, long long npts,
   for (int l = 0; l < 2; ++l)
     for (int c = 0; c < 3; ++c) e[l][c] = mk(0.f, 0.f);
   float m1[2] = {0.f, 0.f}, m0[2] = {0.f, 0.f};  // error bound (holograms)
-  __shared__ float s_amp;
   const int pb = item_start[item], pe = item_start[item + 1];
-  for (int p = pb; p < pe; ++p) {
-    const int nm = min(max(nmax[p], 0), nmaxp - 1);
-    const zd* abp = ab + size_t(p) * nmaxp * 2;
+  for (int g0 = pb; g0 < pe; g0 += s_count) {
+    __syncthreads();  // the previous group's records and s_count are read
+    if (warp == 0) {
+      // the group: the next particles (up to 32) whose records fit
+      const int p = g0 + lane;
+      const int nm = p < pe ? min(max(nmax[p], 0), nmaxp - 1) : 0;
+      int size = p < pe ? PAIRV_QUADS * (nm + 1) : 0;
+      for (int o = 1; o < 32; o <<= 1) {  // inclusive prefix sum
+        const int v = __shfl_up_sync(0xffffffffu, size, o);
+        if (lane >= o) size += v;
+      }
+      const unsigned fits = __ballot_sync(0xffffffffu, p < pe && size <= rec_quads);
+      const int G = max(1, __popc(fits));  // one particle always fits
+      s_nm[lane] = nm;
+      const int excl = __shfl_up_sync(0xffffffffu, size, 1);
+      const int last = __shfl_sync(0xffffffffu, size, G - 1);
+      if (lane < G) s_off[lane] = lane ? excl : 0;
+      if (lane == 0) {
+        s_count = G;
+        s_off[G] = last;
+      }
+    }
     __syncthreads();
-    stage_pair_value(abp, nm, rec);
-    if (kHologram && threadIdx.x < 32) {
-      double a = 0.;
-      for (int n = 1 + threadIdx.x; n <= nm; n += 32) a += order_amplitude(abp + 2 * n, n);
-      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-      if (threadIdx.x == 0) s_amp = float(a);
+    const int G = s_count;
+    {
+      // stage: three threads per order over all the group's orders
+      float2* r2 = reinterpret_cast<float2*>(rec);
+      const int total = 3 * (s_off[G] / PAIRV_QUADS);
+      int j = 0;
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        while (3 * (s_off[j + 1] / PAIRV_QUADS) <= t) ++j;
+        const int u = t - 3 * (s_off[j] / PAIRV_QUADS);
+        const int n = u / 3, part = u - 3 * n;
+        float v[PAIRV_VALUES];
+        pair_value_part(ab + size_t(g0 + j) * nmaxp * 2 + 2 * n, n, part, v);
+        const int lo = part == 0 ? 0 : (part == 1 ? 7 : 10);
+        const int hi = part == 0 ? 7 : (part == 1 ? 10 : PAIRV_VALUES);
+        float2* dst = r2 + 2 * s_off[j] + PAIRV_VALUES * n;
+        for (int q = lo; q < hi; ++q) dst[q] = make_float2(v[q], v[q]);
+      }
+      if (kHologram) {
+        for (int jj = warp; jj < G; jj += blockDim.x >> 5) {
+          const zd* abp = ab + size_t(g0 + jj) * nmaxp * 2;
+          float a = 0.f;
+          for (int n = 1 + lane; n <= s_nm[jj]; n += 32) a += order_amplitude(abp + 2 * n, n);
+          for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+          if (lane == 0) s_amp[jj] = a;
+        }
+      }
     }
     __syncthreads();
     if (live0) {
-      const lmb_sphere sp = spheres[p];
-      Geometry<float> g[2];
-      for (int l = 0; l < 2; ++l)
-        g[l] = geometry<float, true>(k, x[l] - sp.x_p, y[l] - sp.y_p, z[l] - sp.z_p,
-                                     z[l], sp.z_p, bohren);
-      PairSumsV S;
-      order_sum_pair(pair_in(g[0], g[1]), rec, nm, S);
+      for (int j = 0; j < G; ++j) {
+        const lmb_sphere sp = spheres[g0 + j];
+        Geometry<float> g[2];
+        for (int l = 0; l < 2; ++l)
+          g[l] = geometry<float, true>(k, x[l] - sp.x_p, y[l] - sp.y_p, z[l] - sp.z_p,
+                                       z[l], sp.z_p, bohren);
+        PairSumsV S;
+        order_sum_pair(pair_in(g[0], g[1]), rec + s_off[j], s_nm[j], S);
+        const float amp = kHologram ? s_amp[j] : 0.f;
 #pragma unroll
-      for (int l = 0; l < 2; ++l) {
-        const Sums<float> sl = pair_lane_value(S, l, g[l].smu);
-        cplx<float> ep[3];
-        epilogue<float>(g[l], sl, cart, ep);
-        if (aberr != 0.) {
-          const cplx<float> ph =
-              aberration_phase<float>(aberr, x[l] - sp.x_p, y[l] - sp.y_p, sp.z_p);
-          for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
+        for (int l = 0; l < 2; ++l) {
+          const Sums<float> sl = pair_lane_value(S, l, g[l].smu);
+          cplx<float> ep[3];
+          epilogue<float>(g[l], sl, cart, ep);
+          if (aberr != 0.) {
+            const cplx<float> ph =
+                aberration_phase<float>(aberr, x[l] - sp.x_p, y[l] - sp.y_p, sp.z_p);
+            for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
+          }
+          for (int c = 0; c < 3; ++c) e[l][c] = e[l][c] + ep[c];
+          if (kHologram) holo_bound_add(ep, amp, g[l].ikr, m1[l], m0[l]);
         }
-        for (int c = 0; c < 3; ++c) e[l][c] = e[l][c] + ep[c];
-        if (kHologram) holo_bound_add(ep, s_amp, g[l].ikr, m1[l], m0[l]);
       }
     }
   }
-  if (!live0) return;
-  for (int l = 0; l < 2; ++l) {
-    if (l == 1 && !live1) break;
-    const long long pix = l ? p1 : p0;
-    if (kHologram) {
-      float* o = reinterpret_cast<float*>(out) + (size_t)item * npts;
+  if constexpr (kHologram) {
+    float* o = reinterpret_cast<float*>(out) + (size_t)item * npts;
+    bool mark[2] = {false, false};
+    for (int l = 0; l < 2; ++l) {
+      if (!(l == 0 ? live0 : live1)) continue;
       const float h = intensity<float>(e[l]);
-      o[pix] = holo_needs_fp64(h, m1[l], m0[l]) ? -1.f : h;
-    } else {
-      float2* o = reinterpret_cast<float2*>(out) + (size_t)item * 3 * npts;
+      mark[l] = holo_needs_fp64(h, m1[l], m0[l]);
+      if (!mark[l]) o[l ? p1 : p0] = h;
+    }
+    holo_resum64(mark[0], p0, mark[1], p1, base, smem, resum_group, coords, npts,
+                 spheres, pb, pe, ab, nmax, nmaxp, k, flags, aberr, o);
+  } else {
+    if (!live0) return;
+    float2* o = reinterpret_cast<float2*>(out) + (size_t)item * 3 * npts;
+    for (int l = 0; l < 2; ++l) {
+      if (l == 1 && !live1) break;
+      const long long pix = l ? p1 : p0;
       for (int c = 0; c < 3; ++c) o[c * npts + pix] = make_float2(e[l][c].re, e[l][c].im);
     }
   }

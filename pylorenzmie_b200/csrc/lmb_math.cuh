@@ -163,6 +163,34 @@ LMB_HD f2 padd(f2 a, f2 b) {
 #endif
 }
 
+// Approximate FP32 reciprocal square root (a few ulp): the starting value
+// of the FP64 Newton-Raphson step of phase_turns64.
+LMB_HD float rsqrt_seed(float x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(x);
+#else
+  return 1.f / sqrtf(x);
+#endif
+}
+
+// sqrt(x) to a few ulp (x >= 0), for error estimates.
+LMB_HD float approx_sqrt(float x) {
+  return x > 1e-30f ? x * rsqrt_seed(x) : 0.f;
+}
+
+// e^{2 pi i t}
+LMB_HD cplx<float> cis_turns(float t) {
+  float s, c;
+#if defined(__CUDA_ARCH__)
+  sincospif(2.f * t, &s, &c);
+#else
+  const double a = 6.283185307179586 * double(t);
+  s = float(sin(a));
+  c = float(cos(a));
+#endif
+  return mk(c, s);
+}
+
 LMB_HD float lsqrt(float x) { return sqrtf(x); }
 LMB_HD double lsqrt(double x) { return sqrt(x); }
 LMB_HD float labs_(float x) { return fabsf(x); }

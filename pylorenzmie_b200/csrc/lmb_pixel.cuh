@@ -82,25 +82,36 @@ struct Geometry {
 //   z: the pixel's own z coordinate; zp: the particle's z
 LMB_HD double reduce_2pi(double t) { return remainder(t, 6.283185307179586); }
 
-// t reduced to about [-pi, pi] by Cody and Waite's additive reduction
-// (W. J. Cody, W. Waite, Software Manual for the Elementary Functions,
-// 1980) with 2 pi split into a double C1 and its remainder C2: with a fused
-// multiply-add, t - q C1 is exact for |q| < 2^20, so the result carries an
-// absolute error of about 1e-16 + q 1e-32.  For the phase arguments of the
-// field kernels (|t| up to ~10^4 rad); larger |t| take reduce_2pi.
-LMB_HD double reduce_2pi_cw(double t) {
-  const double C1 = 6.283185307179586;       // 2 pi rounded to double
-  const double C2 = 2.4492935982947064e-16;  // 2 pi - C1
-  if (!(fabs(t) < 1e6)) return reduce_2pi(t);
-  const double q = rint(t * 0.15915494309189535);
-  return fma(-q, C2, fma(-q, C1, t));
+// The phase sign(kz) k (r - |dzc|) - k z of a pixel, in turns (units of
+// 2 pi) and reduced to [-1/2, 1/2], in FP64: r = sqrt(rho^2 + dzc^2) from
+// an FP32 starting value of 1/sqrt refined by one Newton-Raphson step
+// (y <- y (3 - x y^2) / 2, which squares its relative error of ~2^-22 to
+// ~1e-13), then w = (k / 2 pi) (r - |dzc|) and w - rint(w).  The error is
+// ~1e-10 turns at the largest distances of a frame, against ~1e-5 for the
+// same argument in FP32.  Outside 1e-30 < r^2 < 1e30 (the FP32 range of
+// the starting value) r is the FP64 square root.
+LMB_HD double phase_turns64(double k, double dx, double dy, double dzc,
+                            double s, double z) {
+  const double kt = k * 0.15915494309189535;  // k / (2 pi)
+  const double r2 = fma(dzc, dzc, fma(dx, dx, dy * dy));
+  double r;
+  if (r2 > 1e-30 && r2 < 1e30) {
+    const double y = rsqrt_seed(float(r2));
+    const double t = r2 * y;
+    r = t * fma(-0.5 * t, y, 1.5);
+  } else {
+    r = sqrt(r2);
+  }
+  double w = s * fma(kt, r, -kt * fabs(dzc));
+  if (z != 0.) w = fma(-kt, z, w);
+  return w - rint(w);
 }
 
-// kPhase64: form the phase argument sign(kz) (kr - |kz|) - k z in FP64 from
-// the FP64 offsets (R = float only).  Far from the particle (kr ~ 10^3 rad)
-// the FP32 argument, and even the FP32 roundings of kx, ky and kz that it
-// is formed from, are off by ~1e-4 rad; in FP64 the phase is exact to FP32
-// rounding.  The fits' crops (kr ~ 10^2) do not need it.
+// kPhase64: form the phase sign(kz) (kr - |kz|) - k z in FP64 from the FP64
+// offsets (phase_turns64; R = float only).  Far from the particle (kr ~
+// 10^3 rad) the FP32 argument, and even the FP32 roundings of kx, ky and kz
+// that it is formed from, are off by ~1e-4 rad; in FP64 the phase is exact
+// to FP32 rounding.  The fits' crops (kr ~ 10^2) do not need it.
 template <typename R, bool kPhase64 = false>
 LMB_HD Geometry<R> geometry(double k, double dx, double dy, double dzc,
                             double z, double zp, bool bohren) {
@@ -136,12 +147,9 @@ LMB_HD Geometry<R> geometry(double k, double dx, double dy, double dzc,
     g.h0 = mk(R(0), -sigma);
     if (sigma == s) {
       // sign(kz) (kr - |kz|) - k z, with kr - |kz| = krho^2/(kr + |kz|)
-      if (kPhase64) {
-        const double rho2 = dx * dx + dy * dy;
-        const double r = sqrt(rho2 + dzc * dzc);
-        double arg = double(s) * k * rho2 / (r + fabs(dzc));
-        if (z != 0.) arg -= k * z;
-        g.phase = cis(R(reduce_2pi_cw(arg)));
+      if constexpr (kPhase64) {
+        static_assert(sizeof(R) == sizeof(float), "FP32 geometry only");
+        g.phase = cis_turns(float(phase_turns64(k, dx, dy, dzc, double(s), z)));
       } else {
         R arg = s * krho2 / (kr + labs_(kz));
         if (z != 0.) arg += R(reduce_2pi(-k * z));
@@ -888,16 +896,19 @@ LMB_HD R intensity(const cplx<R>* e) {
 #define HOLO_FIELD_FLOOR 1e-7f
 #define HOLO_TOL 2e-5f
 
-// (n + 1/2)(|a_n| + |b_n|): order n's share of A_p.
-LMB_HD double order_amplitude(const cplx<double>* ab, int n) {
-  return (double(n) + 0.5) * (sqrt(norm2(ab[0])) + sqrt(norm2(ab[1])));
+// (n + 1/2)(|a_n| + |b_n|): order n's share of A_p (FP32: the bound needs
+// no more).
+LMB_HD float order_amplitude(const cplx<double>* ab, int n) {
+  const float a2 = norm2(mk(float(ab[0].re), float(ab[0].im)));
+  const float b2 = norm2(mk(float(ab[1].re), float(ab[1].im)));
+  return (float(n) + 0.5f) * (approx_sqrt(a2) + approx_sqrt(b2));
 }
 
 // Per-pixel accumulation of the bound over the particles: m1 += |E_p|,
 // m0 += A_p / kr.
 LMB_HD void holo_bound_add(const cplx<float>* ep, float amp, float ikr,
                            float& m1, float& m0) {
-  m1 += sqrtf(norm2(ep[0]) + norm2(ep[1]) + norm2(ep[2]));
+  m1 += approx_sqrt(norm2(ep[0]) + norm2(ep[1]) + norm2(ep[2]));
   m0 += amp * ikr;
 }
 

@@ -247,7 +247,7 @@ API void h_hologram_pair(const double* coords, long long npts, const double* p,
   for (int j = 0; j < np; ++j) {
     const double* abj = ab + size_t(j) * (cap + 1) * 4;
     q[j].resize(PAIRV_QUADS * (nmax[j] + 1));
-    double a = 0.;
+    float a = 0.f;
     for (int n = 0; n <= nmax[j]; ++n) {
       zd c[2];
       for (int i = 0; i < 2; ++i) c[i] = mk(abj[4 * n + 2 * i], abj[4 * n + 2 * i + 1]);
@@ -257,7 +257,7 @@ API void h_hologram_pair(const double* coords, long long npts, const double* p,
         q[j][PAIRV_QUADS * n + i] = Quad<float>{v[2 * i], v[2 * i], v[2 * i + 1], v[2 * i + 1]};
       if (n > 0) a += order_amplitude(c, n);
     }
-    amp[j] = float(a);
+    amp[j] = a;
   }
   for (long long i = 0; i < npts; i += 2) {
     const long long i1 = i + 1 < npts ? i + 1 : i;
