@@ -376,6 +376,16 @@ def b200_arm(args):
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
         extras = run_extras(dev, inst, value)
+    ns = north_star(value, extras)
+
+    # the FP32 peak from the clock: SMs x 128 FP32 lanes x 2 FLOP x MHz
+    csum = clocks.summary()
+    if csum.get('sm_mhz'):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        clk_peak = sms * 128 * 2 * csum['sm_mhz'] * 1e6 / 1e12
+        roofline['peak_clock_derived'] = clk_peak
+        roofline['frac_clock_derived'] = achieved / clk_peak
+        roofline['sm_mhz_median'] = csum['sm_mhz']
 
     if world > 1:
         tdist.destroy_process_group()
@@ -400,7 +410,8 @@ def b200_arm(args):
         'cpu_baseline': cpu_base,
         'e2e': e2e,
         'gpu_launches': gpu_launches,
-        'clocks': clocks.summary(),
+        'clocks': csum,
+        'north_star': ns,
         'extras': extras,
     }
     print(json.dumps(line), flush=True)
@@ -716,6 +727,31 @@ def run_extras(dev, inst, chosen_value):
         'vs_oracle_fit': compare_fits(df.iloc[sub].reset_index(drop=True),
                                       ref)}
     return out
+
+
+def north_star(chosen, extras):
+    '''The target figures of the hot path, beside their targets: the
+    chosen form against plain FP64 on the same GPU, the FP32 frame
+    hologram's error against FP64, and the fits against the oracle's.'''
+    ns = {'chosen_features_per_s': chosen,
+          'targets': {'chosen_over_plain': 50., 'hologram_abs_error': 2e-5,
+                      'a_p_um': 1e-3, 'n_p': 1e-4, 'z_p_px': 0.02}}
+    if not extras:
+        return ns
+    plain = extras.get('plain_fp64_gpu', {})
+    ns['plain_fp64_gpu_features_per_s'] = plain.get('value')
+    ns['chosen_over_plain'] = plain.get('chosen_over_plain')
+    frame = extras.get('frame_fp32', {})
+    ns['frame_fp32_mpx_per_s'] = frame.get('value')
+    ns['frame_fp32_max_abs_error_vs_fp64'] = frame.get(
+        'max_abs_error_vs_fp64')
+    for key in ('mixed_crops_e2e', 'layered_stream_e2e'):
+        cmp = extras.get(key, {}).get('vs_oracle_fit')
+        if cmp:
+            ns[key + '_vs_oracle_fit_max_abs'] = {
+                k: cmp[k]['max_abs'] for k in ('x_p', 'y_p', 'z_p', 'a_p',
+                                                'n_p')}
+    return ns
 
 
 def oracle_fits(tasks):

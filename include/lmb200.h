@@ -377,6 +377,10 @@ size_t lmb_fit_workspace_bytes(int nfeatures, long long total_pixels,
  * read them in stream order (a copy on the same stream, or after
  * cudaStreamSynchronize).  With stats the call waits for that kernel too.
  * Features whose pixels fall outside [0, total_pixels) end with status -1.
+ * Host resources: a calling thread's first fit on a device makes a ring of
+ * 32 pinned 64-byte slots with an event each (plus timing events with
+ * stats); they are kept for that thread's later fits and released when
+ * the thread exits.
  */
 int lmb_fit_batch(const lmb_feature *features, int nfeatures,
                   long long total_pixels, const float *data,
@@ -547,15 +551,19 @@ int lmb_fit_batch_streamed(const lmb_feature *features, int nfeatures,
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  Requests whose lmb_fit_workspace_bytes
- * exceed LMB_FIT_NOALLOC_SCRATCH_BYTES are rejected with
- * LMB_ERR_WORKSPACE before anything is launched (about 500 features of
- * 201x201 pixels fit at the capacity a 0.75 um sphere needs).  All calls share the one array, which keeps the
- * last call's contents; the fit re-initializes every counter, state and
- * table it reads, and the counters are zeroed again at each call.  Calls
- * from this process are serialized by a lock, but calls whose work could
- * overlap on the GPU (for example from another thread that bypasses this
- * entry point's return) would race on the array.
+ * before any stream capture.  The fit runs the synchronous round loop: it
+ * reads the round counters back and waits for the stream every round, and
+ * returns only when the stream has drained, errors included.  Requests
+ * whose lmb_fit_workspace_bytes exceed LMB_FIT_NOALLOC_SCRATCH_BYTES are
+ * rejected with LMB_ERR_WORKSPACE before anything is launched; check
+ * lmb_fit_workspace_bytes(n, pixels, nmax_cap) against it.  For 201x201
+ * crops that is at most 568 features at nmax_cap 26, 487 at 40 and 404 at
+ * 60.  All calls share the one array, which keeps the last call's contents;
+ * the fit re-initializes every counter, state and table it reads, and the
+ * counters are zeroed again at each call.  Calls from this process are
+ * serialized by a lock, but calls whose work could overlap on the GPU (for
+ * example from another thread that bypasses this entry point's return)
+ * would race on the array.
  */
 #define LMB_FIT_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 int lmb_fit_batch_noalloc(const lmb_feature *features, int nfeatures,

@@ -570,7 +570,11 @@ def _stream_worker(n):
     global _STREAM_WORKER
     if _STREAM_WORKER is None or _STREAM_WORKER._max_workers < n:
         from concurrent.futures import ThreadPoolExecutor
+        old = _STREAM_WORKER
         _STREAM_WORKER = ThreadPoolExecutor(max_workers=n)
+        if old is not None:
+            # its threads end once the fits already given to them return
+            old.shutdown(wait=False)
     return _STREAM_WORKER
 
 

@@ -592,7 +592,9 @@ namespace {
 // Host-side resources of the pipelined round loop, one set per host thread
 // and device: a ring of pinned slots, each taking a copy of the fit's
 // counters (8 ints) and work totals (2 x 64 bit) after a round, and an
-// event per slot.  Made on first use and kept until the process exits.
+// event per slot (32 slots of 64 bytes and 32 events), plus the timing
+// events of the fits that ask for stats.  Made on a thread's first fit on
+// a device and released when that thread exits.
 constexpr int kRingSlots = 32;
 constexpr int kSlotInts = 16;
 constexpr size_t kSlotCopyBytes = 8 * sizeof(int) + 2 * sizeof(unsigned long long);
@@ -600,13 +602,29 @@ constexpr int kRingDevices = 64;
 struct RoundRing {
   int* slots = nullptr;
   cudaEvent_t done[kRingSlots] = {};
+  ~RoundRing() {
+    if (!slots) return;
+    // a fit may return with copies into its last slots still queued
+    for (int i = 0; i < kRingSlots; ++i) {
+      cudaEventSynchronize(done[i]);
+      cudaEventDestroy(done[i]);
+    }
+    cudaFreeHost(slots);
+  }
+};
+
+struct EventPool {
+  std::vector<cudaEvent_t> events;
+  ~EventPool() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+  }
 };
 
 std::vector<cudaEvent_t>* timing_pool() {
-  static thread_local std::vector<cudaEvent_t> pools[kRingDevices];
+  static thread_local EventPool pools[kRingDevices];
   const int dev = current_device();
   if (dev < 0 || dev >= kRingDevices) return nullptr;
-  return &pools[dev];
+  return &pools[dev].events;
 }
 
 RoundRing* round_ring() {
@@ -1111,9 +1129,14 @@ extern "C" int lmb_fit_batch_noalloc(const lmb_feature* features, int nfeatures,
   LMB_CK(cudaMemsetAsync(reinterpret_cast<char*>(scratch) + L.counters, 0,
                          sizeof(int) * 16, as_stream(stream)));
   // the synchronous round loop: the pipelined one pins host memory
-  return fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
-                        n_m, wavelength, magnification, noise, nmax_cap,
-                        settings, results, scratch,
-                        size_t(LMB_FIT_NOALLOC_SCRATCH_BYTES), nullptr, stream,
-                        1, nullptr, nullptr, nullptr, 0., true);
+  const int status =
+      fit_batch_impl(features, nfeatures, total_pixels, data, coords, params,
+                     n_m, wavelength, magnification, noise, nmax_cap, settings,
+                     results, scratch, size_t(LMB_FIT_NOALLOC_SCRATCH_BYTES),
+                     nullptr, stream, 1, nullptr, nullptr, nullptr, 0., true);
+  // An error can leave kernels that write the array queued; wait for them
+  // before the lock lets the next call in (this allocates nothing).
+  const cudaError_t drained = cudaStreamSynchronize(as_stream(stream));
+  if (status == LMB_OK && drained != cudaSuccess) return LMB_ERR_CUDA;
+  return status;
 }
