@@ -26,12 +26,14 @@ def fit_201(data, start):
                DEFAULT_INSTRUMENT)
 
 
-def fit_crop(data, shape, start, fractions=None, core_indices=None):
+def fit_crop(data, shape, start, fractions=None, core_indices=None,
+             settings=None):
     '''The reference fitting algorithm on one crop of any shape; a layered
-    sphere keeps its inner radius fractions and indices.'''
+    sphere keeps its inner radius fractions and indices.  settings: scipy
+    least_squares settings (None: the Optimizer's defaults).'''
     particle = dict(zip(KEYS, start))
     if fractions is not None:
         particle['fractions'] = list(fractions)
         particle['core_indices'] = list(core_indices)
     return fit(np.asarray(data).ravel(), meshgrid(tuple(shape)), particle,
-               DEFAULT_INSTRUMENT)
+               DEFAULT_INSTRUMENT, settings=settings)

@@ -108,3 +108,49 @@ def test_large_sphere_jacobian_vs_finite_differences(p):
               ofield.hologram(c, [dict(zip(KEYS, pm))], inst)) / (2 * step)
         err = np.abs(J[j] - fd).max() / np.abs(fd).max()
         assert err < 3e-4, (KEYS[j], err)
+
+
+def config4_spheres(n, side, seed):
+    '''Spheres of the differentiation workload's distribution: a_p
+    U(3, 6) um, n_p U(1.4, 2.0), z_p U(200, 600) px (at least 10 px above
+    the sphere's top), centred +-2 px on a side x side crop.'''
+    rng = np.random.default_rng(seed)
+    c = (side - 1) / 2.
+    out = []
+    for _ in range(n):
+        a = rng.uniform(3., 6.)
+        out.append([c + rng.uniform(-2, 2), c + rng.uniform(-2, 2),
+                    max(rng.uniform(200., 600.), a / 0.048 + 10.), a,
+                    rng.uniform(1.4, 2.0), 0.])
+    return out
+
+
+@pytest.mark.parametrize('shape,p', [((201, 201), q) for q in
+                                     config4_spheres(3, 201, 41)] +
+                         [((401, 401), config4_spheres(1, 401, 42)[0])])
+def test_chi2_gradient_vs_torch_fp64_autograd_large(shape, p):
+    '''The chi^2 gradient at the differentiation workload's sizes (n_max
+    90-190): as test_chi2_gradient_vs_torch_fp64_autograd.'''
+    test_chi2_gradient_vs_torch_fp64_autograd(shape, p)
+
+
+def test_jacobian_vs_torch_fp64_forward_mode_large():
+    '''All six Jacobian columns of a 401x401 crop of a large sphere against
+    forward-mode derivatives (torch.func.jvp) of the FP64 torch
+    restatement, within 5e-5 of each column's maximum.'''
+    from pylorenzmie_b200.theory import autograd as ag
+    p = config4_spheres(1, 401, 43)[0]
+    c = ofield.meshgrid((401, 401))
+    _, J = ag.jacobian(torch.tensor(p, dtype=torch.float64, device='cuda'),
+                       c)
+    J = J[0].cpu().numpy()
+    p0 = torch.tensor(p, dtype=torch.float64)
+    errs = []
+    for j in range(6):
+        e = torch.zeros(6, dtype=torch.float64)
+        e[j] = 1.
+        _, col = torch.func.jvp(lambda q: torch_model.hologram(q, c), (p0,),
+                                (e,))
+        col = col.numpy()
+        errs.append(np.abs(J[j] - col).max() / np.abs(col).max())
+    assert max(errs) < 5e-5, dict(zip(KEYS, errs))
