@@ -29,14 +29,21 @@ from . import _kernels as K
 JAC_KEYS = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p', 'k_p')
 
 
-def _records(particles):
-    '''SPHERE_DTYPE records (r_p + r_0, a_p, n_p, k_p) of a particle list.'''
-    rec = np.zeros(len(particles), dtype=K.SPHERE_DTYPE)
-    for i, p in enumerate(particles):
+def _row(p):
+    # plain attribute reads where the particle has them (r_p and r_0
+    # build arrays)
+    try:
+        r = (p.x_p + p.x_0, p.y_p + p.y_0, p.z_p + p.z_0)
+    except AttributeError:
         r = np.asarray(p.r_p, dtype=float) + np.asarray(
             getattr(p, 'r_0', (0., 0., 0.)), dtype=float)
-        rec[i] = (r[0], r[1], r[2], p.a_p, p.n_p, getattr(p, 'k_p', 0.))
-    return rec
+    return (float(r[0]), float(r[1]), float(r[2]), float(p.a_p),
+            float(p.n_p), float(getattr(p, 'k_p', 0.)))
+
+
+def _records(particles):
+    '''SPHERE_DTYPE records (r_p + r_0, a_p, n_p, k_p) of a particle list.'''
+    return np.array([_row(p) for p in particles], dtype=K.SPHERE_DTYPE)
 
 
 class LorenzMie(LMObject):
@@ -191,7 +198,7 @@ class LorenzMie(LMObject):
         f = self._field_items([list(self.particle)], cartesian, bohren)[0]
         if device:
             return f
-        return f.to(torch.complex128).cpu().numpy()
+        return K.to_numpy(f, torch.complex128)
 
     def scattered_field(self, particle, cartesian=True, bohren=True,
                         device=False):
@@ -199,14 +206,14 @@ class LorenzMie(LMObject):
         f = self._field_items([[particle]], cartesian, bohren)[0]
         if device:
             return f
-        return f.to(torch.complex128).cpu().numpy()
+        return K.to_numpy(f, torch.complex128)
 
     def hologram(self, cartesian=True, bohren=True, device=False):
         '''Hologram |E + x|^2, numpy float64 (npts,) unless device=True.'''
         h = self._hologram_items([list(self.particle)], cartesian, bohren)[0]
         if device:
             return h
-        return h.to(torch.float64).cpu().numpy()
+        return K.to_numpy(h, torch.float64)
 
     def batch_field(self, particle_lists, cartesian=True, bohren=True):
         '''(B, 3, npts) complex tensor, one particle list per item.'''
@@ -231,7 +238,7 @@ class LorenzMie(LMObject):
                                      cartesian, bohren)
         if device:
             return h
-        return h.to(torch.float64).cpu().numpy()
+        return K.to_numpy(h, torch.float64)
 
     # ------------------------------------------------------------------
     def jac(self, device=False):
@@ -249,7 +256,7 @@ class LorenzMie(LMObject):
         J = J[0]
         if device:
             return {k: J[i] for i, k in enumerate(JAC_KEYS)}
-        J = J.cpu().numpy()
+        J = K.to_numpy(J, torch.float64)
         return {k: J[i] for i, k in enumerate(JAC_KEYS)}
 
     def hologram_and_jac(self, bohren=True):
