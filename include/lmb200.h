@@ -500,6 +500,21 @@ int lmb_de_draws_many(int nsearch, void *const *bitgens, const int *masked,
                       long long *fill, unsigned char *cross);
 
 /*
+ * The random pixel subset that Mask draws for a fit (analysis/Mask.py:64-72,
+ * 82-105: np.random.rand(*shape) < fraction, excluded pixels removed), on
+ * the global RandomState's own bit generator (BitGenerator.ctypes
+ * .bit_generator): one next_double per pixel in pixel order, as
+ * RandomState.random_sample draws them, so the generator ends where numpy
+ * leaves it and the subset is numpy's.  Pixel i is kept when its draw is
+ * below fraction and exclude[i] (exclude may be NULL) is zero; index
+ * (room for n) receives the kept pixels in increasing order, *count their
+ * number.  Host only; the caller holds the generator's lock.
+ */
+int lmb_mask_select(void *bitgen, long long n, double fraction,
+                    const unsigned char *exclude, long long *index,
+                    long long *count);
+
+/*
  * lmb_fit_batch (any layer count) that starts before all of its pixel data
  * is on the device.  No counterpart in the reference, whose fits run one
  * feature at a time on the host.

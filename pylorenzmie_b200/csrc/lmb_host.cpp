@@ -316,3 +316,24 @@ extern "C" int lmb_de_draws_many(int nsearch, void* const* bitgens,
   }
   return LMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// The random pixel subset of Mask (analysis/Mask.py:64-72, 82-105) on
+// numpy's own bit generator: one uniform per pixel from next_double, in
+// pixel order -- the draws of RandomState.random_sample, which
+// np.random.rand(*shape) makes -- and pixel i kept when its draw is below
+// fraction and exclude[i] (when given) is zero.  index receives the kept
+// pixels in increasing order (room for n), *count their number.
+extern "C" int lmb_mask_select(void* bitgen, long long n, double fraction,
+                               const unsigned char* exclude, long long* index,
+                               long long* count) {
+  if (!bitgen || n < 0 || !index || !count) return LMB_ERR_ARG;
+  NpBitgen* g = static_cast<NpBitgen*>(bitgen);
+  long long k = 0;
+  for (long long i = 0; i < n; ++i) {
+    const bool keep = g->next_double(g->state) < fraction;
+    if (keep && !(exclude && exclude[i])) index[k++] = i;
+  }
+  *count = k;
+  return LMB_OK;
+}

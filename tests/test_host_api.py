@@ -124,6 +124,42 @@ def test_mask():
     assert Mask().properties == {'fraction': 0.1}
 
 
+@pytest.mark.parametrize('shape,fraction', [((121, 121), 0.1),
+                                            ((37, 53), 0.5), ((1, 1), 0.3),
+                                            ((0, 5), 0.1), ((64, 64), 1.)])
+@pytest.mark.parametrize('excluded', [False, True])
+def test_mask_draws_are_numpys(shape, fraction, excluded):
+    '''The subset drawn by the library on the global generator is
+    np.random.rand(*shape) < fraction with the excluded pixels removed,
+    and the generator ends where numpy's own draws leave it.'''
+    from pylorenzmie_b200.analysis import Mask, Hologram
+    exclude = None
+    if excluded:
+        exclude = np.random.default_rng(1).random(shape) < 0.3
+    np.random.seed(7)
+    state = np.random.get_state()
+    m = Mask(fraction=fraction, exclude=exclude)
+    m.shape = shape
+    after = np.random.rand(3)
+    np.random.set_state(state)
+    ref = np.random.rand(*shape) < fraction
+    if exclude is not None:
+        ref[exclude] = False
+    assert np.array_equal(m(), ref)
+    assert np.array_equal(np.random.rand(3), after)
+    if 0 not in shape:
+        h = Hologram(np.random.default_rng(2).random(shape),
+                     corner=(3., 5.))
+        np.random.set_state(state)
+        data, coords = m.apply(h)
+        np.random.set_state(state)
+        want = np.random.rand(*shape) < fraction
+        if exclude is not None:
+            want[exclude] = False
+        assert np.array_equal(data, h.data[want])
+        assert np.array_equal(coords, h.coordinates[:, want])
+
+
 def test_optimizer_configuration():
     opt = Optimizer(model=LorenzMie())
     assert opt.result is None and opt.mask is None
