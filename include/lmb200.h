@@ -503,16 +503,20 @@ int lmb_de_draws_many(int nsearch, void *const *bitgens, const int *masked,
  * The random pixel subset that Mask draws for a fit (analysis/Mask.py:64-72,
  * 82-105: np.random.rand(*shape) < fraction, excluded pixels removed), on
  * the global RandomState's own bit generator (BitGenerator.ctypes
- * .bit_generator): one next_double per pixel in pixel order, as
+ * .bit_generator): one uniform per pixel in pixel order, as
  * RandomState.random_sample draws them, so the generator ends where numpy
  * leaves it and the subset is numpy's.  Pixel i is kept when its draw is
  * below fraction and exclude[i] (exclude may be NULL) is zero; index
  * (room for n) receives the kept pixels in increasing order, *count their
- * number.  Host only; the caller holds the generator's lock.
+ * number.  layout 0 draws through the generator's next_double; layout 1
+ * advances numpy's MT19937 state (624 words and a position) itself, a
+ * block at a time -- for an MT19937 only, after checking that both
+ * layouts give the same subsets and states.  Host only; the caller holds
+ * the generator's lock.
  */
 int lmb_mask_select(void *bitgen, long long n, double fraction,
-                    const unsigned char *exclude, long long *index,
-                    long long *count);
+                    const unsigned char *exclude, int layout,
+                    long long *index, long long *count);
 
 /*
  * lmb_fit_batch (any layer count) that starts before all of its pixel data

@@ -123,7 +123,7 @@ _SIGNATURES = {
     'lmb_de_shuffles': (_i, [_vp, _vp, _ll, _ll, _i, _vp]),
     'lmb_de_draws': (_i, [_vp, _i, _i, _d, _d, _vp, _vp, _ll, _i, _vp, _i,
                           _d, _vp, _vp]),
-    'lmb_mask_select': (_i, [_vp, _ll, _d, _vp, _vp, _vp]),
+    'lmb_mask_select': (_i, [_vp, _ll, _d, _vp, _i, _vp, _vp]),
     'lmb_de_draws_many': (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ll,
                                _i, _vp, _i, _vp, _vp, _vp]),
 }

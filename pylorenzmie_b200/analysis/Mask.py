@@ -8,6 +8,36 @@ from .. import _native
 from ..lib import LMObject
 
 
+_MT_BLOCKS = None
+
+
+def _mt_blocks_ok():
+    '''Whether lmb_mask_select's MT19937 layout (the generator's words
+    advanced by the library) reproduces its next_double layout on this
+    numpy: the same subsets and the same final state over draws that
+    straddle several blocks, checked once on scratch generators.'''
+    global _MT_BLOCKS
+    if _MT_BLOCKS is None:
+        ok = True
+        g = [np.random.MT19937(2024), np.random.MT19937(2024)]
+        for n, frac in ((1, 0.5), (311, 0.1), (1247, 0.7), (5000, 0.3)):
+            out = []
+            for layout, bg in enumerate(g):
+                idx = np.empty(n, dtype=np.int64)
+                cnt = ctypes.c_longlong()
+                st = _native.load().lmb_mask_select(
+                    bg.ctypes.bit_generator.value, n, frac, None, layout,
+                    idx.ctypes.data, ctypes.byref(cnt))
+                ok = ok and st == _native.LMB_OK
+                out.append(idx[:cnt.value])
+            ok = ok and np.array_equal(out[0], out[1])
+        s0, s1 = (bg.state['state'] for bg in g)
+        ok = (ok and np.array_equal(s0['key'], s1['key'])
+              and s0['pos'] == s1['pos'])
+        _MT_BLOCKS = bool(ok)
+    return _MT_BLOCKS
+
+
 @dataclass
 class Mask(LMObject):
     shape: tuple | None = None
@@ -45,10 +75,11 @@ class Mask(LMObject):
         index = np.empty(n, dtype=np.int64)
         count = ctypes.c_longlong()
         bg = np.random.mtrand._rand._bit_generator
+        layout = int(isinstance(bg, np.random.MT19937) and _mt_blocks_ok())
         with bg.lock:
             st = _native.load().lmb_mask_select(
                 bg.ctypes.bit_generator.value, n, float(self.fraction),
-                None if exclude is None else exclude.ctypes.data,
+                None if exclude is None else exclude.ctypes.data, layout,
                 index.ctypes.data, ctypes.byref(count))
         _native.check(st, 'lmb_mask_select')
         self._index = index[:count.value]

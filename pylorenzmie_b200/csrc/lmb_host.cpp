@@ -319,20 +319,99 @@ extern "C" int lmb_de_draws_many(int nsearch, void* const* bitgens,
 
 // ---------------------------------------------------------------------------
 // The random pixel subset of Mask (analysis/Mask.py:64-72, 82-105) on
-// numpy's own bit generator: one uniform per pixel from next_double, in
-// pixel order -- the draws of RandomState.random_sample, which
-// np.random.rand(*shape) makes -- and pixel i kept when its draw is below
-// fraction and exclude[i] (when given) is zero.  index receives the kept
-// pixels in increasing order (room for n), *count their number.
+// numpy's own bit generator: one uniform per pixel, in pixel order -- the
+// draws of RandomState.random_sample, which np.random.rand(*shape) makes
+// -- and pixel i kept when its draw is below fraction and exclude[i] (when
+// given) is zero.  index receives the kept pixels in increasing order
+// (room for n), *count their number.
+//
+// layout 0 draws through the generator's next_double.  layout 1 is for
+// numpy's MT19937 state (624 32-bit words and a position), which it
+// advances itself: the Mersenne Twister of M. Matsumoto and T. Nishimura
+// (ACM TOMACS 8, 3 (1998)) -- a block of 624 words regenerated when used
+// up, each word tempered on output -- with a double made of two words,
+// (a >> 5) 2^26 + (b >> 6) over 2^53, as numpy's next_double makes it.
+// Tempering a block's words in one loop costs a fraction of a function
+// call per word; the caller checks once that both layouts agree.
+namespace {
+
+constexpr int kMtN = 624, kMtM = 397;
+
+struct MtState {
+  uint32_t key[kMtN];
+  int pos;
+};
+
+void mt_regenerate(MtState* s) {
+  const uint32_t upper = 0x80000000u, lower = 0x7fffffffu, a = 0x9908b0dfu;
+  int i = 0;
+  for (; i < kMtN - kMtM; ++i) {
+    const uint32_t y = (s->key[i] & upper) | (s->key[i + 1] & lower);
+    s->key[i] = s->key[i + kMtM] ^ (y >> 1) ^ ((0u - (y & 1u)) & a);
+  }
+  for (; i < kMtN - 1; ++i) {
+    const uint32_t y = (s->key[i] & upper) | (s->key[i + 1] & lower);
+    s->key[i] = s->key[i + kMtM - kMtN] ^ (y >> 1) ^ ((0u - (y & 1u)) & a);
+  }
+  const uint32_t y = (s->key[kMtN - 1] & upper) | (s->key[0] & lower);
+  s->key[kMtN - 1] = s->key[kMtM - 1] ^ (y >> 1) ^ ((0u - (y & 1u)) & a);
+  s->pos = 0;
+}
+
+inline uint32_t mt_temper(uint32_t y) {
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+inline double mt_double(uint32_t a, uint32_t b) {
+  return (double(a >> 5) * 67108864.0 + double(b >> 6)) / 9007199254740992.0;
+}
+
+inline uint32_t mt_word(MtState* s) {
+  if (s->pos >= kMtN) mt_regenerate(s);
+  return mt_temper(s->key[s->pos++]);
+}
+
+}  // namespace
+
 extern "C" int lmb_mask_select(void* bitgen, long long n, double fraction,
-                               const unsigned char* exclude, long long* index,
-                               long long* count) {
-  if (!bitgen || n < 0 || !index || !count) return LMB_ERR_ARG;
+                               const unsigned char* exclude, int layout,
+                               long long* index, long long* count) {
+  if (!bitgen || n < 0 || !index || !count || layout < 0 || layout > 1)
+    return LMB_ERR_ARG;
   NpBitgen* g = static_cast<NpBitgen*>(bitgen);
   long long k = 0;
-  for (long long i = 0; i < n; ++i) {
-    const bool keep = g->next_double(g->state) < fraction;
-    if (keep && !(exclude && exclude[i])) index[k++] = i;
+  if (layout == 0) {
+    for (long long i = 0; i < n; ++i) {
+      const bool keep = g->next_double(g->state) < fraction;
+      if (keep && !(exclude && exclude[i])) index[k++] = i;
+    }
+    *count = k;
+    return LMB_OK;
+  }
+  MtState* s = static_cast<MtState*>(g->state);
+  if (s->pos < 0 || s->pos > kMtN) return LMB_ERR_ARG;
+  long long i = 0;
+  while (i < n) {
+    if (s->pos >= kMtN) mt_regenerate(s);
+    const long long pairs = std::min<long long>((kMtN - s->pos) / 2, n - i);
+    if (pairs == 0) {  // one word left in the block: the draw straddles it
+      const uint32_t a = mt_word(s);
+      const uint32_t b = mt_word(s);
+      if (mt_double(a, b) < fraction && !(exclude && exclude[i])) index[k++] = i;
+      ++i;
+      continue;
+    }
+    const uint32_t* w = s->key + s->pos;
+    for (long long j = 0; j < pairs; ++j) {
+      const double u = mt_double(mt_temper(w[2 * j]), mt_temper(w[2 * j + 1]));
+      if (u < fraction && !(exclude && exclude[i + j])) index[k++] = i + j;
+    }
+    s->pos += int(2 * pairs);
+    i += pairs;
   }
   *count = k;
   return LMB_OK;

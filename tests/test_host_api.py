@@ -160,6 +160,31 @@ def test_mask_draws_are_numpys(shape, fraction, excluded):
         assert np.array_equal(coords, h.coordinates[:, want])
 
 
+def test_mask_mt19937_layouts_agree():
+    '''lmb_mask_select's two layouts -- through next_double, and numpy's
+    MT19937 words advanced a block at a time -- give the same subsets and
+    leave the generator in the same state, for draws that straddle blocks
+    (a double takes two of a block's 624 words).'''
+    import ctypes
+    import pylorenzmie_b200.analysis.Mask as mask_module
+    assert mask_module._mt_blocks_ok()
+    lib = _native.load()
+    g = [np.random.MT19937(99), np.random.MT19937(99)]
+    for n, frac in [(0, 0.1), (1, 0.9), (311, 0.1), (312, 0.5), (313, 0.5),
+                    (14641, 0.1), (7, 1.0), (5, 0.0)]:
+        out = []
+        for layout, bg in enumerate(g):
+            idx = np.empty(max(n, 1), dtype=np.int64)
+            cnt = ctypes.c_longlong()
+            assert lib.lmb_mask_select(bg.ctypes.bit_generator.value, n,
+                                       frac, None, layout, idx.ctypes.data,
+                                       ctypes.byref(cnt)) == _native.LMB_OK
+            out.append(idx[:cnt.value].copy())
+        assert np.array_equal(out[0], out[1]), n
+        s0, s1 = (bg.state['state'] for bg in g)
+        assert np.array_equal(s0['key'], s1['key']) and s0['pos'] == s1['pos']
+
+
 def test_optimizer_configuration():
     opt = Optimizer(model=LorenzMie())
     assert opt.result is None and opt.mask is None
