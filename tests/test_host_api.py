@@ -166,7 +166,8 @@ def test_mask_mt19937_layouts_agree():
     leave the generator in the same state, for draws that straddle blocks
     (a double takes two of a block's 624 words).'''
     import ctypes
-    import pylorenzmie_b200.analysis.Mask as mask_module
+    import importlib
+    mask_module = importlib.import_module('pylorenzmie_b200.analysis.Mask')
     assert mask_module._mt_blocks_ok()
     lib = _native.load()
     g = [np.random.MT19937(99), np.random.MT19937(99)]
