@@ -461,9 +461,7 @@ def run_extras(dev, inst, chosen_value):
     out['reference_gpu_batch_hologram'] = reference_batch_hologram(dev)
 
     # hologram throughput of a 1280x1024 frame with 16 spheres
-    p = workloads.frame(seed=5)
-    while p.shape[0] < 16:
-        p = np.vstack([p, workloads.frame(seed=5 + p.shape[0])])[:16]
+    p = workloads.bench_frame()
     frames = {}
     for fp64 in (False, True):
         m = LorenzMie(coordinates=LorenzMie.meshgrid((1024, 1280)),

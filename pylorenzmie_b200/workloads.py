@@ -228,15 +228,46 @@ def _run_estimate_frame(device_search, repeat, optimize=False):
             print(f'optimize_frame {rep}: {time.perf_counter() - t0:.4f} s')
 
 
+def bench_frame():
+    '''Sphere parameters (16, 6) of the frame that bench.py times: seeded
+    frames stacked until 16 spheres.'''
+    p = frame(seed=5)
+    while p.shape[0] < 16:
+        p = np.vstack([p, frame(seed=5 + p.shape[0])])[:16]
+    return p
+
+
+def _run_frame(repeat, fp64=False):
+    '''LorenzMie.hologram(device=True) of the 16-sphere 1280x1024 frame,
+    ``repeat`` times; prints the milliseconds of each.'''
+    import time
+    import torch
+    from .theory import LorenzMie, Instrument
+    m = LorenzMie(coordinates=LorenzMie.meshgrid((1024, 1280)),
+                  particle=spheres(bench_frame()), instrument=Instrument(),
+                  double_precision=fp64)
+    for rep in range(repeat):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m.hologram(device=True)
+        torch.cuda.synchronize()
+        print(f'frame {rep}: {(time.perf_counter() - t0) * 1e3:.3f} ms')
+
+
 if __name__ == '__main__':
     # python -m pylorenzmie_b200.workloads estimate_frame [--device-search]
     #     [--optimize]
+    # python -m pylorenzmie_b200.workloads frame [--fp64]
     # runs one workload through the public API, e.g. under a profiler
     import argparse
     ap = argparse.ArgumentParser()
-    ap.add_argument('workload', choices=['estimate_frame'])
+    ap.add_argument('workload', choices=['estimate_frame', 'frame'])
     ap.add_argument('--device-search', action='store_true')
     ap.add_argument('--repeat', type=int, default=2)
     ap.add_argument('--optimize', action='store_true')
+    ap.add_argument('--fp64', action='store_true')
     a = ap.parse_args()
-    _run_estimate_frame(a.device_search, a.repeat, a.optimize)
+    if a.workload == 'frame':
+        _run_frame(a.repeat, a.fp64)
+    else:
+        _run_estimate_frame(a.device_search, a.repeat, a.optimize)
