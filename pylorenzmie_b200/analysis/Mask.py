@@ -89,8 +89,21 @@ class Mask(LMObject):
 
     def apply(self, hologram):
         '''Selected pixel values (nsel,) and coordinates (2, nsel); a fresh
-        random subset each call (analysis/Mask.py:82-105).'''
+        random subset each call (analysis/Mask.py:82-105).  The pixels are
+        gathered by index: a crop of a frame is a strided view, which a
+        flattening copy would copy whole.'''
         self.shape = hologram.shape
         idx = self._index
-        data = np.asarray(hologram.data).reshape(-1)[idx]
-        return data, hologram.flat_coordinates[:, idx]
+        data = np.asarray(hologram.data)
+        if data.ndim == 2:
+            rows, cols = np.divmod(idx, data.shape[1])
+            values = data[rows, cols]
+            if getattr(hologram, 'is_grid', False):
+                x0, y0 = hologram.corner
+                coords = np.empty((2, idx.size))
+                np.add(cols, float(x0), out=coords[0])
+                np.add(rows, float(y0), out=coords[1])
+            else:
+                coords = hologram.coordinates[:, rows, cols]
+            return values, coords
+        return data.reshape(-1)[idx], hologram.flat_coordinates[:, idx]

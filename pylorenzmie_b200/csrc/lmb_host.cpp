@@ -342,7 +342,15 @@ struct MtState {
   int pos;
 };
 
-void mt_regenerate(MtState* s) {
+// The block loops below are data-parallel; they are built for AVX2 and for
+// the baseline ISA, and the loader picks the clone the CPU supports.
+#if defined(__GNUC__) && !defined(__clang__) && defined(__x86_64__)
+#define LMB_CLONES __attribute__((target_clones("avx2", "default")))
+#else
+#define LMB_CLONES
+#endif
+
+LMB_CLONES void mt_regenerate(MtState* s) {
   const uint32_t upper = 0x80000000u, lower = 0x7fffffffu, a = 0x9908b0dfu;
   int i = 0;
   for (; i < kMtN - kMtM; ++i) {
@@ -375,6 +383,13 @@ inline uint32_t mt_word(MtState* s) {
   return mt_temper(s->key[s->pos++]);
 }
 
+// keep[j] = (the double of words w[2j], w[2j+1]) < fraction, j < m.
+LMB_CLONES void mt_keep_block(const uint32_t* w, long long m, double fraction,
+                              unsigned char* keep) {
+  for (long long j = 0; j < m; ++j)
+    keep[j] = mt_double(mt_temper(w[2 * j]), mt_temper(w[2 * j + 1])) < fraction;
+}
+
 }  // namespace
 
 extern "C" int lmb_mask_select(void* bitgen, long long n, double fraction,
@@ -405,10 +420,20 @@ extern "C" int lmb_mask_select(void* bitgen, long long n, double fraction,
       ++i;
       continue;
     }
-    const uint32_t* w = s->key + s->pos;
-    for (long long j = 0; j < pairs; ++j) {
-      const double u = mt_double(mt_temper(w[2 * j]), mt_temper(w[2 * j + 1]));
-      if (u < fraction && !(exclude && exclude[i + j])) index[k++] = i + j;
+    unsigned char keep[kMtN / 2];
+    mt_keep_block(s->key + s->pos, pairs, fraction, keep);
+    // branch-free compaction: every slot is written, k advances on a keep
+    // (index has room for n, and k <= i + j)
+    if (exclude) {
+      for (long long j = 0; j < pairs; ++j) {
+        index[k] = i + j;
+        k += keep[j] & (exclude[i + j] == 0);
+      }
+    } else {
+      for (long long j = 0; j < pairs; ++j) {
+        index[k] = i + j;
+        k += keep[j];
+      }
     }
     s->pos += int(2 * pairs);
     i += pairs;
