@@ -76,6 +76,17 @@ struct LMEval {
   double jtf[6];
 };
 
+// 1/sqrt(d) for d > 0: the device's reciprocal square root (a few ulp),
+// so that a Cholesky pivot's square root and its reciprocal come from one
+// operation and the divisions by the pivot become multiplications.
+LMB_HD double lm_rsqrt(double d) {
+#if defined(__CUDA_ARCH__)
+  return rsqrt(d);
+#else
+  return 1. / sqrt(d);
+#endif
+}
+
 LMB_HD double enorm(const double* v, int n) {
   double s = 0.;
   for (int i = 0; i < n; ++i) s += v[i] * v[i];
@@ -94,7 +105,7 @@ LMB_HD void lm_take(LMState& s, const LMEval& ev) {
 // Pivoted Cholesky of J^T J (the qrfac equivalent), column norms, Q^T f.
 LMB_HD void lm_factor(LMState& s) {
   const int n = s.n;
-  double w[LM_NV * LM_NV];
+  double w[LM_NV * LM_NV], rinv[LM_NV];
   for (int i = 0; i < n * LM_NV; ++i) w[i] = s.jtj[i];
   for (int j = 0; j < n; ++j) {
     s.ipvt[j] = j;
@@ -132,9 +143,10 @@ LMB_HD void lm_factor(LMState& s) {
       s.nsing = j;
       break;
     }
-    const double rjj = sqrt(d);
-    s.r[j * LM_NV + j] = rjj;
-    for (int k = j + 1; k < n; ++k) s.r[j * LM_NV + k] = w[j * LM_NV + k] / rjj;
+    const double inv = lm_rsqrt(d);
+    rinv[j] = inv;
+    s.r[j * LM_NV + j] = d * inv;
+    for (int k = j + 1; k < n; ++k) s.r[j * LM_NV + k] = w[j * LM_NV + k] * inv;
     for (int i = j + 1; i < n; ++i)
       for (int k = j + 1; k < n; ++k)
         w[i * LM_NV + k] -= s.r[j * LM_NV + i] * s.r[j * LM_NV + k];
@@ -147,14 +159,14 @@ LMB_HD void lm_factor(LMState& s) {
     }
     double sum = s.jtf[s.ipvt[j]];
     for (int i = 0; i < j; ++i) sum -= s.r[i * LM_NV + j] * s.qtf[i];
-    s.qtf[j] = sum / s.r[j * LM_NV + j];
+    s.qtf[j] = sum * rinv[j];
   }
 }
 
 // qrsolv equivalent: S = chol(R^T R + D_p^2) (pivoted order, D_p[j] =
 // dg[ipvt[j]]), solve S^T S z = R^T qtb, x[ipvt[j]] = z[j].
 LMB_HD void lm_qrsolv(const LMState& s, const double* dg, double* x,
-                      double* sm, double* sdiag) {
+                      double* sm, double* sdiag, double* sinv) {
   const int n = s.n;
   double m[LM_NV * LM_NV];
   for (int i = 0; i < n; ++i)
@@ -176,15 +188,19 @@ LMB_HD void lm_qrsolv(const LMState& s, const double* dg, double* x,
       nsing = j;
       break;
     }
-    const double sjj = sqrt(d);
-    sm[j * LM_NV + j] = sjj;
+    const double inv = lm_rsqrt(d);
+    sinv[j] = inv;
+    sm[j * LM_NV + j] = d * inv;
     for (int i = j + 1; i < n; ++i) {
       double e = m[j * LM_NV + i];
       for (int k = 0; k < j; ++k) e -= sm[k * LM_NV + j] * sm[k * LM_NV + i];
-      sm[j * LM_NV + i] = e / sjj;
+      sm[j * LM_NV + i] = e * inv;
     }
   }
-  for (int j = 0; j < n; ++j) sdiag[j] = j < nsing ? sm[j * LM_NV + j] : 0.;
+  for (int j = 0; j < n; ++j) {
+    sdiag[j] = j < nsing ? sm[j * LM_NV + j] : 0.;
+    if (j >= nsing) sinv[j] = 0.;
+  }
   // rhs = R^T qtb
   double z[LM_NV];
   for (int j = 0; j < n; ++j) {
@@ -199,12 +215,12 @@ LMB_HD void lm_qrsolv(const LMState& s, const double* dg, double* x,
     }
     double sum = z[j];
     for (int i = 0; i < j; ++i) sum -= sm[i * LM_NV + j] * z[i];
-    z[j] = sum / sm[j * LM_NV + j];
+    z[j] = sum * sinv[j];
   }
   for (int j = nsing - 1; j >= 0; --j) {  // S z = y
     double sum = z[j];
     for (int i = j + 1; i < nsing; ++i) sum -= sm[j * LM_NV + i] * z[i];
-    z[j] = sum / sm[j * LM_NV + j];
+    z[j] = sum * sinv[j];
   }
   for (int j = 0; j < n; ++j) x[s.ipvt[j]] = z[j];
 }
@@ -214,11 +230,15 @@ LMB_HD void lm_par(LMState& s, double* x) {
   const int n = s.n;
   const double dwarf = 2.2250738585072014e-308;
   const double p1 = 0.1, p001 = 0.001;
-  double wa1[LM_NV], wa2[LM_NV], sm[LM_NV * LM_NV], sdiag[LM_NV];
+  double wa1[LM_NV], wa2[LM_NV], sm[LM_NV * LM_NV], sdiag[LM_NV], sinv[LM_NV];
+  // reciprocals of R's diagonal, independent of one another, so that the
+  // dependent chains of the triangular solves below only multiply
+  double rinv[LM_NV];
+  for (int j = 0; j < s.nsing; ++j) rinv[j] = 1. / s.r[j * LM_NV + j];
   // Gauss-Newton direction
   for (int j = 0; j < n; ++j) wa1[j] = j < s.nsing ? s.qtf[j] : 0.;
   for (int j = s.nsing - 1; j >= 0; --j) {
-    wa1[j] /= s.r[j * LM_NV + j];
+    wa1[j] *= rinv[j];
     const double t = wa1[j];
     for (int i = 0; i < j; ++i) wa1[i] -= s.r[i * LM_NV + j] * t;
   }
@@ -234,14 +254,15 @@ LMB_HD void lm_par(LMState& s, double* x) {
   // lower bound
   double parl = 0.;
   if (s.nsing >= n) {
+    const double idx = 1. / dxnorm;
     for (int j = 0; j < n; ++j) {
       const int l = s.ipvt[j];
-      wa1[j] = s.diag[l] * (wa2[l] / dxnorm);
+      wa1[j] = s.diag[l] * (wa2[l] * idx);
     }
     for (int j = 0; j < n; ++j) {
       double sum = 0.;
       for (int i = 0; i < j; ++i) sum += s.r[i * LM_NV + j] * wa1[i];
-      wa1[j] = (wa1[j] - sum) / s.r[j * LM_NV + j];
+      wa1[j] = (wa1[j] - sum) * rinv[j];
     }
     const double t = enorm(wa1, n);
     parl = ((fp / s.delta) / t) / t;
@@ -265,7 +286,7 @@ LMB_HD void lm_par(LMState& s, double* x) {
     const double t = sqrt(par);
     double dg[LM_NV];
     for (int j = 0; j < n; ++j) dg[j] = t * s.diag[j];
-    lm_qrsolv(s, dg, x, sm, sdiag);
+    lm_qrsolv(s, dg, x, sm, sdiag, sinv);
     for (int j = 0; j < n; ++j) wa2[j] = s.diag[j] * x[j];
     dxnorm = enorm(wa2, n);
     const double temp = fp;
@@ -274,12 +295,13 @@ LMB_HD void lm_par(LMState& s, double* x) {
         iter == 10)
       break;
     // Newton correction: solve S^T w = D P^T x / ||D x||
+    const double idx = 1. / dxnorm;
     for (int j = 0; j < n; ++j) {
       const int l = s.ipvt[j];
-      wa1[j] = s.diag[l] * (wa2[l] / dxnorm);
+      wa1[j] = s.diag[l] * (wa2[l] * idx);
     }
     for (int j = 0; j < n; ++j) {
-      wa1[j] /= sdiag[j];
+      wa1[j] *= sinv[j];
       const double tj = wa1[j];
       for (int i = j + 1; i < n; ++i) wa1[i] -= sm[j * LM_NV + i] * tj;
     }
@@ -332,11 +354,12 @@ LMB_HD int lm_outer(LMState& s, const LMSettings& set) {
   }
   s.gnorm = 0.;
   if (s.fnorm != 0.) {
+    const double ifn = 1. / s.fnorm;
     for (int j = 0; j < n; ++j) {
       const int l = s.ipvt[j];
       if (s.acnorm[l] == 0.) continue;
       double sum = 0.;
-      for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * (s.qtf[i] / s.fnorm);
+      for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * (s.qtf[i] * ifn);
       const double g = fabs(sum / s.acnorm[l]);
       if (g > s.gnorm) s.gnorm = g;
     }
