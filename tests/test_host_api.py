@@ -235,6 +235,19 @@ def test_device_fit_selection():
     assert not opt._device_fit_ok()
 
 
+def test_small_batch_shape():
+    '''Batches below SMALL_BATCH features evaluate with one pixel pair a
+    thread (256 threads x 2 pixels); larger ones keep the default shape.'''
+    import ctypes
+    lib = _native.load()
+    tpb, ppt, minb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert lib.lmb_fit_tile_config(_fit.SMALL_SHAPE, ctypes.byref(tpb),
+                                   ctypes.byref(ppt), ctypes.byref(minb)) == 0
+    assert (tpb.value, ppt.value) == (256, 2)
+    assert _fit.default_shape(1) == _fit.default_shape(63) == _fit.SMALL_SHAPE
+    assert _fit.default_shape(64) == _fit.default_shape(256) == 0
+
+
 def test_packed_features_layout():
     a = np.ones((3, 4))
     b = np.arange(6.)
