@@ -102,150 +102,291 @@ LMB_HD void lm_take(LMState& s, const LMEval& ev) {
   }
 }
 
-// Pivoted Cholesky of J^T J (the qrfac equivalent), column norms, Q^T f.
-LMB_HD void lm_factor(LMState& s) {
-  const int n = s.n;
-  double w[LM_NV * LM_NV], rinv[LM_NV];
-  for (int i = 0; i < n * LM_NV; ++i) w[i] = s.jtj[i];
-  for (int j = 0; j < n; ++j) {
-    s.ipvt[j] = j;
-    const double c = s.jtj[j * LM_NV + j];
+// base[k * stride] for a runtime k with lo <= k < N, and its store, by
+// compare-selects over the unrolled indices (see lm_get).
+template <int N>
+LMB_HD double lm_gets(const double* base, int stride, int k, int lo) {
+  double r = base[lo * stride];
+#pragma unroll
+  for (int l = 0; l < N; ++l)
+    if (l > lo) r = k == l ? base[l * stride] : r;
+  return r;
+}
+template <int N>
+LMB_HD void lm_puts(double* base, int stride, int k, int lo, double val) {
+#pragma unroll
+  for (int l = 0; l < N; ++l)
+    if (l >= lo && k == l) base[l * stride] = val;
+}
+
+// Pivoted Cholesky of J^T J (the qrfac equivalent), column norms, Q^T f,
+// for N free variables: MINPACK's qrfac pivot rule (largest remaining
+// column norm = largest Schur diagonal), written with N a compile-time
+// constant so that the work arrays are indexed by constants (the pivot
+// swaps by compare-selects).  The arithmetic, comparisons and swaps are
+// those of the loops to n, in the same order.
+template <int N>
+LMB_HD void lm_factor_n(LMState& s) {
+  double w[N * N], r[N * N], rinv[N], jf[N], qt[N];
+  int piv[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    jf[i] = s.jtf[i];
+#pragma unroll
+    for (int j = 0; j < N; ++j) w[i * N + j] = s.jtj[i * LM_NV + j];
+  }
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    piv[j] = j;
+    const double c = w[j * N + j];
     s.acnorm[j] = sqrt(c > 0. ? c : 0.);
   }
-  for (int i = 0; i < LM_NV * LM_NV; ++i) s.r[i] = 0.;
-  s.nsing = n;
-  for (int j = 0; j < n; ++j) {
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) r[i] = 0.;
+  int nsing = N;
+  bool stop = false;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if (stop) break;
     int kmax = j;
-    for (int k = j + 1; k < n; ++k)
-      if (w[k * LM_NV + k] > w[kmax * LM_NV + kmax]) kmax = k;
+    double best = w[j * N + j];
+#pragma unroll
+    for (int k = j + 1; k < N; ++k)
+      if (w[k * N + k] > best) {
+        best = w[k * N + k];
+        kmax = k;
+      }
     if (kmax != j) {
-      for (int i = 0; i < n; ++i) {
-        double t = w[i * LM_NV + j];
-        w[i * LM_NV + j] = w[i * LM_NV + kmax];
-        w[i * LM_NV + kmax] = t;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {  // columns j and kmax
+        const double t = w[i * N + j];
+        w[i * N + j] = lm_gets<N>(w + i * N, 1, kmax, j + 1);
+        lm_puts<N>(w + i * N, 1, kmax, j + 1, t);
       }
-      for (int i = 0; i < n; ++i) {
-        double t = w[j * LM_NV + i];
-        w[j * LM_NV + i] = w[kmax * LM_NV + i];
-        w[kmax * LM_NV + i] = t;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {  // rows j and kmax
+        const double t = w[j * N + i];
+        w[j * N + i] = lm_gets<N>(w + i, N, kmax, j + 1);
+        lm_puts<N>(w + i, N, kmax, j + 1, t);
       }
+#pragma unroll
       for (int i = 0; i < j; ++i) {  // rows of R already formed
-        double t = s.r[i * LM_NV + j];
-        s.r[i * LM_NV + j] = s.r[i * LM_NV + kmax];
-        s.r[i * LM_NV + kmax] = t;
+        const double t = r[i * N + j];
+        r[i * N + j] = lm_gets<N>(r + i * N, 1, kmax, j + 1);
+        lm_puts<N>(r + i * N, 1, kmax, j + 1, t);
       }
-      int t = s.ipvt[j];
-      s.ipvt[j] = s.ipvt[kmax];
-      s.ipvt[kmax] = t;
+      int pk = piv[j];
+#pragma unroll
+      for (int l = 0; l < N; ++l)
+        if (l > j && l == kmax) pk = piv[l];
+#pragma unroll
+      for (int l = 0; l < N; ++l)
+        if (l > j && l == kmax) piv[l] = piv[j];
+      piv[j] = pk;
     }
-    const double d = w[j * LM_NV + j];
+    const double d = w[j * N + j];
     if (!(d > 0.)) {
-      s.nsing = j;
+      nsing = j;
+      stop = true;
       break;
     }
     const double inv = lm_rsqrt(d);
     rinv[j] = inv;
-    s.r[j * LM_NV + j] = d * inv;
-    for (int k = j + 1; k < n; ++k) s.r[j * LM_NV + k] = w[j * LM_NV + k] * inv;
-    for (int i = j + 1; i < n; ++i)
-      for (int k = j + 1; k < n; ++k)
-        w[i * LM_NV + k] -= s.r[j * LM_NV + i] * s.r[j * LM_NV + k];
+    r[j * N + j] = d * inv;
+#pragma unroll
+    for (int k = j + 1; k < N; ++k) r[j * N + k] = w[j * N + k] * inv;
+#pragma unroll
+    for (int i = j + 1; i < N; ++i)
+#pragma unroll
+      for (int k = j + 1; k < N; ++k) w[i * N + k] -= r[j * N + i] * r[j * N + k];
   }
   // R^T qtf = P^T J^T f on the nonsingular block; zero beyond it
-  for (int j = 0; j < n; ++j) {
-    if (j >= s.nsing) {
-      s.qtf[j] = 0.;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if (j >= nsing) {
+      qt[j] = 0.;
       continue;
     }
-    double sum = s.jtf[s.ipvt[j]];
-    for (int i = 0; i < j; ++i) sum -= s.r[i * LM_NV + j] * s.qtf[i];
-    s.qtf[j] = sum * rinv[j];
+    double sum = lm_gets<N>(jf, 1, piv[j], 0);
+#pragma unroll
+    for (int i = 0; i < j; ++i) sum -= r[i * N + j] * qt[i];
+    qt[j] = sum * rinv[j];
+  }
+  s.nsing = nsing;
+#pragma unroll
+  for (int i = 0; i < LM_NV * LM_NV; ++i) s.r[i] = 0.;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    s.ipvt[i] = piv[i];
+    s.qtf[i] = qt[i];
+#pragma unroll
+    for (int j = 0; j < N; ++j) s.r[i * LM_NV + j] = r[i * N + j];
   }
 }
 
+LMB_HD void lm_factor(LMState& s) {
+  switch (s.n) {
+    case 1: lm_factor_n<1>(s); break;
+    case 2: lm_factor_n<2>(s); break;
+    case 3: lm_factor_n<3>(s); break;
+    case 4: lm_factor_n<4>(s); break;
+    case 5: lm_factor_n<5>(s); break;
+    default: lm_factor_n<6>(s); break;
+  }
+}
+
+// v[k] and v[k] = val for a runtime k < N, by compare-selects over the
+// unrolled indices, so that v can stay in registers.
+template <int N>
+LMB_HD double lm_get(const double* v, int k) {
+  double r = v[0];
+#pragma unroll
+  for (int l = 1; l < N; ++l) r = k == l ? v[l] : r;
+  return r;
+}
+template <int N>
+LMB_HD void lm_put(double* v, int k, double val) {
+#pragma unroll
+  for (int l = 0; l < N; ++l)
+    if (k == l) v[l] = val;
+}
+
+// lmpar and its qrsolv for N free variables (the loops of MINPACK's lmpar
+// and qrsolv, restated on the normal equations as described above), with
+// N a compile-time constant: the loops unroll, and R, the pivots and the
+// work arrays are indexed by constants (pivot-indexed accesses by
+// compare-selects), so that they can live in registers.  The arithmetic
+// and its order are those of the loops to n.
+template <int N>
+struct LMPar {
+  double R[N * N];   // R (upper triangle used), row-major N x N
+  double rinv[N];    // 1 / R[j][j] for j < nsing
+  double qtf[N], diag[N];
+  int piv[N];
+  int nsing;
+};
+
 // qrsolv equivalent: S = chol(R^T R + D_p^2) (pivoted order, D_p[j] =
 // dg[ipvt[j]]), solve S^T S z = R^T qtb, x[ipvt[j]] = z[j].
-LMB_HD void lm_qrsolv(const LMState& s, const double* dg, double* x,
-                      double* sm, double* sdiag, double* sinv) {
-  const int n = s.n;
-  double m[LM_NV * LM_NV];
-  for (int i = 0; i < n; ++i)
-    for (int j = i; j < n; ++j) {
+template <int N>
+LMB_HD void lm_qrsolv_n(const LMPar<N>& q, const double* dg, double* x,
+                        double* sm, double* sdiag, double* sinv) {
+  double m[N * N];
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int j = i; j < N; ++j) {
       double sum = 0.;
-      for (int k = 0; k <= i; ++k) sum += s.r[k * LM_NV + i] * s.r[k * LM_NV + j];
-      m[i * LM_NV + j] = sum;
+#pragma unroll
+      for (int k = 0; k <= i; ++k) sum += q.R[k * N + i] * q.R[k * N + j];
+      m[i * N + j] = sum;
     }
-  for (int j = 0; j < n; ++j) {
-    const double d = dg[s.ipvt[j]];
-    m[j * LM_NV + j] += d * d;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const double d = lm_get<N>(dg, q.piv[j]);
+    m[j * N + j] += d * d;
   }
-  for (int i = 0; i < LM_NV * LM_NV; ++i) sm[i] = 0.;
-  int nsing = n;
-  for (int j = 0; j < n; ++j) {
-    double d = m[j * LM_NV + j];
-    for (int k = 0; k < j; ++k) d -= sm[k * LM_NV + j] * sm[k * LM_NV + j];
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) sm[i] = 0.;
+  int nsing = N;
+  bool stop = false;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if (stop) break;
+    double d = m[j * N + j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) d -= sm[k * N + j] * sm[k * N + j];
     if (!(d > 0.)) {
       nsing = j;
+      stop = true;
       break;
     }
     const double inv = lm_rsqrt(d);
     sinv[j] = inv;
-    sm[j * LM_NV + j] = d * inv;
-    for (int i = j + 1; i < n; ++i) {
-      double e = m[j * LM_NV + i];
-      for (int k = 0; k < j; ++k) e -= sm[k * LM_NV + j] * sm[k * LM_NV + i];
-      sm[j * LM_NV + i] = e * inv;
+    sm[j * N + j] = d * inv;
+#pragma unroll
+    for (int i = j + 1; i < N; ++i) {
+      double e = m[j * N + i];
+#pragma unroll
+      for (int k = 0; k < j; ++k) e -= sm[k * N + j] * sm[k * N + i];
+      sm[j * N + i] = e * inv;
     }
   }
-  for (int j = 0; j < n; ++j) {
-    sdiag[j] = j < nsing ? sm[j * LM_NV + j] : 0.;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    sdiag[j] = j < nsing ? sm[j * N + j] : 0.;
     if (j >= nsing) sinv[j] = 0.;
   }
   // rhs = R^T qtb
-  double z[LM_NV];
-  for (int j = 0; j < n; ++j) {
+  double z[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
     double sum = 0.;
-    for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * s.qtf[i];
+#pragma unroll
+    for (int i = 0; i <= j; ++i) sum += q.R[i * N + j] * q.qtf[i];
     z[j] = sum;
   }
-  for (int j = 0; j < n; ++j) {  // S^T y = rhs
+#pragma unroll
+  for (int j = 0; j < N; ++j) {  // S^T y = rhs
     if (j >= nsing) {
       z[j] = 0.;
       continue;
     }
     double sum = z[j];
-    for (int i = 0; i < j; ++i) sum -= sm[i * LM_NV + j] * z[i];
+#pragma unroll
+    for (int i = 0; i < j; ++i) sum -= sm[i * N + j] * z[i];
     z[j] = sum * sinv[j];
   }
-  for (int j = nsing - 1; j >= 0; --j) {  // S z = y
+#pragma unroll
+  for (int j = N - 1; j >= 0; --j) {  // S z = y
+    if (j >= nsing) continue;
     double sum = z[j];
-    for (int i = j + 1; i < nsing; ++i) sum -= sm[j * LM_NV + i] * z[i];
+#pragma unroll
+    for (int i = j + 1; i < N; ++i)
+      if (i < nsing) sum -= sm[j * N + i] * z[i];
     z[j] = sum * sinv[j];
   }
-  for (int j = 0; j < n; ++j) x[s.ipvt[j]] = z[j];
+#pragma unroll
+  for (int j = 0; j < N; ++j) lm_put<N>(x, q.piv[j], z[j]);
 }
 
 // lmpar: damping parameter and the step x (the step is p = -x).
-LMB_HD void lm_par(LMState& s, double* x) {
-  const int n = s.n;
+template <int N>
+LMB_HD void lm_par_n(LMState& s, double* x) {
   const double dwarf = 2.2250738585072014e-308;
   const double p1 = 0.1, p001 = 0.001;
-  double wa1[LM_NV], wa2[LM_NV], sm[LM_NV * LM_NV], sdiag[LM_NV], sinv[LM_NV];
+  LMPar<N> q;
+  q.nsing = s.nsing;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    q.piv[i] = s.ipvt[i];
+    q.qtf[i] = s.qtf[i];
+    q.diag[i] = s.diag[i];
+#pragma unroll
+    for (int j = 0; j < N; ++j) q.R[i * N + j] = s.r[i * LM_NV + j];
+  }
+  double wa1[N], wa2[N], sm[N * N], sdiag[N], sinv[N];
   // reciprocals of R's diagonal, independent of one another, so that the
   // dependent chains of the triangular solves below only multiply
-  double rinv[LM_NV];
-  for (int j = 0; j < s.nsing; ++j) rinv[j] = 1. / s.r[j * LM_NV + j];
+#pragma unroll
+  for (int j = 0; j < N; ++j) q.rinv[j] = j < q.nsing ? 1. / q.R[j * N + j] : 0.;
   // Gauss-Newton direction
-  for (int j = 0; j < n; ++j) wa1[j] = j < s.nsing ? s.qtf[j] : 0.;
-  for (int j = s.nsing - 1; j >= 0; --j) {
-    wa1[j] *= rinv[j];
+#pragma unroll
+  for (int j = 0; j < N; ++j) wa1[j] = j < q.nsing ? q.qtf[j] : 0.;
+#pragma unroll
+  for (int j = N - 1; j >= 0; --j) {
+    if (j >= q.nsing) continue;
+    wa1[j] *= q.rinv[j];
     const double t = wa1[j];
-    for (int i = 0; i < j; ++i) wa1[i] -= s.r[i * LM_NV + j] * t;
+#pragma unroll
+    for (int i = 0; i < j; ++i) wa1[i] -= q.R[i * N + j] * t;
   }
-  for (int j = 0; j < n; ++j) x[s.ipvt[j]] = wa1[j];
+#pragma unroll
+  for (int j = 0; j < N; ++j) lm_put<N>(x, q.piv[j], wa1[j]);
   int iter = 0;
-  for (int j = 0; j < n; ++j) wa2[j] = s.diag[j] * x[j];
-  double dxnorm = enorm(wa2, n);
+#pragma unroll
+  for (int j = 0; j < N; ++j) wa2[j] = q.diag[j] * x[j];
+  double dxnorm = enorm(wa2, N);
   double fp = dxnorm - s.delta;
   if (fp <= p1 * s.delta) {
     s.par = 0.;
@@ -253,27 +394,32 @@ LMB_HD void lm_par(LMState& s, double* x) {
   }
   // lower bound
   double parl = 0.;
-  if (s.nsing >= n) {
+  if (q.nsing >= N) {
     const double idx = 1. / dxnorm;
-    for (int j = 0; j < n; ++j) {
-      const int l = s.ipvt[j];
-      wa1[j] = s.diag[l] * (wa2[l] * idx);
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      const int l = q.piv[j];
+      wa1[j] = lm_get<N>(q.diag, l) * (lm_get<N>(wa2, l) * idx);
     }
-    for (int j = 0; j < n; ++j) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
       double sum = 0.;
-      for (int i = 0; i < j; ++i) sum += s.r[i * LM_NV + j] * wa1[i];
-      wa1[j] = (wa1[j] - sum) * rinv[j];
+#pragma unroll
+      for (int i = 0; i < j; ++i) sum += q.R[i * N + j] * wa1[i];
+      wa1[j] = (wa1[j] - sum) * q.rinv[j];
     }
-    const double t = enorm(wa1, n);
+    const double t = enorm(wa1, N);
     parl = ((fp / s.delta) / t) / t;
   }
   // upper bound
-  for (int j = 0; j < n; ++j) {
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
     double sum = 0.;
-    for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * s.qtf[i];
-    wa1[j] = sum / s.diag[s.ipvt[j]];
+#pragma unroll
+    for (int i = 0; i <= j; ++i) sum += q.R[i * N + j] * q.qtf[i];
+    wa1[j] = sum / lm_get<N>(q.diag, q.piv[j]);
   }
-  const double gnorm = enorm(wa1, n);
+  const double gnorm = enorm(wa1, N);
   double paru = gnorm / s.delta;
   if (paru == 0.) paru = dwarf / (s.delta < p1 ? s.delta : p1);
   double par = s.par;
@@ -284,11 +430,13 @@ LMB_HD void lm_par(LMState& s, double* x) {
     ++iter;
     if (par == 0.) par = dwarf > p001 * paru ? dwarf : p001 * paru;
     const double t = sqrt(par);
-    double dg[LM_NV];
-    for (int j = 0; j < n; ++j) dg[j] = t * s.diag[j];
-    lm_qrsolv(s, dg, x, sm, sdiag, sinv);
-    for (int j = 0; j < n; ++j) wa2[j] = s.diag[j] * x[j];
-    dxnorm = enorm(wa2, n);
+    double dg[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) dg[j] = t * q.diag[j];
+    lm_qrsolv_n<N>(q, dg, x, sm, sdiag, sinv);
+#pragma unroll
+    for (int j = 0; j < N; ++j) wa2[j] = q.diag[j] * x[j];
+    dxnorm = enorm(wa2, N);
     const double temp = fp;
     fp = dxnorm - s.delta;
     if (fabs(fp) <= p1 * s.delta || (parl == 0. && fp <= temp && temp < 0.) ||
@@ -296,22 +444,36 @@ LMB_HD void lm_par(LMState& s, double* x) {
       break;
     // Newton correction: solve S^T w = D P^T x / ||D x||
     const double idx = 1. / dxnorm;
-    for (int j = 0; j < n; ++j) {
-      const int l = s.ipvt[j];
-      wa1[j] = s.diag[l] * (wa2[l] * idx);
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      const int l = q.piv[j];
+      wa1[j] = lm_get<N>(q.diag, l) * (lm_get<N>(wa2, l) * idx);
     }
-    for (int j = 0; j < n; ++j) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
       wa1[j] *= sinv[j];
       const double tj = wa1[j];
-      for (int i = j + 1; i < n; ++i) wa1[i] -= sm[j * LM_NV + i] * tj;
+#pragma unroll
+      for (int i = j + 1; i < N; ++i) wa1[i] -= sm[j * N + i] * tj;
     }
-    const double tn = enorm(wa1, n);
+    const double tn = enorm(wa1, N);
     const double parc = ((fp / s.delta) / tn) / tn;
     if (fp > 0.) parl = parl > par ? parl : par;
     if (fp < 0.) paru = paru < par ? paru : par;
     par = parl > par + parc ? parl : par + parc;
   }
   s.par = par;
+}
+
+LMB_HD void lm_par(LMState& s, double* x) {
+  switch (s.n) {
+    case 1: lm_par_n<1>(s, x); break;
+    case 2: lm_par_n<2>(s, x); break;
+    case 3: lm_par_n<3>(s, x); break;
+    case 4: lm_par_n<4>(s, x); break;
+    case 5: lm_par_n<5>(s, x); break;
+    default: lm_par_n<6>(s, x); break;
+  }
 }
 
 // Inner loop head: choose the next trial step.  Writes s.p.
