@@ -477,27 +477,43 @@ LMB_HD void lm_par(LMState& s, double* x) {
 }
 
 // Inner loop head: choose the next trial step.  Writes s.p.
-LMB_HD void lm_trial(LMState& s) {
-  const int n = s.n;
+template <int N>
+LMB_HD void lm_trial_n(LMState& s) {
   double x[LM_NV];
-  lm_par(s, x);
-  double wa3[LM_NV];
-  for (int j = 0; j < n; ++j) {
-    s.p[j] = -x[j];
-    wa3[j] = s.diag[j] * s.p[j];
+  lm_par_n<N>(s, x);
+  double p[N], wa3[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    p[j] = -x[j];
+    s.p[j] = p[j];
+    wa3[j] = s.diag[j] * p[j];
   }
-  s.pnorm = enorm(wa3, n);
+  s.pnorm = enorm(wa3, N);
   if (s.iter == 1 && s.pnorm < s.delta) s.delta = s.pnorm;
   // predicted reduction from ||R P^T p||
-  for (int j = 0; j < n; ++j) wa3[j] = 0.;
-  for (int j = 0; j < n; ++j) {
-    const double t = s.p[s.ipvt[j]];
+#pragma unroll
+  for (int j = 0; j < N; ++j) wa3[j] = 0.;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const double t = lm_get<N>(p, s.ipvt[j]);
+#pragma unroll
     for (int i = 0; i <= j; ++i) wa3[i] += s.r[i * LM_NV + j] * t;
   }
-  const double temp1 = enorm(wa3, n) / s.fnorm;
+  const double temp1 = enorm(wa3, N) / s.fnorm;
   const double temp2 = (sqrt(s.par) * s.pnorm) / s.fnorm;
   s.prered = temp1 * temp1 + temp2 * temp2 / 0.5;
   s.dirder = -(temp1 * temp1 + temp2 * temp2);
+}
+
+LMB_HD void lm_trial(LMState& s) {
+  switch (s.n) {
+    case 1: lm_trial_n<1>(s); break;
+    case 2: lm_trial_n<2>(s); break;
+    case 3: lm_trial_n<3>(s); break;
+    case 4: lm_trial_n<4>(s); break;
+    case 5: lm_trial_n<5>(s); break;
+    default: lm_trial_n<6>(s); break;
+  }
 }
 
 // Outer loop body after a new Jacobian at x: scaling, gradient test, trial.
@@ -517,12 +533,18 @@ LMB_HD int lm_outer(LMState& s, const LMSettings& set) {
   s.gnorm = 0.;
   if (s.fnorm != 0.) {
     const double ifn = 1. / s.fnorm;
-    for (int j = 0; j < n; ++j) {
-      const int l = s.ipvt[j];
-      if (s.acnorm[l] == 0.) continue;
+    double acn[LM_NV];
+#pragma unroll
+    for (int l = 0; l < LM_NV; ++l) acn[l] = s.acnorm[l];
+#pragma unroll
+    for (int j = 0; j < LM_NV; ++j) {
+      if (j >= n) break;
+      const double a = lm_get<LM_NV>(acn, s.ipvt[j]);
+      if (a == 0.) continue;
       double sum = 0.;
+#pragma unroll
       for (int i = 0; i <= j; ++i) sum += s.r[i * LM_NV + j] * (s.qtf[i] * ifn);
-      const double g = fabs(sum / s.acnorm[l]);
+      const double g = fabs(sum / a);
       if (g > s.gnorm) s.gnorm = g;
     }
   }
