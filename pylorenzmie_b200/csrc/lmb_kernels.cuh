@@ -76,8 +76,9 @@ __device__ int warp_sphere_ab(double a_p, double n_p, double k_p, double n_m,
   for (int n = 1 + lane; n <= s.nmax; n += 32)
     mie_orders(s, n, w.nz, w.nz2, w.nx, w.nx2);
   __syncwarp();
-  if (lane == 0) mie_d1_inside(s, w.nz, w.nz2, w.d1in, w.d1inz);
-  if (lane == 1) mie_d1_medium(s, w.nx, w.nx2, w.d1m, w.d1mx);
+  // the inside and the medium's D1 on lanes 0 and 1, in step
+  if (lane < 2)
+    mie_d1_both(s, lane, w.nz, w.nz2, w.nx, w.nx2, w.d1in, w.d1inz, w.d1m, w.d1mx);
   __syncwarp();
   if (lane == 0)
     mie_upward(s, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
