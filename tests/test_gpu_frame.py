@@ -50,6 +50,26 @@ def test_frame_fp32_vs_fp64_and_oracle(seed):
     assert np.abs(m.hologram() - h32[idx]).max() <= 1e-6
 
 
+def test_frames_fp32_within_2e5_many_seeds():
+    '''Every pixel of 20 more seeded frames (1-16 spheres each) within
+    2e-5 of the FP64 kernel, which is itself pinned to the oracle above.'''
+    import torch
+    from pylorenzmie_b200 import LorenzMie, workloads
+    coords = LorenzMie.meshgrid((1024, 1280))
+    m32 = LorenzMie(coordinates=coords)
+    m64 = LorenzMie(coordinates=coords, double_precision=True)
+    worst = 0.
+    for seed in range(3, 23):
+        spheres = workloads.spheres(workloads.frame(seed=seed))
+        m32.particle = spheres
+        m64.particle = spheres
+        d = (m32.hologram(device=True).double() -
+             m64.hologram(device=True)).abs().max().item()
+        worst = max(worst, d)
+        assert d <= 2e-5, (seed, d)
+    assert worst > 0.
+
+
 def test_frame_batch_items_fp64_resum():
     '''Several frames in one launch (batch_hologram): each item's marked
     pixels are summed again in FP64.'''
