@@ -184,10 +184,11 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
   AbScratch w;
   if (layered_parallel(nmaxp, L)) {
     // Warp-parallel: all downward recurrences on lanes of their own
-    // (core, medium and two per shell), then every shell's upward
-    // recurrences on one lane each, then the shells in order with their
-    // Ha/Hb updates spread over the orders.  Same arithmetic per order as
-    // the serial form below.
+    // (core, medium and two per shell), then each shell argument's upward
+    // D3 chain on a lane of its own, then Q's factors over the orders and
+    // their running products one lane per shell, then the shells in order
+    // with their Ha/Hb updates spread over the orders.  The same
+    // recurrences as the serial form below.
     dz* d1c = reinterpret_cast<dz*>(scratch);
     dz* sh = d1c + na;  // shell ii: d1a, d1b, d3a, d3b, q at sh + 5 (ii-1) na
     ha = sh + 5 * (L - 1) * na;
@@ -220,15 +221,31 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
       layered_d1_down(z, s.nmax, out);
     }
     __syncwarp();
-    if (lane >= 1 && lane < L) {
-      dz* b = sh + 5 * (lane - 1) * na;
-      layered_shell_rec(s, layered_shell_setup(s, lane), b, b + na, b + 2 * na,
-                        b + 3 * na, b + 4 * na);
+    if (lane < 2 * (L - 1)) {
+      // each shell argument's upward psi*zeta and D3 chain on a lane of its
+      // own, one code path
+      const int ii = lane / 2 + 1, which = lane & 1;
+      const ShellSetup h = layered_shell_setup(s, ii);
+      dz* b = sh + 5 * (ii - 1) * na;
+      layered_d3_up(which == 0 ? h.z1 : h.z2, s.nmax, b + which * na,
+                    b + (2 + which) * na);
     }
     for (int n = lane; n <= s.nmax; n += 32) {
       ha[n] = d1c[n];
       hb[n] = d1c[n];
     }
+    __syncwarp();
+    // the factors of every shell's Q, over (shell, order) pairs
+    for (int j = lane; j < (L - 1) * s.nmax; j += 32) {
+      const int ii = j / s.nmax + 1, n = j - (ii - 1) * s.nmax + 1;
+      dz* b = sh + 5 * (ii - 1) * na;
+      b[4 * na + n] = layered_q_ratio(layered_shell_setup(s, ii), n, b, b + na,
+                                      b + 2 * na, b + 3 * na);
+    }
+    __syncwarp();
+    if (lane < L - 1)
+      layered_q_product(layered_shell_setup(s, lane + 1), s.nmax,
+                        sh + (5 * lane + 4) * na);
     __syncwarp();
     for (int ii = 1; ii < L; ++ii) {
       const ShellSetup h = layered_shell_setup(s, ii);

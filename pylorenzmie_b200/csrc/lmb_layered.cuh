@@ -117,7 +117,7 @@ LMB_HD void layered_d1_down(dz z, int nmax, dz* d) {
 // Ha, Hb of the outermost layer after the core and all shells.
 //   d1a, d1b: scratch of nmax+1 duals each; ha, hb: nmax+1 duals (output)
 // Runs on one thread; with two lanes available the caller may split the
-// two downward recurrences (see warp_layered_hab).
+// two downward recurrences (see warp_layered_ab).
 LMB_HD void layered_core(const LayeredScalars& s, dz* d1a, dz* ha, dz* hb) {
   const int L = s.L;
   dz z1;
@@ -158,32 +158,44 @@ LMB_HD ShellSetup layered_shell_setup(const LayeredScalars& s, int ii) {
   return h;
 }
 
-// Upward recurrences of shell ii for n = 1..nmax: psi*zeta at z1 and z2,
-// D3 at both, and the ratio Q (Eqs. (13)-(15)); stores D3(z1), D3(z2) and
-// Q after step n in d3a[n], d3b[n], q[n].  Serial in n.
-LMB_HD void layered_shell_rec(const LayeredScalars& s, const ShellSetup& h,
-                              const dz* d1a, const dz* d1b, dz* d3a_out,
-                              dz* d3b_out, dz* q_out) {
+// The upward recurrence of one argument z of a shell (z1 or z2) for
+// n = 1..nmax: psi*zeta (Eq. (13)) and D3 (Eq. (14)), given D1 at z;
+// stores D3 in d3[0..nmax].  The only serial chain of a shell: the ratio
+// Q (Eq. (15)) follows from the stored D1, D3 order by order
+// (layered_q_ratio, layered_q_product).
+LMB_HD void layered_d3_up(dz z, int nmax, const dz* d1, dz* d3) {
   const zd ii1 = mk(0., 1.);
-  dz pza = 0.5 * (1. - dexpi(2., h.z1));
-  dz pzb = 0.5 * (1. - dexpi(2., h.z2));
-  dz d3a = dconst(ii1), d3b = dconst(ii1);
-  dz q = (dexpi(-2., h.z2) + (-1.)) / (dexpi(-2., h.z1) + (-1.));
-  const dz iz1 = dinv(h.z1), iz2 = dinv(h.z2);
-  for (int n = 1; n <= s.nmax; ++n) {
-    const double fn = double(n);
-    const dz nz1 = fn * iz1, nz2 = fn * iz2;
-    const dz d3a_prev = d3a, d3b_prev = d3b;
-    pza = pza * ((nz1 - d1a[n - 1]) * (nz1 - d3a_prev));
-    pzb = pzb * ((nz2 - d1b[n - 1]) * (nz2 - d3b_prev));
-    d3a = d1a[n] + ii1 * dinv(pza);
-    d3b = d1b[n] + ii1 * dinv(pzb);
-    const dz num = (h.z1 * d1a[n] + fn) * (fn - h.z1 * d3a_prev);
-    const dz den = (h.z2 * d1b[n] + fn) * (fn - h.z2 * d3b_prev);
-    q = h.xr2 * (q * num / den);
-    d3a_out[n] = d3a;
-    d3b_out[n] = d3b;
-    q_out[n] = q;
+  dz pz = 0.5 * (1. - dexpi(2., z));
+  dz cur = dconst(ii1);
+  d3[0] = cur;
+  const dz iz = dinv(z);
+  for (int n = 1; n <= nmax; ++n) {
+    const dz nz = double(n) * iz;
+    pz = pz * ((nz - d1[n - 1]) * (nz - cur));
+    cur = d1[n] + ii1 * dinv(pz);
+    d3[n] = cur;
+  }
+}
+
+// The factor of order n >= 1 in Q_n = Q_{n-1} * r_n (Eq. (15)):
+//   r_n = (x_{l-1}/x_l)^2 (z1 D1_n(z1) + n)(n - z1 D3_{n-1}(z1))
+//                       / ((z2 D1_n(z2) + n)(n - z2 D3_{n-1}(z2))).
+// Orders are independent.
+LMB_HD dz layered_q_ratio(const ShellSetup& h, int n, const dz* d1a,
+                          const dz* d1b, const dz* d3a, const dz* d3b) {
+  const double fn = double(n);
+  const dz num = (h.z1 * d1a[n] + fn) * (fn - h.z1 * d3a[n - 1]);
+  const dz den = (h.z2 * d1b[n] + fn) * (fn - h.z2 * d3b[n - 1]);
+  return h.xr2 * (num / den);
+}
+
+// Q_n for n = 1..nmax, in place over the factors r_n that q[1..nmax] holds
+// on entry, from Q_0 = (e^{-2i z2} - 1) / (e^{-2i z1} - 1).
+LMB_HD void layered_q_product(const ShellSetup& h, int nmax, dz* q) {
+  dz cur = (dexpi(-2., h.z2) + (-1.)) / (dexpi(-2., h.z1) + (-1.));
+  for (int n = 1; n <= nmax; ++n) {
+    cur = cur * q[n];
+    q[n] = cur;
   }
 }
 
@@ -208,9 +220,10 @@ LMB_HD void layered_shell_update(const ShellSetup& h, int n, const dz* d1a,
 
 // One shell ii >= 1 given the downward D1 at z1 (d1a) and z2 (d1b):
 // upward psi*zeta, D3, Q, and Ha/Hb updated in place for n = 1..nmax, in
-// one serial pass (no scratch).  The same arithmetic as
-// layered_shell_rec + layered_shell_update, which the warp-parallel form
-// uses.
+// one serial pass (no scratch).  The same recurrences as layered_d3_up,
+// layered_q_ratio, layered_q_product and layered_shell_update, which the
+// warp-parallel form uses; Q's factors are grouped differently there, so
+// the two forms agree to rounding.
 LMB_HD void layered_shell_up(const LayeredScalars& s, int ii, const dz* d1a,
                              const dz* d1b, dz* ha, dz* hb) {
   const ShellSetup h = layered_shell_setup(s, ii);
@@ -263,23 +276,24 @@ LMB_HD void layered_coefficient(const LayeredScalars& s, int n, const dz& ha,
   const double pss = psix[n] * x, ps1s = psix[n - 1] * x;
   const zd ze = zeta[n], ze1 = zeta[n - 1];
   const zd zes = x * zetax[n], ze1s = x * zetax[n - 1];
-  const zd im = 1. / m;
+  const zd im = recip(m);
   // a_n: fac = Ha/m + n/x
   const zd fa = ha.v * im + nx;
   const zd fa_s = ha.s * im - nx;          // d(n/x)/ds = -n/x
   const zd fa_m = ha.m * im - ha.v * (im * im);
   const zd numa = fa * ps - ps1, dena = fa * ze - ze1;
-  const zd a = numa / dena;
+  const zd ida = recip(dena);
+  const zd a = numa * ida;
   // b_n: fac = Hb m + n/x
   const zd fb = hb.v * m + nx;
   const zd fb_s = hb.s * m - nx;
   const zd fb_m = hb.m * m + hb.v;
   const zd numb = fb * ps - ps1, denb = fb * ze - ze1;
-  const zd b = numb / denb;
+  const zd idb = recip(denb);
+  const zd b = numb * idb;
   out[0] = a;
   out[1] = b;
   if (dout == 0) return;
-  const zd ida = 1. / dena, idb = 1. / denb;
   const zd a_s = ((fa_s * ps + fa * pss - ps1s) - a * (fa_s * ze + fa * zes - ze1s)) * ida;
   const zd a_m = (fa_m * ps - a * (fa_m * ze)) * ida;
   const zd b_s = ((fb_s * ps + fb * pss - ps1s) - b * (fb_s * ze + fb * zes - ze1s)) * idb;

@@ -99,8 +99,12 @@ static int layered_ab_impl(const double* radii, const double* idx, int L,
     if (split) {
       std::vector<dz> d3a(nm + 2), d3b(nm + 2), q(nm + 2);
       const ShellSetup h = layered_shell_setup(s, ii);
-      layered_shell_rec(s, h, d1a.data(), d1b.data(), d3a.data(), d3b.data(),
-                        q.data());
+      layered_d3_up(h.z1, nm, d1a.data(), d3a.data());
+      layered_d3_up(h.z2, nm, d1b.data(), d3b.data());
+      for (int n = 1; n <= nm; ++n)
+        q[n] = layered_q_ratio(h, n, d1a.data(), d1b.data(), d3a.data(),
+                               d3b.data());
+      layered_q_product(h, nm, q.data());
       ha[0] = dconst(mk(0., 0.));
       hb[0] = dconst(mk(0., 0.));
       for (int n = 1; n <= nm; ++n)

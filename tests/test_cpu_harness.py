@@ -315,14 +315,16 @@ def test_reverse_epilogue_matches_forward(h, shape, p, bohren):
     ([0.5, 1.2, 2.0], [1.4, 1.7, 1.55 + 0.001j]),
     ([0.2, 0.5, 0.9, 1.4, 2.4], [1.35, 1.7, 1.4, 1.6 + 0.003j, 1.5]),
 ])
-def test_layered_split_shell_is_identical(h, radii, idx):
-    '''The split shell functions (upward recurrences stored, then
-    independent per-order updates: the warp-parallel kernel path) give
-    bit-identical coefficients and tangents to the fused serial pass.'''
+def test_layered_split_shell_matches_serial(h, radii, idx):
+    '''The split shell functions of the warp-parallel kernel path (each
+    argument's D3 chain stored, Q's factors per order and their running
+    product, then independent per-order updates) agree with the fused
+    serial pass to rounding: Q's factors are grouped differently, so the
+    two differ by ~1e-15 of the largest coefficient (1e-13 asserted).'''
     a1, d1 = h.layered_ab(radii, idx, 1.34, 0.447, deriv=True)
     a2, d2 = h.layered_ab(radii, idx, 1.34, 0.447, deriv=True, split=True)
-    np.testing.assert_array_equal(a1, a2)
-    np.testing.assert_array_equal(d1, d2)
+    assert np.abs(a2 - a1).max() <= 1e-13 * np.abs(a1).max()
+    assert np.abs(d2 - d1).max() <= 1e-13 * np.abs(d1).max()
 
 
 def test_hologram_error_bound(h):
