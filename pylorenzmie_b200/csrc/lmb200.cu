@@ -259,7 +259,7 @@ int lmb_sphere_ab(const lmb_sphere* spheres, int nspheres, double n_m,
   if (!(wavelength > 0.) || !(n_m > 0.)) return LMB_ERR_ARG;
   const size_t smem = ab_scratch_bytes(nmax_cap + 1);
   LMB_CK(smem_attr((const void*)k_sphere_ab, smem));
-  k_sphere_ab<<<nspheres, 32, smem, as_stream(stream)>>>(
+  k_sphere_ab<<<nspheres, 64, smem, as_stream(stream)>>>(
       spheres, nspheres, n_m, wavelength, nmax_cap, reinterpret_cast<zd*>(ab),
       reinterpret_cast<zd*>(dab), nmax, status);
   LMB_CK(cudaGetLastError());
@@ -277,7 +277,7 @@ int lmb_layered_ab(const double* radii, const double* indices, int nlayers,
   if (!(wavelength > 0.) || !(n_m > 0.)) return LMB_ERR_ARG;
   const size_t smem = layered_scratch_bytes(nmax_cap + 1, nlayers);
   LMB_CK(smem_attr((const void*)k_layered_ab, smem));
-  k_layered_ab<<<nspheres, 32, smem, as_stream(stream)>>>(
+  k_layered_ab<<<nspheres, 64, smem, as_stream(stream)>>>(
       radii, indices, nlayers, nspheres, n_m, wavelength, nmax_cap,
       reinterpret_cast<zd*>(ab), reinterpret_cast<zd*>(dab), nmax, status);
   LMB_CK(cudaGetLastError());
@@ -788,7 +788,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   auto launch_step = [&]() {
     cudaMemsetAsync(c.counters + 1, 0, sizeof(int), st);
     cudaMemsetAsync(c.counters + 4, 0, 2 * sizeof(int), st);  // [4], [5]
-    k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
+    k_fit_step<<<nfeatures, 64, ab_smem, st>>>(c);
     launches += 1;
     ++iterations;
   };
@@ -800,7 +800,7 @@ int fit_batch_impl(const lmb_feature* features, int nfeatures,
   do {
     if (stats && mark() != cudaSuccess) { status = LMB_ERR_CUDA; break; }
     k_fit_setup<<<1, 1024, 0, st>>>(c);
-    k_fit_step<<<nfeatures, 32, ab_smem, st>>>(c);
+    k_fit_step<<<nfeatures, 64, ab_smem, st>>>(c);
     launches += 2;
     if (pipelined) {
       // Round r's counters (and the work totals after them) land in slot

@@ -54,16 +54,38 @@ __device__ inline AbScratch carve_ab_scratch(char* base, int nmaxp) {
   return s;
 }
 
-// Called by all 32 lanes of a warp.  ab: [nmaxp][2] zd, dab: [nmaxp][4] zd
-// (may be null).  Returns the status (uniform over the warp).
-__device__ int warp_sphere_ab(double a_p, double n_p, double k_p, double n_m,
-                              double wavelength, int nmax_cap, AbScratch w,
-                              zd* ab, zd* dab, int* nmax_out) {
-  const int lane = threadIdx.x & 31;
+// Called by all 64 threads of a two-warp block.  ab: [nmaxp][2] zd, dab:
+// [nmaxp][4] zd (may be null).  The serial recurrences are FP64 chains of
+// dependent operations, so their time is latency: warp 0 runs the inside
+// D1 while warp 1 runs the medium's D1 and then its upward psi/zeta, and
+// the two warps interleave (two branches of one warp would run one after
+// the other).  Then warp 0 forms a_n, b_n over the orders.  Both warps pass
+// the one __syncthreads whatever the inputs.  Returns the status on warp 0
+// (uniform over it); warp 1's return value means nothing.
+__device__ int block_sphere_ab(double a_p, double n_p, double k_p, double n_m,
+                               double wavelength, int nmax_cap, AbScratch w,
+                               zd* ab, zd* dab, int* nmax_out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nmaxp = nmax_cap + 1;
   const MieScalars s = mie_setup(a_p, n_p, k_p, n_m, wavelength);
   const bool ok = (s.x > 0.) && (s.x < 1e7) && s.nmax >= 1 &&
                   s.nmax <= nmax_cap && isfinite(s.m.re) && isfinite(s.m.im);
+  if (ok) {
+    if (warp == 0) {
+      for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_inside(s, n, w.nz, w.nz2);
+      __syncwarp();
+      if (lane == 0) mie_d1_inside(s, w.nz, w.nz2, w.d1in, w.d1inz);
+    } else {
+      for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_medium(s, n, w.nx, w.nx2);
+      __syncwarp();
+      if (lane == 0) {
+        mie_d1_medium(s, w.nx, w.nx2, w.d1m, w.d1mx);
+        mie_upward(s, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
+      }
+    }
+  }
+  __syncthreads();
+  if (warp != 0) return LMB_OK;
   if (!ok) {
     for (int n = lane; n < nmaxp; n += 32) {
       ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
@@ -71,18 +93,9 @@ __device__ int warp_sphere_ab(double a_p, double n_p, double k_p, double n_m,
         for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
     }
     if (lane == 0) *nmax_out = (s.nmax >= 0 && s.nmax < (1 << 30)) ? s.nmax : 0;
+    __syncwarp();
     return LMB_ERR_NMAX;
   }
-  for (int n = 1 + lane; n <= s.nmax; n += 32)
-    mie_orders(s, n, w.nz, w.nz2, w.nx, w.nx2);
-  __syncwarp();
-  // the inside and the medium's D1 on lanes 0 and 1, in step
-  if (lane < 2)
-    mie_d1_both(s, lane, w.nz, w.nz2, w.nx, w.nx2, w.d1in, w.d1inz, w.d1m, w.d1mx);
-  __syncwarp();
-  if (lane == 0)
-    mie_upward(s, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
-  __syncwarp();
   for (int n = lane; n < nmaxp; n += 32) {
     if (n == 0 || n > s.nmax) {
       ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
@@ -103,6 +116,7 @@ __device__ int warp_sphere_ab(double a_p, double n_p, double k_p, double n_m,
   return LMB_OK;
 }
 
+// One two-warp block (64 threads) per sphere.
 __global__ void k_sphere_ab(const lmb_sphere* spheres, int n, double n_m,
                             double wavelength, int nmax_cap, zd* ab, zd* dab,
                             int* nmax, int* status) {
@@ -112,18 +126,15 @@ __global__ void k_sphere_ab(const lmb_sphere* spheres, int n, double n_m,
   const int nmaxp = nmax_cap + 1;
   AbScratch w = carve_ab_scratch(smem, nmaxp);
   const lmb_sphere sp = spheres[i];
-  const int st = warp_sphere_ab(sp.a_p, sp.n_p, sp.k_p, n_m, wavelength,
-                                nmax_cap, w, ab + size_t(i) * nmaxp * 2,
-                                dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
-                                nmax + i);
+  const int st = block_sphere_ab(sp.a_p, sp.n_p, sp.k_p, n_m, wavelength,
+                                 nmax_cap, w, ab + size_t(i) * nmaxp * 2,
+                                 dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
+                                 nmax + i);
   if (threadIdx.x == 0) status[i] = st;
 }
 
 // ---------------------------------------------------------------------------
-// Multilayer spheres: one warp per sphere.  Lane 0 runs the core and the
-// shells' upward recurrences, lanes 0/1 the two downward D1 recurrences of
-// each shell, lane 1 the medium's recurrences meanwhile; then all lanes form
-// a_n, b_n over n.
+// Multilayer spheres: one two-warp block per sphere (block_layered_ab).
 
 __host__ __device__ inline size_t layered_scratch_serial_bytes(int nmaxp) {
   return 4 * size_t(nmaxp + 1) * sizeof(dz) + ab_scratch_bytes(nmaxp);
@@ -147,11 +158,16 @@ __host__ __device__ inline size_t layered_scratch_bytes(int nmaxp, int L) {
                                     : layered_scratch_serial_bytes(nmaxp);
 }
 
-// radii [L] ascending (um), idx [L][2] (re, im), core first.
-__device__ int warp_layered_ab(const double* radii, const double* idx, int L,
-                               double n_m, double wavelength, int nmax_cap,
-                               char* scratch, zd* ab, zd* dab, int* nmax_out) {
-  const int lane = threadIdx.x & 31;
+// radii [L] ascending (um), idx [L][2] (re, im), core first.  Called by all
+// 64 threads of a two-warp block.  Warp 1 runs the medium's recurrences
+// (D1, then upward psi/zeta) while warp 0 runs the layers' and their Ha/Hb;
+// the two warps interleave.  Then warp 0 forms a_n, b_n over the orders.
+// Both warps pass the one __syncthreads whatever the inputs.  Returns the
+// status on warp 0 (uniform over it); warp 1's return value means nothing.
+__device__ int block_layered_ab(const double* radii, const double* idx, int L,
+                                double n_m, double wavelength, int nmax_cap,
+                                char* scratch, zd* ab, zd* dab, int* nmax_out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nmaxp = nmax_cap + 1;
   bool ok = L >= 1 && L <= LMB_MAX_LAYERS;
   for (int l = 0; ok && l < L; ++l)
@@ -162,46 +178,35 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     s = layered_setup(radii, idx, L, n_m, wavelength);
     ok = s.nmax >= 1 && s.nmax <= nmax_cap && s.x[L - 1] < 1e7;
   }
-  if (!ok) {
-    for (int n = lane; n < nmaxp; n += 32) {
-      ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
-      if (dab)
-        for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
-    }
-    if (lane == 0) *nmax_out = 0;
-    __syncwarp();
-    return LMB_ERR_NMAX;
-  }
-  MieScalars med;
-  med.k = s.k;
-  med.x = s.x[L - 1];
-  med.n_m = n_m;
-  med.m = s.m[L - 1];
-  med.nmax = s.nmax;
   const size_t na = size_t(nmaxp + 1);
-  dz* ha;
-  dz* hb;
-  AbScratch w;
-  if (layered_parallel(nmaxp, L)) {
-    // Warp-parallel: all downward recurrences on lanes of their own
-    // (core, medium and two per shell), then each shell argument's upward
-    // D3 chain on a lane of its own, then Q's factors over the orders and
-    // their running products one lane per shell, then the shells in order
-    // with their Ha/Hb updates spread over the orders.  The same
-    // recurrences as the serial form below.
-    dz* d1c = reinterpret_cast<dz*>(scratch);
-    dz* sh = d1c + na;  // shell ii: d1a, d1b, d3a, d3b, q at sh + 5 (ii-1) na
-    ha = sh + 5 * (L - 1) * na;
-    hb = ha + na;
-    w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
+  const bool par = layered_parallel(nmaxp, L);
+  // parallel form: the core's D1, then shell ii's d1a, d1b, d3a, d3b, q at
+  // sh + 5 (ii-1) na; serial form: d1a, d1b.  Then Ha, Hb, the medium's.
+  dz* d1c = reinterpret_cast<dz*>(scratch);
+  dz* sh = d1c + na;
+  dz* ha = par ? sh + 5 * (L - 1) * na : d1c + 2 * na;
+  dz* hb = ha + na;
+  const AbScratch w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
+  if (ok && warp == 1) {
+    MieScalars med;
+    med.k = s.k;
+    med.x = s.x[L - 1];
+    med.n_m = n_m;
+    med.m = s.m[L - 1];
+    med.nmax = s.nmax;
     for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_medium(med, n, w.nx, w.nx2);
     __syncwarp();
-    if (lane == 1) {
+    if (lane == 0) {
       mie_d1_medium(med, w.nx, w.nx2, w.d1m, w.d1mx);
       mie_upward(med, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
-    } else if (lane < 2 * L) {
-      // the core (lane 0) and each shell's two arguments (lanes 2..2L-1):
-      // one code path, so these recurrences run in step across the lanes
+    }
+  } else if (ok && par) {
+    // Each phase on one code path across the lanes: the downward D1 chains
+    // of the core (lane 0) and of both arguments of each shell (lanes
+    // 1..2L-2); each shell argument's upward D3 chain (lanes 0..2L-3); Q's
+    // factors over (shell, order) pairs and their running products one lane
+    // per shell; the shells in order, their Ha/Hb updates over the orders.
+    if (lane < 2 * L - 1) {
       dz z;
       dz* out;
       if (lane == 0) {
@@ -210,7 +215,7 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
         z.m = (L == 1) ? mk(s.x[0], 0.) : mk(0., 0.);
         out = d1c;
       } else {
-        const int ii = (lane - 2) / 2 + 1, which = (lane - 2) & 1;
+        const int ii = (lane - 1) / 2 + 1, which = (lane - 1) & 1;
         const bool outer = ii == L - 1;
         const double xx = which == 0 ? s.x[ii] : s.x[ii - 1];
         z.v = xx * s.m[ii];
@@ -222,8 +227,6 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     }
     __syncwarp();
     if (lane < 2 * (L - 1)) {
-      // each shell argument's upward psi*zeta and D3 chain on a lane of its
-      // own, one code path
       const int ii = lane / 2 + 1, which = lane & 1;
       const ShellSetup h = layered_shell_setup(s, ii);
       dz* b = sh + 5 * (ii - 1) * na;
@@ -235,7 +238,6 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
       hb[n] = d1c[n];
     }
     __syncwarp();
-    // the factors of every shell's Q, over (shell, order) pairs
     for (int j = lane; j < (L - 1) * s.nmax; j += 32) {
       const int ii = j / s.nmax + 1, n = j - (ii - 1) * s.nmax + 1;
       dz* b = sh + 5 * (ii - 1) * na;
@@ -259,19 +261,11 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
                              ha, hb);
       __syncwarp();
     }
-  } else {
-    dz* d1a = reinterpret_cast<dz*>(scratch);
-    dz* d1b = d1a + na;
-    ha = d1b + na;
-    hb = ha + na;
-    w = carve_ab_scratch(reinterpret_cast<char*>(hb + na), nmaxp);
-    for (int n = 1 + lane; n <= s.nmax; n += 32) mie_orders_medium(med, n, w.nx, w.nx2);
-    __syncwarp();
+  } else if (ok) {
+    // serial form, for scratch too large for the parallel one
+    dz* d1a = d1c;
+    dz* d1b = d1c + na;
     if (lane == 0) layered_core(s, d1a, ha, hb);
-    if (lane == 1) {
-      mie_d1_medium(med, w.nx, w.nx2, w.d1m, w.d1mx);
-      mie_upward(med, w.nx, w.nx2, w.d1m, w.d1mx, w.psi, w.psix, w.zeta, w.zetax);
-    }
     __syncwarp();
     for (int ii = 1; ii < L; ++ii) {
       const bool outer = ii == L - 1;
@@ -288,8 +282,10 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
       __syncwarp();
     }
   }
+  __syncthreads();
+  if (warp != 0) return LMB_OK;
   for (int n = lane; n < nmaxp; n += 32) {
-    if (n == 0 || n > s.nmax) {
+    if (!ok || n == 0 || n > s.nmax) {
       ab[2 * n] = ab[2 * n + 1] = mk(0., 0.);
       if (dab)
         for (int j = 0; j < 4; ++j) dab[4 * n + j] = mk(0., 0.);
@@ -303,11 +299,12 @@ __device__ int warp_layered_ab(const double* radii, const double* idx, int L,
     if (dab)
       for (int j = 0; j < 4; ++j) dab[4 * n + j] = dout[j];
   }
-  if (lane == 0) *nmax_out = s.nmax;
+  if (lane == 0) *nmax_out = ok ? s.nmax : 0;
   __syncwarp();
-  return LMB_OK;
+  return ok ? LMB_OK : LMB_ERR_NMAX;
 }
 
+// One two-warp block (64 threads) per sphere.
 __global__ void k_layered_ab(const double* radii, const double* indices, int L,
                              int n, double n_m, double wavelength, int nmax_cap,
                              zd* ab, zd* dab, int* nmax, int* status) {
@@ -315,11 +312,11 @@ __global__ void k_layered_ab(const double* radii, const double* indices, int L,
   const int i = blockIdx.x;
   if (i >= n) return;
   const int nmaxp = nmax_cap + 1;
-  const int st = warp_layered_ab(radii + size_t(i) * L, indices + size_t(i) * L * 2,
-                                 L, n_m, wavelength, nmax_cap, smem,
-                                 ab + size_t(i) * nmaxp * 2,
-                                 dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
-                                 nmax + i);
+  const int st = block_layered_ab(radii + size_t(i) * L, indices + size_t(i) * L * 2,
+                                  L, n_m, wavelength, nmax_cap, smem,
+                                  ab + size_t(i) * nmaxp * 2,
+                                  dab ? dab + size_t(i) * nmaxp * 4 : (zd*)0,
+                                  nmax + i);
   if (threadIdx.x == 0) status[i] = st;
 }
 
@@ -1452,20 +1449,18 @@ k_fit_eval_warp(FitCtx c) {
   }
 }
 
-// One warp per feature: gather sums, advance the LM state machine, and
-// compute the Mie coefficients of the next evaluation point.
-__global__ void __launch_bounds__(32)
-k_fit_step(FitCtx c) {
-  extern __shared__ __align__(16) char smem[];
-  __shared__ double s_p[6];
-  __shared__ int s_need;
-  const int f = blockIdx.x;
-  const int lane = threadIdx.x;
-  if (f >= c.nf) return;
-  if (c.counters[3]) return;  // tile table overflow: nothing ran
+// Warp 0 of k_fit_step: gather the feature's sums, advance the LM state
+// machine, and write the next evaluation point to p (lane 0).  Returns,
+// uniformly over the warp, whether that point's Mie coefficients are needed:
+// 0 for a finished, withdrawn or not yet admitted feature.  *phase gets the
+// phase the feature was in.
+__device__ __forceinline__ int fit_step_advance(const FitCtx& c, int f, int lane, double* p,
+                                                int* phase_out) {
+  if (c.counters[3]) return 0;  // tile table overflow: nothing ran
   LMState* gs = c.state + f;
   const int phase = gs->phase;
-  if (phase == LM_PHASE_DONE) return;
+  *phase_out = phase;
+  if (phase == LM_PHASE_DONE) return 0;
   if (phase == LM_PHASE_INIT && c.ready) {
     // one read for the whole warp: the flag may change while we look
     int r = 0;
@@ -1477,21 +1472,19 @@ k_fit_step(FitCtx c) {
         gs->info = -4;
         c.ev[f].active = 0;
       }
-      return;
+      return 0;
     }
     if (f >= r) {
       if (lane == 0) atomicAdd(c.counters + 4, 1);
-      return;
+      return 0;
     }
   }
-  const int nmaxp = c.nmax_cap + 1;
-  if (lane == 0) {
-    s_need = 0;
-    if (phase == LM_PHASE_INIT) {
-      for (int j = 0; j < 6; ++j) s_p[j] = c.base[f * 6 + j];
-      s_need = 1;
-    }
+  if (phase == LM_PHASE_INIT) {
+    if (lane == 0)
+      for (int j = 0; j < 6; ++j) p[j] = c.base[f * 6 + j];
+    return 1;
   }
+  int need = 0;
   if (phase == LM_PHASE_FIRST || phase == LM_PHASE_TRIAL) {
     double v[FIT_NSUM];
     for (int j = 0; j < FIT_NSUM; ++j) v[j] = 0.;
@@ -1514,37 +1507,65 @@ k_fit_step(FitCtx c) {
         c.ev[f].active = 0;
       } else {
         s.phase = LM_PHASE_TRIAL;
-        for (int j = 0; j < 6; ++j) s_p[j] = c.base[f * 6 + j];
-        for (int a = 0; a < s.n; ++a) s_p[s.slot[a]] = s.x[a] + s.p[a];
-        s_need = 1;
+        for (int j = 0; j < 6; ++j) p[j] = c.base[f * 6 + j];
+        for (int a = 0; a < s.n; ++a) p[s.slot[a]] = s.x[a] + s.p[a];
+        need = 1;
       }
       *gs = s;
     }
+    need = __shfl_sync(0xffffffffu, need, 0);
   }
-  __syncwarp();
-  if (!s_need) return;
-  int st;
-  if (c.nlayers > 1) {
-    __shared__ double s_r[LMB_MAX_LAYERS], s_i[2 * LMB_MAX_LAYERS];
+  return need;
+}
+
+// One two-warp block per feature: warp 0 gathers the sums and advances the
+// LM state machine; then both warps compute the Mie coefficients of the
+// next evaluation point (block_sphere_ab, block_layered_ab) and stage their
+// records, and warp 0 lists the feature's tiles.  Both warps pass every
+// __syncthreads on every path.
+__global__ void __launch_bounds__(64)
+k_fit_step(FitCtx c) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ double s_p[6];
+  __shared__ double s_r[LMB_MAX_LAYERS], s_i[2 * LMB_MAX_LAYERS];
+  __shared__ int s_need, s_st;
+  const int f = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (f >= c.nf) return;  // the whole block
+  LMState* gs = c.state + f;
+  int phase = LM_PHASE_DONE;
+  if (warp == 0) {
+    const int need = fit_step_advance(c, f, lane, s_p, &phase);
+    __syncwarp();
     const int L = c.nlayers;
-    if (lane < L) {
+    if (need && L > 1 && lane < L) {
       const bool outer = lane == L - 1;
       s_r[lane] = outer ? s_p[3] : c.layer_frac[size_t(f) * (L - 1) + lane] * s_p[3];
       s_i[2 * lane] = outer ? s_p[4] : c.layer_index[(size_t(f) * (L - 1) + lane) * 2];
       s_i[2 * lane + 1] =
           outer ? s_p[5] : c.layer_index[(size_t(f) * (L - 1) + lane) * 2 + 1];
     }
-    __syncwarp();
-    st = warp_layered_ab(s_r, s_i, L, c.n_m, c.wavelength, c.nmax_cap, smem,
-                         c.ab + size_t(f) * nmaxp * 2, c.dab + size_t(f) * nmaxp * 4,
-                         c.nmax + f);
+    if (lane == 0) s_need = need;
+  }
+  __syncthreads();  // both warps, on every path
+  if (!s_need) return;
+  const int nmaxp = c.nmax_cap + 1;
+  int st;
+  if (c.nlayers > 1) {
+    st = block_layered_ab(s_r, s_i, c.nlayers, c.n_m, c.wavelength, c.nmax_cap,
+                          smem, c.ab + size_t(f) * nmaxp * 2,
+                          c.dab + size_t(f) * nmaxp * 4, c.nmax + f);
   } else {
     AbScratch w = carve_ab_scratch(smem, nmaxp);
-    st = warp_sphere_ab(s_p[3], s_p[4], s_p[5], c.n_m, c.wavelength, c.nmax_cap,
-                        w, c.ab + size_t(f) * nmaxp * 2, c.dab + size_t(f) * nmaxp * 4,
-                        c.nmax + f);
+    st = block_sphere_ab(s_p[3], s_p[4], s_p[5], c.n_m, c.wavelength, c.nmax_cap,
+                         w, c.ab + size_t(f) * nmaxp * 2, c.dab + size_t(f) * nmaxp * 4,
+                         c.nmax + f);
   }
-  if (st == LMB_OK) {
+  // warp 0's status, a_n, b_n (global) and n_max for both warps, which
+  // stage the records together
+  if (threadIdx.x == 0) s_st = st;
+  __syncthreads();
+  if (s_st == LMB_OK) {
     const zd* abf = c.ab + size_t(f) * nmaxp * 2;
     const zd* dabf = c.dab + size_t(f) * nmaxp * 4;
     const int nm = min(c.nmax[f], nmaxp - 1);
@@ -1554,6 +1575,7 @@ k_fit_step(FitCtx c) {
     else
       stage_coef<float, true>(abf, dabf, nm, c.coef32 + size_t(f) * nmaxp * JAC_QUADS);
   }
+  if (warp != 0) return;
   int base = -1;
   const int tb = c.tile_begin[f], nt = c.tile_begin[f + 1] - tb;
   if (lane == 0) {

@@ -63,20 +63,18 @@ LMB_HD MieScalars mie_setup(double a_p, double n_p, double k_p, double n_m,
   return s;
 }
 
-// Per-order quotients of the recurrences for order n (1 <= n <= nmax):
-// nz = n/z, nz2 = n/z^2 with z = m x (inside), nx = n/x, nx2 = n/x^2
-// (medium).  Off the recurrences' chains, so a warp forms them in parallel.
-LMB_HD void mie_orders(const MieScalars& s, int n, zd* nz, zd* nz2, double* nx,
-                       double* nx2) {
+
+// Per-order quotients of the recurrences for order n (1 <= n <= nmax), off
+// the recurrences' chains, so that a warp forms them in parallel: inside,
+// nz = n/z and nz2 = n/z^2 with z = m x.
+LMB_HD void mie_orders_inside(const MieScalars& s, int n, zd* nz, zd* nz2) {
   const zd z = s.x * s.m;
   const zd z2 = z * z;
   nz[n] = double(n) / z;
   nz2[n] = double(n) / z2;
-  nx[n] = double(n) / s.x;
-  nx2[n] = nx[n] / s.x;
 }
 
-// The medium's quotients only (nx, nx2), for the multilayer medium.
+// The medium's: nx = n/x, nx2 = n/x^2.
 LMB_HD void mie_orders_medium(const MieScalars& s, int n, double* nx,
                               double* nx2) {
   nx[n] = double(n) / s.x;
@@ -99,42 +97,24 @@ LMB_HD void mie_d1_medium(const MieScalars& s, const double* nx,
   }
 }
 
-// Upward psi (real), zeta, with d/dx; needs the medium D1.
-// Both downward D1 recurrences (D1(m x) inside, complex; D1(x) in the
-// medium, real) through one code path: which = 0 runs the inside one,
-// which = 1 the medium's in complex arithmetic with zero imaginary part
-// (which stays exactly zero; the real part differs from mie_d1_medium's by
-// the rounding of the reciprocal).  On lanes 0 and 1 of a warp the two
-// chains then run in step instead of one after the other, as divergent
-// branches would.
-LMB_HD void mie_d1_both(const MieScalars& s, int which, const zd* nz,
-                        const zd* nz2, const double* nx, const double* nx2,
-                        zd* d1in, zd* d1inz, double* d1m, double* d1mx) {
+// D1(m x) inside the sphere, with dD1/dz at z = m x: the zero-start
+// downward recurrence from n_max (Sphere.py), complex.
+LMB_HD void mie_d1_inside(const MieScalars& s, const zd* nz, const zd* nz2,
+                          zd* d1in, zd* d1inz) {
   zd d = mk(0., 0.), dz = mk(0., 0.);
-  if (which == 0) {
-    d1in[s.nmax] = d;
-    d1inz[s.nmax] = dz;
-  } else {
-    d1m[s.nmax] = 0.;
-    d1mx[s.nmax] = 0.;
-  }
+  d1in[s.nmax] = d;
+  d1inz[s.nmax] = dz;
   for (int n = s.nmax; n > 0; --n) {
-    const zd q = which == 0 ? nz[n] : mk(nx[n], 0.);
-    const zd q2 = which == 0 ? nz2[n] : mk(nx2[n], 0.);
-    const zd inv = recip(d + q);
-    const zd dw = dz - q2;
-    d = q - inv;
-    dz = (inv * inv) * dw - q2;
-    if (which == 0) {
-      d1in[n - 1] = d;
-      d1inz[n - 1] = dz;
-    } else {
-      d1m[n - 1] = d.re;
-      d1mx[n - 1] = dz.re;
-    }
+    const zd inv = recip(d + nz[n]);
+    const zd dw = dz - nz2[n];
+    d = nz[n] - inv;
+    dz = (inv * inv) * dw - nz2[n];
+    d1in[n - 1] = d;
+    d1inz[n - 1] = dz;
   }
 }
 
+// Upward psi (real), zeta, with d/dx; needs the medium D1.
 LMB_HD void mie_upward(const MieScalars& s, const double* nxs,
                        const double* nx2s, const double* d1, const double* d1x,
                        double* psi, double* psix, zd* zeta, zd* zetax) {

@@ -32,11 +32,12 @@ API int h_sphere_ab(double a_p, double n_p, double k_p, double n_m, double lam,
       psix(s.nmax + 1);
   std::vector<zd> nz(s.nmax + 1), nz2(s.nmax + 1);
   std::vector<double> nx(s.nmax + 1), nx2(s.nmax + 1);
-  for (int n = 1; n <= s.nmax; ++n)
-    mie_orders(s, n, nz.data(), nz2.data(), nx.data(), nx2.data());
-  for (int which = 0; which < 2; ++which)  // as the kernel's lanes 0 and 1
-    mie_d1_both(s, which, nz.data(), nz2.data(), nx.data(), nx2.data(),
-                d1in.data(), d1inz.data(), d1m.data(), d1mx.data());
+  for (int n = 1; n <= s.nmax; ++n) {  // as the kernel's two warps
+    mie_orders_inside(s, n, nz.data(), nz2.data());
+    mie_orders_medium(s, n, nx.data(), nx2.data());
+  }
+  mie_d1_inside(s, nz.data(), nz2.data(), d1in.data(), d1inz.data());
+  mie_d1_medium(s, nx.data(), nx2.data(), d1m.data(), d1mx.data());
   mie_upward(s, nx.data(), nx2.data(), d1m.data(), d1mx.data(), psi.data(),
              psix.data(), zeta.data(), zetax.data());
   memset(ab, 0, sizeof(double) * 4 * (cap + 1));
