@@ -452,12 +452,17 @@ k_field(const double* __restrict__ coords, long long npts,
 
 // FP64 re-summation, inside k_field_pair<true>, of the block's pixels whose
 // FP32 error bound exceeded HOLO_TOL (mark0/mark1: the thread's two
-// pixels).  One warp per marked pixel and one lane per particle, so that a
-// pixel's particles run their FP64 recurrences side by side; the particles
-// go in groups of `group` (<= 32), whose FP64 records (2 Quad<double> per
-// order, nmaxp orders per slot) are staged in smem after the marked-pixel
-// list and the FP64 field accumulators.  Lanes are combined by a fixed
-// shuffle tree and groups in order, so the result does not depend on
+// pixels).  The particles go in groups of `group` (<= 32), whose FP64
+// records (2 Quad<double> per order, nmaxp orders per slot) are staged in
+// smem after the marked-pixel list and the FP64 field accumulators.  Two
+// ways to spread the work, chosen per block by their cost in order steps:
+// - few marked pixels: one warp per marked pixel and one lane per particle,
+//   so that a pixel's particles run their recurrences side by side (lanes
+//   combined by a fixed shuffle tree);
+// - many marked pixels, or few particles (large spheres mark most pixels):
+//   one thread per marked pixel, its particles in order.
+// The choice depends only on the marked count and the particles' n_max,
+// and groups are summed in order, so the result does not depend on
 // scheduling.  Every thread of the block calls this.
 __device__ void holo_resum64(bool mark0, long long q0, bool mark1, long long q1,
                              long long base, char* smem, int group,
@@ -481,6 +486,21 @@ __device__ void holo_resum64(bool mark0, long long q0, bool mark1, long long q1,
   const bool bohren = flags & LMB_BOHREN;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
+  // order steps of each way: a warp per pixel waits for its group's
+  // largest n_max; a thread per pixel walks every particle's orders
+  long long by_lane = 0, by_thread = 0;
+  for (int g0 = pb; g0 < pe; g0 += group) {
+    int mx = 0;
+    long long sum = 0;
+    for (int j = g0; j < min(g0 + group, pe); ++j) {
+      const int nm = min(max(nmax[j], 0), nmaxp - 1);
+      mx = max(mx, nm);
+      sum += nm;
+    }
+    by_lane += (long long)((F + nwarps - 1) / nwarps) * mx;
+    by_thread += (long long)((F + int(blockDim.x) - 1) / int(blockDim.x)) * sum;
+  }
+  const bool per_thread = by_thread < by_lane;
   for (int g0 = pb; g0 < pe; g0 += group) {
     const int G = min(group, pe - g0);
     __syncthreads();  // the previous group's records are no longer read
@@ -490,6 +510,35 @@ __device__ void holo_resum64(bool mark0, long long q0, bool mark1, long long q1,
                                 rec + size_t(j) * 2 * nmaxp);
     }
     __syncthreads();
+    if (per_thread) {
+      for (int f = threadIdx.x; f < F; f += blockDim.x) {
+        const long long pix = base + list[f];
+        const double x = coords[pix], y = coords[npts + pix], z = coords[2 * npts + pix];
+        cplx<double> e[3];
+        for (int c = 0; c < 3; ++c) e[c] = mk(acc[6 * f + 2 * c], acc[6 * f + 2 * c + 1]);
+        for (int j = 0; j < G; ++j) {
+          const int p = g0 + j;
+          const int nm = min(max(nmax[p], 0), nmaxp - 1);
+          const lmb_sphere sp = spheres[p];
+          const Geometry<double> g =
+              geometry<double>(k, x - sp.x_p, y - sp.y_p, z - sp.z_p, z, sp.z_p, bohren);
+          const Sums<double> sm = order_sum<double>(g, rec + size_t(j) * 2 * nmaxp, nm);
+          cplx<double> ep[3];
+          epilogue<double>(g, sm, cart, ep);
+          if (aberr != 0.) {
+            const cplx<double> ph =
+                aberration_phase<double>(aberr, x - sp.x_p, y - sp.y_p, sp.z_p);
+            for (int c = 0; c < 3; ++c) ep[c] = ph * ep[c];
+          }
+          for (int c = 0; c < 3; ++c) e[c] = e[c] + ep[c];
+        }
+        for (int c = 0; c < 3; ++c) {
+          acc[6 * f + 2 * c] = e[c].re;
+          acc[6 * f + 2 * c + 1] = e[c].im;
+        }
+      }
+      continue;
+    }
     for (int f = warp; f < F; f += nwarps) {
       const long long pix = base + list[f];
       cplx<double> e[3];

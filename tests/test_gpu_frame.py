@@ -122,3 +122,29 @@ def test_fit_mixed_large_crops_vs_oracle():
         for k, t in tol.items():
             assert abs(df[k][i] - oracle[i][k]) <= t, (i, k)
         assert abs(df['redchi'][i] / oracle[i]['redchi'] - 1) < 1e-3
+
+
+@pytest.mark.parametrize('spheres_um', [(12.,), (6., 9.), (24.,)])
+def test_large_spheres_resum_per_thread(spheres_um):
+    '''One or two large spheres (n_max 120-490): their error bound marks
+    most pixels, and with so few particles the FP64 re-sum takes one thread
+    per marked pixel rather than one lane per particle.  Every pixel stays
+    within 2e-5 of the FP64 kernel, and the FP64 kernel matches the oracle
+    on sampled pixels.'''
+    from pylorenzmie_b200 import LorenzMie, workloads
+    shape = (384, 448)
+    P = np.zeros((len(spheres_um), 6))
+    for i, a in enumerate(spheres_um):
+        P[i] = [130. + 180. * i, 190. - 20. * i, a / 0.048 + 40., a, 1.45, 0.]
+    spheres = workloads.spheres(P)
+    coords = LorenzMie.meshgrid(shape)
+    h32 = LorenzMie(coordinates=coords, particle=spheres).hologram()
+    h64 = LorenzMie(coordinates=coords, particle=spheres,
+                    double_precision=True).hologram()
+    assert np.all(np.abs(h32 - h64) <= 2e-5)
+    rng = np.random.default_rng(3)
+    idx = np.union1d(rng.choice(coords.shape[1], 400, replace=False),
+                     np.argsort(h64)[-20:])
+    ref = ofield.hologram(coords[:, idx], [dict(zip(KEYS, p)) for p in P],
+                          ofield.DEFAULT_INSTRUMENT)
+    assert np.abs(h64[idx] - ref).max() <= 1e-9
