@@ -254,14 +254,66 @@ def _run_frame(repeat, fp64=False):
         print(f'frame {rep}: {(time.perf_counter() - t0) * 1e3:.3f} ms')
 
 
+# 1280x1024 frames of spheres of one size each (radius um, count), at
+# z = a_p / 0.048 + 60 px: the bench's frame, then sizes that make the FP64
+# re-sum of the FP32 kernel mark few or most pixels
+FRAME_SIZES = ((1.0, 16), (3.0, 16), (6.0, 4), (12.0, 2), (24.0, 1),
+               (1.0, 64))
+
+
+def size_frame(a_p, count, shape=(1024, 1280), seed=1):
+    '''Sphere parameters (count, 6): radius a_p (um), n_p 1.5, at
+    z = a_p / 0.048 + 60 px, uniform over the frame.'''
+    rng = np.random.default_rng(seed)
+    p = np.zeros((count, 6))
+    p[:, 3] = a_p
+    p[:, 4] = 1.5
+    p[:, 2] = a_p / 0.048 + 60.
+    p[:, 0] = rng.uniform(0, shape[1], count)
+    p[:, 1] = rng.uniform(0, shape[0], count)
+    return p
+
+
+def _run_frame_sizes(repeat):
+    '''Median CUDA-event milliseconds of LorenzMie.hologram(device=True) for
+    the bench frame and each FRAME_SIZES frame.'''
+    import torch
+    from .theory import LorenzMie, Instrument
+    from .theory import _kernels as K
+    inst = Instrument()
+    cases = [('bench frame', bench_frame())]
+    cases += [(f'{n} x {a} um', size_frame(a, n)) for a, n in FRAME_SIZES]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for name, p in cases:
+        m = LorenzMie(coordinates=LorenzMie.meshgrid((1024, 1280)),
+                      particle=spheres(p), instrument=inst)
+        for _ in range(3):
+            m.hologram(device=True)
+        ts = []
+        for _ in range(max(repeat, 1)):
+            torch.cuda.synchronize()
+            e0.record()
+            m.hologram(device=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        nmax = K.wiscombe_yang(p[:, 3], p[:, 4], p[:, 5], inst.n_m,
+                               inst.wavelength)
+        print(f'{name:14s} sum_nmax {int(nmax.sum()):5d} '
+              f'{float(np.median(ts)):8.3f} ms')
+
+
 if __name__ == '__main__':
     # python -m pylorenzmie_b200.workloads estimate_frame [--device-search]
     #     [--optimize]
     # python -m pylorenzmie_b200.workloads frame [--fp64]
+    # python -m pylorenzmie_b200.workloads frame_sizes [--repeat N]
     # runs one workload through the public API, e.g. under a profiler
     import argparse
     ap = argparse.ArgumentParser()
-    ap.add_argument('workload', choices=['estimate_frame', 'frame'])
+    ap.add_argument('workload', choices=['estimate_frame', 'frame',
+                                         'frame_sizes'])
     ap.add_argument('--device-search', action='store_true')
     ap.add_argument('--repeat', type=int, default=2)
     ap.add_argument('--optimize', action='store_true')
@@ -269,5 +321,7 @@ if __name__ == '__main__':
     a = ap.parse_args()
     if a.workload == 'frame':
         _run_frame(a.repeat, a.fp64)
+    elif a.workload == 'frame_sizes':
+        _run_frame_sizes(a.repeat)
     else:
         _run_estimate_frame(a.device_search, a.repeat, a.optimize)
