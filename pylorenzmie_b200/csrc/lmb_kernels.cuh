@@ -26,7 +26,7 @@
 namespace lmb {
 
 // ---------------------------------------------------------------------------
-// Mie coefficients: one warp per sphere.
+// Mie coefficients: one two-warp block per sphere.
 
 struct AbScratch {
   zd *d1in, *d1inz, *zeta, *zetax, *nz, *nz2;

@@ -117,7 +117,7 @@ LMB_HD void layered_d1_down(dz z, int nmax, dz* d) {
 // Ha, Hb of the outermost layer after the core and all shells.
 //   d1a, d1b: scratch of nmax+1 duals each; ha, hb: nmax+1 duals (output)
 // Runs on one thread; with two lanes available the caller may split the
-// two downward recurrences (see warp_layered_ab).
+// two downward recurrences (see block_layered_ab).
 LMB_HD void layered_core(const LayeredScalars& s, dz* d1a, dz* ha, dz* hb) {
   const int L = s.L;
   dz z1;
