@@ -569,10 +569,12 @@ int lmb_fit_batch_streamed(const lmb_feature *features, int nfeatures,
  * or other allocating routine and takes no stats.
  *
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  The fit runs the synchronous round loop: it
- * reads the round counters back and waits for the stream every round, and
- * returns only when the stream has drained, errors included.  Requests
+ * (cudaGetSymbolAddress, with that device current).  The fit runs the
+ * synchronous round loop: it reads the round counters back and waits for
+ * the stream every round, and returns only when the stream has drained,
+ * errors included.  So no call, the first or any later one, may be made
+ * while the stream (or, in global capture mode, any stream) is being
+ * captured into a graph.  Requests
  * whose lmb_fit_workspace_bytes exceed LMB_FIT_NOALLOC_SCRATCH_BYTES are
  * rejected with LMB_ERR_WORKSPACE before anything is launched; check
  * lmb_fit_workspace_bytes(n, pixels, nmax_cap) against it.  For 201x201
