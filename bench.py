@@ -62,8 +62,43 @@ def dist_env():
 # ---------------------------------------------------------------------------
 # CPU side: the reference algorithm (oracle) on the host cores
 
-def cpu_fit_rate(nfeat, seed=0):
-    '''features/s of the oracle fit over a spawn pool of all host cores.'''
+def _reference_fit_201(data, start):
+    '''One 201x201 fit by the reference's own Optimizer, installed in
+    baseline/_ref: its numpy LorenzMie (theory/LorenzMie.py) and
+    scipy least_squares with the forward-difference Jacobian
+    (analysis/Optimizer.py:196-222), default variables and settings.
+    Returns the fitted values and success, or None without the install.'''
+    import types
+    import numpy as np
+    ref = ROOT / 'baseline' / '_ref'
+    if not (ref / 'pylorenzmie').is_dir():
+        return None
+    if str(ref) not in sys.path:
+        sys.path.insert(0, str(ref))
+    sys.modules.setdefault('trackpy', types.ModuleType('trackpy'))
+    from pylorenzmie.theory.LorenzMie import LorenzMie as RefLorenzMie
+    from pylorenzmie.theory import Sphere as RefSphere
+    from pylorenzmie.theory import Instrument as RefInstrument
+    from pylorenzmie.analysis.Optimizer import Optimizer as RefOptimizer
+    from pylorenzmie.analysis.Hologram import Hologram as RefHologram
+    inst = RefInstrument()
+    inst.magnification, inst.wavelength, inst.n_m = 0.048, 0.447, 1.340
+    part = RefSphere()
+    part.r_p = list(start[:3])
+    part.a_p, part.n_p, part.k_p = start[3], start[4], start[5]
+    model = RefLorenzMie(particle=part, instrument=inst)
+    opt = RefOptimizer(model=model)
+    r = opt.optimize(RefHologram(np.asarray(data).reshape(201, 201)))
+    keys = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')
+    return {**{k: float(r[k]) for k in keys}, 'success': bool(r['success'])}
+
+
+def cpu_fit_rate(nfeat, seed=0, reference=False):
+    '''features/s of the oracle fit over a spawn pool of all host cores.
+    With reference, the reference's own Optimizer (baseline/_ref) also fits
+    the same crops in the same pool; its rate and its largest parameter
+    differences from the oracle's fits are returned as a fifth item (None
+    without the install).'''
     import multiprocessing as mp
     import numpy as np
     from pylorenzmie_b200 import workloads
@@ -74,6 +109,7 @@ def cpu_fit_rate(nfeat, seed=0):
     for var in ('OMP_NUM_THREADS', 'MKL_NUM_THREADS', 'OPENBLAS_NUM_THREADS'):
         os.environ[var] = '1'
     ctx = mp.get_context('spawn')
+    ref = None
     with ctx.Pool(cores) as pool:
         data = pool.starmap(bench_tasks.render_201,
                             [(truth[i], 1000 + i) for i in range(nfeat)])
@@ -81,7 +117,26 @@ def cpu_fit_rate(nfeat, seed=0):
         res = pool.starmap(bench_tasks.fit_201,
                            [(data[i], start[i]) for i in range(nfeat)])
         dt = time.perf_counter() - t0
+        if reference:
+            t1 = time.perf_counter()
+            rres = pool.starmap(_reference_fit_201,
+                                [(data[i], start[i]) for i in range(nfeat)])
+            rdt = time.perf_counter() - t1
+            if all(r is not None for r in rres):
+                keys = ('x_p', 'y_p', 'z_p', 'a_p', 'n_p')
+                ref = {'value': nfeat / rdt, 'unit': UNIT, 'cores': cores,
+                       'kind': 'reference',
+                       'sample': f'the same {nfeat} crops, {rdt:.1f} s wall '
+                                 f'on {cores} processes',
+                       'success_fraction': float(np.mean(
+                           [r['success'] for r in rres])),
+                       'max_abs_diff_vs_port': {
+                           k: float(max(abs(r[k] - o[k])
+                                        for r, o in zip(rres, res)))
+                           for k in keys}}
     ok = float(np.mean([r['success'] for r in res]))
+    if reference:
+        return nfeat / dt, cores, dt, ok, ref
     return nfeat / dt, cores, dt, ok
 
 
@@ -188,12 +243,17 @@ def b200_arm(args):
         # before the first GPU call: the pool uses spawn anyway
         cores = os.cpu_count() or 1
         sample = min(max(2 * cores, 8), 64)
-        rate, cores, dt, ok = cpu_fit_rate(sample, seed=3)
+        rate, cores, dt, ok, ref_opt = cpu_fit_rate(sample, seed=3,
+                                                    reference=True)
         cpu_base = {'value': rate, 'unit': UNIT, 'cores': cores,
                     'kind': 'port',
                     'sample': f'{sample} features of the same workload, '
                               f'oracle FP64 model + scipy lm (FD Jacobian), '
-                              f'{dt:.1f} s wall on {cores} processes'}
+                              f'{dt:.1f} s wall on {cores} processes',
+                    # the reference's own Optimizer on the same crops
+                    'reference_optimizer': ref_opt or {
+                        'unavailable': 'reference not installed in '
+                                       'baseline/_ref'}}
 
     import ctypes
     import numpy as np
