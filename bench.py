@@ -62,25 +62,41 @@ def dist_env():
 # ---------------------------------------------------------------------------
 # CPU side: the reference algorithm (oracle) on the host cores
 
-def _reference_fit_201(data, start):
-    '''One 201x201 fit by the reference's own Optimizer, installed in
-    baseline/_ref: its numpy LorenzMie (theory/LorenzMie.py) and
-    scipy least_squares with the forward-difference Jacobian
-    (analysis/Optimizer.py:196-222), default variables and settings.
-    Returns the fitted values and success, or None without the install.'''
+def _import_reference():
+    '''Pool initializer: import the reference (baseline/_ref) once per
+    worker, before anything is timed.'''
+    try:
+        _reference_modules()
+    except Exception:  # pragma: no cover - reported by the fit itself
+        pass
+
+
+def _reference_modules():
     import types
-    import numpy as np
     ref = ROOT / 'baseline' / '_ref'
     if not (ref / 'pylorenzmie').is_dir():
         return None
     if str(ref) not in sys.path:
         sys.path.insert(0, str(ref))
     sys.modules.setdefault('trackpy', types.ModuleType('trackpy'))
-    from pylorenzmie.theory.LorenzMie import LorenzMie as RefLorenzMie
-    from pylorenzmie.theory import Sphere as RefSphere
-    from pylorenzmie.theory import Instrument as RefInstrument
-    from pylorenzmie.analysis.Optimizer import Optimizer as RefOptimizer
-    from pylorenzmie.analysis.Hologram import Hologram as RefHologram
+    from pylorenzmie.theory.LorenzMie import LorenzMie
+    from pylorenzmie.theory import Sphere, Instrument
+    from pylorenzmie.analysis.Optimizer import Optimizer
+    from pylorenzmie.analysis.Hologram import Hologram
+    return LorenzMie, Sphere, Instrument, Optimizer, Hologram
+
+
+def _reference_fit_201(data, start):
+    '''One 201x201 fit by the reference's own Optimizer, installed in
+    baseline/_ref: its numpy LorenzMie (theory/LorenzMie.py) and
+    scipy least_squares with the forward-difference Jacobian
+    (analysis/Optimizer.py:196-222), default variables and settings.
+    Returns the fitted values and success, or None without the install.'''
+    import numpy as np
+    mods = _reference_modules()
+    if mods is None:
+        return None
+    RefLorenzMie, RefSphere, RefInstrument, RefOptimizer, RefHologram = mods
     inst = RefInstrument()
     inst.magnification, inst.wavelength, inst.n_m = 0.048, 0.447, 1.340
     part = RefSphere()
@@ -110,7 +126,8 @@ def cpu_fit_rate(nfeat, seed=0, reference=False):
         os.environ[var] = '1'
     ctx = mp.get_context('spawn')
     ref = None
-    with ctx.Pool(cores) as pool:
+    with ctx.Pool(cores,
+                  initializer=_import_reference if reference else None) as pool:
         data = pool.starmap(bench_tasks.render_201,
                             [(truth[i], 1000 + i) for i in range(nfeat)])
         t0 = time.perf_counter()

@@ -320,9 +320,16 @@ int lmb_hologram_aberrated(const double* coords, long long npts,
                       nmax_cap, k, flags, out, stream, aberration);
 }
 
+// Threads (pixels) per k_chi2 block.  Fixed, so that a crop's pixels fall
+// into the same blocks whatever else shares the launch (its chi^2 is then
+// bit-identical searched alone or beside others); 128 rather than 256
+// because a DE crop's ~300 pixels left most of a second 256-thread block
+// waiting at its barriers.
+constexpr int CHI2_TPB = 128;
+
 size_t lmb_chi2_workspace_bytes(long long npts, int nitems) {
   if (npts <= 0 || nitems <= 0) return 0;
-  const size_t n = size_t((npts + 255) / 256) * size_t(nitems);
+  const size_t n = size_t((npts + CHI2_TPB - 1) / CHI2_TPB) * size_t(nitems);
   return align_up(n * sizeof(double), 256) + n * sizeof(int);
 }
 
@@ -347,10 +354,11 @@ static int chi2_launch(const double* coords, long long npts, const double* data,
     return LMB_OK;
   }
   if (!coords || !data || !spheres || !item_start || !ab || !nmax) return LMB_ERR_ARG;
-  if (nitems > 65535 || (span + 255) / 256 > 0x7fffffffLL) return LMB_ERR_ARG;
+  if (nitems > 65535 || (span + CHI2_TPB - 1) / CHI2_TPB > 0x7fffffffLL)
+    return LMB_ERR_ARG;
   if (!workspace || workspace_bytes < lmb_chi2_workspace_bytes(span, nitems))
     return LMB_ERR_WORKSPACE;
-  const int tpb = 256;
+  const int tpb = CHI2_TPB;
   const int nb = int((span + tpb - 1) / tpb);
   double* partial = reinterpret_cast<double*>(workspace);
   int* partial_bad = reinterpret_cast<int*>(
