@@ -345,3 +345,17 @@ def test_packed_write_range_any_cut():
     assert np.all(out[:a] == -1.) and np.all(out[b:] == -1.)
     np.testing.assert_array_equal(pk.write_data(np.empty(pk.total, np.float32)),
                                   ref)
+
+
+def test_chi2_workspace_blocks_of_128():
+    '''The population chi^2 partials: one per 128-pixel block of the largest
+    crop and per item (a DE crop of 293 pixels takes 3 blocks), then an
+    int flag per partial; 0 for an empty launch.'''
+    lib = _native.load()
+    for npts, nitems in [(293, 960), (128, 1), (129, 7), (40401, 3)]:
+        nb = (npts + 127) // 128
+        n = nb * nitems
+        want = (n * 8 + 255) // 256 * 256 + n * 4
+        assert lib.lmb_chi2_workspace_bytes(npts, nitems) == want
+    assert lib.lmb_chi2_workspace_bytes(0, 5) == 0
+    assert lib.lmb_chi2_workspace_bytes(10, 0) == 0
