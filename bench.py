@@ -454,6 +454,12 @@ def b200_arm(args):
     if rank == 0 and world == 1 and not args.no_extras:
         extras = run_extras(dev, inst, value)
     ns = north_star(value, extras)
+    ref_opt = (cpu_base or {}).get('reference_optimizer', {})
+    if 'max_abs_diff_vs_port' in ref_opt:
+        # the oracle's restatement of the fit against the reference's own
+        # Optimizer on the same crops (the pin of the CPU baseline)
+        ns['reference_optimizer_vs_oracle_fit_max_abs'] = \
+            ref_opt['max_abs_diff_vs_port']
 
     # the FP32 peak from the clock: SMs x 128 FP32 lanes x 2 FLOP x MHz
     csum = clocks.summary()
