@@ -21,9 +21,13 @@ from . import _native
 
 _lock = threading.Lock()
 _memory = {}
-PROBE_FEATURES = 32
+# the probe batch: up to PROBE_FEATURES of the caller's features (a shape
+# that is fastest on a few features need not be on a full batch, whose
+# tiles fill the GPU differently, so the batch size is part of the class)
+PROBE_FEATURES = 256
 NMAX_BUCKETS = (32, 64, 128, 256, 1024)
 PIXEL_BUCKETS = (64 * 64, 128 * 128, 256 * 256, 512 * 512)
+BATCH_BUCKETS = (64, 256)
 
 
 def cache_path():
@@ -54,9 +58,11 @@ def _bucket(value, edges):
     return edges[-1] * 2
 
 
-def problem_key(gpu_name, nmax_cap, mean_pixels, layered=False):
+def problem_key(gpu_name, nmax_cap, mean_pixels, layered=False,
+                batch=PROBE_FEATURES):
     return (f'{gpu_name}|nmax<={_bucket(nmax_cap, NMAX_BUCKETS)}|'
             f'px<={_bucket(mean_pixels, PIXEL_BUCKETS)}|'
+            f'b<={_bucket(batch, BATCH_BUCKETS)}|'
             f'{"layered" if layered else "sphere"}')
 
 
@@ -100,7 +106,7 @@ def tune(packed, starts, instrument, variables, nmax_cap, layers=None,
     name = torch.cuda.get_device_name(dev)
     B = packed.features.shape[0]
     mean_px = float(packed.features['npix'].mean()) if B else 0.
-    key = problem_key(name, nmax_cap, mean_px, layers is not None)
+    key = problem_key(name, nmax_cap, mean_px, layers is not None, B)
     hit = lookup(key)
     if hit is not None:
         return int(hit['config'])

@@ -1270,8 +1270,9 @@ k_fit_eval(FitCtx c) {
 // 6-column Jacobian of each.  (dx, dy, dz): pixel minus particle position.
 // With kRecompute the pixel geometry is formed again after the order loop
 // instead of being held in registers across it (the empty asm statements
-// keep the compiler from merging the two computations).
-template <bool kRecompute, bool kAberr = false>
+// keep the compiler from merging the two computations).  U: the order
+// loop's unroll factor.
+template <bool kRecompute, bool kAberr = false, int U = 2>
 __device__ inline void holo_jac_pair(double k, const double* dx,
                                      const double* dy, double dz, double zp,
                                      bool bohren, const float4* rec, int nm,
@@ -1281,7 +1282,7 @@ __device__ inline void holo_jac_pair(double k, const double* dx,
   for (int l = 0; l < 2; ++l)
     g[l] = geometry<float>(k, dx[l], dy[l], dz, 0., zp, bohren);
   PairSums P;
-  order_sum_jac_pair(pair_in(g[0], g[1]), rec, nm, P);
+  order_sum_jac_pair<U>(pair_in(g[0], g[1]), rec, nm, P);
   if (kRecompute) {
     for (int l = 0; l < 2; ++l) {
       double x = dx[l], y = dy[l];
@@ -1373,8 +1374,10 @@ k_fit_eval_pair(FitCtx c) {
       const double dx[2] = {x0 - ep.p[0], x1 - ep.p[0]};
       const double dy[2] = {y0 - ep.p[1], y1 - ep.p[1]};
       float H[2], dH[2][6];
-      holo_jac_pair<kRecompute, kAberr>(c.k, dx, dy, -ep.p[2], ep.p[2], bohren,
-                                        rec, nm, kf, H, dH, c.aberr);
+      // the order loop unrolled by 3 where a thread holds 4 or more pixel
+      // pairs (measured faster there), by 2 elsewhere
+      holo_jac_pair<kRecompute, kAberr, (PPT >= 8 ? 3 : 2)>(
+          c.k, dx, dy, -ep.p[2], ep.p[2], bohren, rec, nm, kf, H, dH, c.aberr);
 #pragma unroll
       for (int lane = 0; lane < 2; ++lane) {
         if (lane == 1 && !v1) break;

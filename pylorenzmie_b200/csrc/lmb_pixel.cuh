@@ -396,8 +396,9 @@ LMB_HD cplx<f2> pacc(cplx<f2> acc, f2 w, cplx<f2> v) {
 }
 
 // rec: PAIR_QUADS float4 per order (index n * PAIR_QUADS + j); the two
-// values of a float4 are (x, y) and (z, w).
-template <typename Q4>
+// values of a float4 are (x, y) and (z, w).  U: the order loop's unroll
+// factor (the fit's evaluation kernels pick it by their pixels per thread).
+template <int U = 2, typename Q4>
 LMB_HD void order_sum_jac_pair(const PairIn& in, const Q4* rec, int nmax,
                                PairSums& A) {
   const f2 z2 = pk(0.f, 0.f), m1 = pk(-1.f, -1.f);
@@ -413,7 +414,7 @@ LMB_HD void order_sum_jac_pair(const PairIn& in, const Q4* rec, int nmax,
   f2 dpim1 = z2, dpi = z2, ndd = z2;         // d/ds
   cplx<f2> h2 = in.hm1, h1 = in.h0, hp2 = zero, hp1 = zero;
   const f2 sv = in.sv, ikr = in.ikr, mkr = in.mkr;
-#pragma unroll 2
+#pragma unroll U
   for (int n = 1; n <= nmax; ++n) {
     const Q4* r = rec + PAIR_QUADS * n;
     f2 v[PAIR_VALUES];

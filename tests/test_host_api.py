@@ -298,6 +298,10 @@ def test_autotune_keys_and_cache(tmp_path, monkeypatch):
     k3 = autotune.problem_key('B200', 33, 201 * 201)
     assert k1 == k2 and k1 != k3
     assert 'layered' in autotune.problem_key('B200', 30, 100, layered=True)
+    # batches of up to 64, up to 256 and more are tuned apart
+    kb = [autotune.problem_key('B200', 30, 201 * 201, batch=b)
+          for b in (32, 64, 65, 256, 257, 1024)]
+    assert kb[0] == kb[1] != kb[2] == kb[3] != kb[4] == kb[5]
     assert autotune.cache_path() == tmp_path / 'tune.json'
     autotune._store('x', {'config': 3})
     autotune._memory.clear()
