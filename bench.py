@@ -453,7 +453,7 @@ def b200_arm(args):
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
         extras = run_extras(dev, inst, value)
-    ns = north_star(value, extras)
+    ns = target_figures(value, extras)
     ref_opt = (cpu_base or {}).get('reference_optimizer', {})
     if 'max_abs_diff_vs_port' in ref_opt:
         # the oracle's restatement of the fit against the reference's own
@@ -494,7 +494,7 @@ def b200_arm(args):
         'e2e': e2e,
         'gpu_launches': gpu_launches,
         'clocks': csum,
-        'north_star': ns,
+        'target_figures': ns,
         'extras': extras,
     }
     print(json.dumps(line), flush=True)
@@ -963,7 +963,7 @@ def layered_parity(opt, inst, dev, imgs, sides, start, frac, core, sub, df,
             'same_minimum_tight': shared, 'rows': rows}
 
 
-def north_star(chosen, extras):
+def target_figures(chosen, extras):
     '''The target figures of the hot path, beside their targets: the
     chosen form against plain FP64 on the same GPU, the FP32 frame
     hologram's error against FP64, and the fits against the oracle's.'''
